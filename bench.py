@@ -1,0 +1,300 @@
+"""Benchmark of the coupled lattice update on B200: MLUPS of the fused
+D3Q19-MRT + D3Q7 + pyrolysis step at 256^3 (FP32), one replica per GPU.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+                    [--workload pyro3d|pyro2d|flow2d] [--size S] [--precision fp32|fp16|fp64]
+
+One JSON line on rank 0.  ``value`` is whole-job MLUPS (cells x steps x ranks /
+max-over-ranks device time) with the state resident in HBM; ``e2e`` is the same
+metric through the public API with a host->device copy of the boundary values
+and a device->host read of the diagnostics every step.  Multi-GPU runs are
+independent replicas (one seeded geometry per rank, no data-path collective):
+weak scaling.  ``--impl reference`` times the CPU restatement of the reference
+step (the Taichi reference cannot run here) with every host thread.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+import numpy as np  # noqa: E402
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="pyro3d", choices=["pyro3d", "pyro2d", "flow2d"])
+    ap.add_argument("--size", type=int, default=0, help="edge length override (default: the workload's)")
+    ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "fp64"])
+    ap.add_argument("--collision", default="")
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps for the e2e leg (default: --steps)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--seed", type=int, default=0)
+    return ap.parse_args()
+
+
+def make_workload(args, seed):
+    from lbm_porouschem_b200 import workloads
+    if args.workload == "pyro3d":
+        n = args.size or 256
+        w = workloads.pyro3d(n, seed=seed, precision=args.precision, collision=args.collision or "mrt")
+    elif args.workload == "pyro2d":
+        nx = args.size or 512
+        w = workloads.pyro2d(nx, nx // 2, seed=seed, precision=args.precision, collision=args.collision or "bgk")
+    else:
+        nx = args.size or 256
+        w = workloads.flow2d(nx, nx // 2, seed=seed, precision=args.precision, collision=args.collision or "bgk")
+    return w
+
+
+def describe(w, args):
+    c = w.cfg
+    lat = "D2Q9+D2Q5" if c.dim == 2 else "D3Q19+D3Q7"
+    if c.thermal == "none":
+        lat = "D2Q9" if c.dim == 2 else "D3Q19"
+    return {
+        "workload": f"{w.name} {lat} {c.collision.upper()}" + (" conjugate-heat+pyrolysis" if c.pyro else "")
+                    + f" {c.precision}",
+        "cells": c.ncells, "porosity": round(w.porosity, 4),
+        "l2": "state larger than L2 (no flush needed)" if c.ncells * c.Q * 8 > 126e6 else "state fits in L2",
+    }
+
+
+# ----------------------------------------------------------------- clocks
+class ClockSampler:
+    """nvidia-smi samples during the timed region (read-only queries)."""
+
+    Q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+         "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+         "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.rows = []
+        self.proc = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.Q}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.rows.append([x.strip() for x in line.split(",")])
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = [r for r in self.rows if len(r) >= 9]
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"], "samples": 0}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "", 1).isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "", 1).isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ------------------------------------------------------------ CPU legs
+def cpu_leg(w, steps_wanted, budget_s, warmup=1):
+    """Time the CPU restatement (oracle/, FP32, OpenMP over all host threads) on the
+    same workload; run as many of `steps_wanted` full steps as fit in budget_s."""
+    from oracle import oracle
+    oracle.build_oracle()
+    o = oracle.Oracle(w.cfg, real="f32", threads=os.cpu_count())
+    o.init(w.solid, w.reactive, **w.init)
+    t0 = time.perf_counter()
+    o.step(warmup)
+    t_one = (time.perf_counter() - t0) / max(warmup, 1)
+    n = max(1, min(steps_wanted, int(budget_s / max(t_one, 1e-9))))
+    t0 = time.perf_counter()
+    o.step(n)
+    dt = time.perf_counter() - t0
+    cores = o.threads()
+    o.close()
+    return w.cfg.ncells * n / dt / 1e6, n, cores, dt
+
+
+def read_traffic(w):
+    """Per-step DRAM traffic of the step kernels from the committed ncu summary, if any."""
+    p = ROOT / "profiles" / f"traffic_{w.name}_{w.cfg.precision}.txt"
+    if not p.exists():
+        return None
+    for line in p.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_step:"):
+            return float(line.split(":", 1)[1])
+    return None
+
+
+# ---------------------------------------------------------------- main
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        w = make_workload(args, args.seed)
+        budget = 150.0
+        mlups, n, cores, dt = cpu_leg(w, args.steps, budget, warmup=max(1, min(args.warmup, 2)))
+        from lbm_porouschem_b200 import workloads as W
+        line = {
+            "impl": "reference", "metric": "coupled MLUPS", "value": round(mlups, 3), "unit": "MLUPS",
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(dt / n * 1e3, 3), "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded packing)",
+            "config": describe(w, args),
+            "cpu_baseline": {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+                             "sample": f"{n} full steps of the same workload (C restatement of the "
+                                       f"reference step, OpenMP; Taichi reference not runnable here)"},
+            "e2e": {"value": round(mlups, 3), "unit": "MLUPS", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line), flush=True)
+        return 0
+
+    import torch
+    import torch.distributed as dist
+    from lbm_porouschem_b200 import workloads as W
+    from lbm_porouschem_b200.lattice import Lattice
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        t = torch.tensor([v], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    w = make_workload(args, args.seed + rank)
+    cfg = w.cfg
+    stream = torch.cuda.Stream()
+    lat = Lattice(cfg, device=f"cuda:{local}", stream=stream)
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    alg_bytes = W.algorithmic_bytes_per_step(cfg, w.solid)
+    nbc = sum(1 for s in cfg.sides if s.active)
+
+    # ---- device-resident throughput (value)
+    with torch.cuda.stream(stream):
+        lat.step(args.warmup)
+    stream.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    ev0 = torch.cuda.Event(enable_timing=True)
+    ev1 = torch.cuda.Event(enable_timing=True)
+    ev0.record(stream)
+    lat.step(args.steps)
+    ev1.record(stream)
+    ev1.synchronize()
+    ms = ev0.elapsed_time(ev1)
+    clk = clocks.stop()
+    barrier()
+    torch.cuda.synchronize()
+    ms_max = max_over_ranks(ms)
+    value = cfg.ncells * args.steps * world / (ms_max * 1e-3) / 1e6
+    launches = args.steps * (2 if nbc else 1)
+
+    # ---- end to end through the public API (host copies inside the timed region)
+    k2 = args.e2e_steps or args.steps
+    sides = cfg.sides
+    pinned_diag = None
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k2):
+        lat.set_sides(sides)          # H2D: 6 side records from host memory
+        lat.step(1, diag=True)
+        pinned_diag = lat.read_diag()  # D2H: diagnostics (synchronises the stream)
+    e1.record(stream)
+    e1.synchronize()
+    wall = time.perf_counter() - t0
+    ms_e2e = max(e0.elapsed_time(e1), wall * 1e3)
+    ms_e2e = max_over_ranks(ms_e2e)
+    e2e_value = cfg.ncells * k2 * world / (ms_e2e * 1e-3) / 1e6
+    import ctypes
+    from lbm_porouschem_b200 import _native as N
+    h2d = 6 * ctypes.sizeof(N.lbm_side_desc)
+    d2h = 10 * 8
+
+    # ---- roofline of the step kernels (bulk + boundary): algorithmic bytes / event time
+    peaks = {}
+    pk = ROOT / "MEASURED_PEAKS.json"
+    if pk.exists():
+        peaks = json.loads(pk.read_text())
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    peak_src = "measured" if "hbm_gbs" in peaks else "fallback"
+    step_s = ms / args.steps * 1e-3
+    achieved = alg_bytes / step_s / 1e9
+    traffic = read_traffic(w)
+
+    if rank == 0:
+        line = {
+            "metric": "coupled MLUPS", "value": round(value, 2), "unit": "MLUPS", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(ms_max / args.steps, 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "fp16": "f16-storage/f32", "fp64": "f64"}[cfg.precision],
+            "data": "synthetic (seeded sphere/disk packing; one geometry per rank)",
+            "config": {**describe(w, args), "parallelism": f"replicas x{world}"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": traffic,
+                         "algorithmic_bytes_per_step": alg_bytes,
+                         "bytes_per_lu": round(alg_bytes / cfg.ncells, 2),
+                         "note": f"step kernels (bulk + boundary) per step; peak {peak_src}"},
+            "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h, "steps": k2},
+            "gpu_launches": launches,
+            "clocks": clk,
+            "diag_last": {k: pinned_diag[k] for k in ("mass", "energy", "umax", "nonfinite")},
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            mlups, n, cores, dt = cpu_leg(w, 50, 20.0)
+            line["cpu_baseline"] = {"value": round(mlups, 3), "unit": "MLUPS", "cores": cores, "kind": "port",
+                                    "sample": f"{n} full steps of {w.name} (FP32 C restatement, OpenMP)"}
+        print(json.dumps(line), flush=True)
+    lat.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,195 @@
+/*
+ * lbm_b200.h -- C ABI of the sm_100a lattice update of LBM_porousChem.
+ *
+ * The reference has no FFI: its solver object is the plug-in and its Taichi
+ * kernels are methods of the @ti.data_oriented solver class
+ * (src/LBM/LBM2D/__init__.py:29-70, src/LBM/LBM3D/__init__.py:11-62), selected
+ * by src/LBM/app.py:32-58.  Each entry point below replaces one piece of that
+ * class's hot path; the Python host layer (lbm_porouschem_b200.solver) keeps
+ * the class surface and calls these through ctypes.
+ *
+ * Conventions
+ *  - Plain C types only; no exceptions cross the ABI.  Every call returns an
+ *    int32 status (LBM_OK = 0); lbm_last_error() gives a message for the
+ *    calling thread's last failure.
+ *  - Device memory is owned by the caller (torch tensors on the Python side)
+ *    and handed over with lbm_bind(); sizes come from lbm_required_bytes().
+ *  - All GPU work is issued on the caller's stream (a cudaStream_t passed as
+ *    void*; NULL = legacy default stream).  One handle per host thread.
+ *  - Cell index c = x + nx*(y + ny*z) (x fastest).  A field shaped (nx,ny,nz)
+ *    in the reference's numpy convention is this layout in Fortran order.
+ */
+#ifndef LBM_B200_H
+#define LBM_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define LBM_ABI_VERSION 1
+
+#if defined(__GNUC__)
+#define LBM_API __attribute__((visibility("default")))
+#else
+#define LBM_API
+#endif
+
+/* status codes */
+#define LBM_OK 0
+#define LBM_ERR_ARG 1        /* bad argument or descriptor */
+#define LBM_ERR_UNBOUND 2    /* a required field has no device buffer */
+#define LBM_ERR_CUDA 3       /* a CUDA call failed */
+#define LBM_ERR_NONFINITE 4  /* diagnostics saw NaN/Inf */
+#define LBM_ERR_SIZE 5       /* a size exceeds a fixed limit */
+
+/* descriptor enums */
+#define LBM_COLL_BGK 0
+#define LBM_COLL_MRT 1
+#define LBM_PREC_FP32 0
+#define LBM_PREC_FP16 1 /* FP16 storage of f - w*rho0 and g - wt*T0, FP32 arithmetic */
+#define LBM_PREC_FP64 2
+#define LBM_EOS_IDEAL_GAS 0      /* util/flag.py:64-67 FLUID_STATE_EQUATION */
+#define LBM_EOS_INCOMPRESSIBLE 1
+#define LBM_THERMAL_NONE 0
+#define LBM_THERMAL_CONJUGATE 1  /* one temperature distribution over fluid and solid */
+#define LBM_BC_PERIODIC 0        /* util/flag.py:89-94 BC */
+#define LBM_BC_ZEROGRADIENT 1
+#define LBM_BC_FIXEDVALUE 2
+
+/* mask byte: bit0/bit1 = solid at even/odd step parity, bit2 = reactive solid */
+#define LBM_MASK_SOLID 3u
+#define LBM_MASK_REACTIVE 4u
+
+/* One domain side: 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+  (reference side order,
+ * src/LBM/LBM3D/_core.py:72).  active = 1 applies non-equilibrium
+ * extrapolation (BC_MODEL.NEE, src/LBM/LBM2D/_boundary.py:17-101) on that
+ * side; 0 leaves it periodic. */
+typedef struct lbm_side_desc {
+  int32_t active;
+  int32_t v_type;   /* LBM_BC_*, velocity  (set_BC mapping src/LBM/LBM2D/_io.py:385-402) */
+  int32_t rho_type; /* LBM_BC_*, density */
+  int32_t T_type;   /* LBM_BC_*, temperature distribution (_scalarField.py:83-122) */
+  double v[3];
+  double rho;
+  double T;         /* normalised temperature */
+} lbm_side_desc;
+
+typedef struct lbm_desc {
+  int32_t struct_size;  /* = sizeof(lbm_desc); guards ABI drift */
+  int32_t dim;          /* 2: D2Q9 + D2Q5, 3: D3Q19 + D3Q7 */
+  int32_t nx, ny, nz;   /* nz = 1 for dim 2 */
+  int32_t collision;    /* LBM_COLL_* */
+  int32_t precision;    /* LBM_PREC_* */
+  int32_t eos;          /* LBM_EOS_* */
+  int32_t thermal;      /* LBM_THERMAL_* */
+  int32_t pyro;         /* 1: Arrhenius pyrolysis with solid->fluid flip (needs thermal) */
+  int32_t half_force_velocity; /* 1: u includes F/2 (reference: 0) */
+  int32_t reserved0;
+  double nu;            /* lattice viscosity visco*dt/dx^2 (_evolution.py:227-249) */
+  double force[3];      /* body acceleration in lattice units (Guo forcing) */
+  double tauT_fluid;    /* thermal relaxation time in fluid cells */
+  double tauT_solid;    /* thermal relaxation time in solid cells */
+  double pyro_A, pyro_b, pyro_Ea, pyro_Tmin; /* k = A (T+1e-6)^b exp(-Ea/(R(T+1e-6))), T>Tmin */
+  double T_ref, T_scale;  /* T_phys = T*T_scale + T_ref (_scalarField.py:39-42) */
+  double dt_phys;         /* seconds per lattice step */
+  double heat_norm;       /* dH/(c_s T_scale): normalised temperature drop per unit dalpha */
+  double gas_coef;        /* (1 - char_yield)*rho_s: gas mass released per unit dalpha */
+  double alpha_flip;      /* reactive fraction below which a solid cell turns fluid */
+  double mrt_s[19];       /* MRT rates per moment; viscous moments use 1/tau(rho) */
+  double rho0, T0;        /* FP16 storage shift references */
+  lbm_side_desc side[6];
+} lbm_desc;
+
+/* Diagnostics (FP64 accumulation).  No reference counterpart except umax,
+ * Tmin, Tmax (src/LBM/LBM2D/_io.py:538-588). */
+typedef struct lbm_diag {
+  double mass;        /* sum rho over fluid cells */
+  double energy;      /* sum T over all cells (normalised) */
+  double solid_alpha; /* sum of reactive fraction over reactive solid cells */
+  double umax;        /* max |u| over fluid cells */
+  double Tmin, Tmax;  /* over all cells */
+  double nonfinite;   /* count of NaN/Inf in rho or T */
+  double nfluid;      /* fluid cell count */
+  double res_num;     /* sum |u - u_prev|^2 over fluid cells (residual numerator) */
+  double res_den;     /* sum |u|^2 over fluid cells */
+  int64_t step;       /* lattice steps taken since lbm_init_equilibrium */
+} lbm_diag;
+
+/* Bindable fields (lbm_bind / lbm_required_bytes). */
+#define LBM_FIELD_F 0       /* flow populations, 2 x Q planes (A/B), storage precision */
+#define LBM_FIELD_G 1       /* temperature populations, 2 x QT planes */
+#define LBM_FIELD_MASK 2    /* uint8 per cell */
+#define LBM_FIELD_ALPHA 3   /* float32 reactive fraction per cell */
+#define LBM_FIELD_REL 4     /* float32 gas release per cell, 2 planes */
+#define LBM_FIELD_RHO 5     /* macro outputs: rho (compute precision) */
+#define LBM_FIELD_U 6       /* 3 planes */
+#define LBM_FIELD_T 7
+#define LBM_FIELD_UPREV 8   /* 3 float32 planes, residual reference */
+#define LBM_FIELD_SCRATCH 9 /* reduction partials + control block */
+#define LBM_NUM_FIELDS 10
+
+/* lbm_step flags */
+#define LBM_STEP_DIAG 1      /* reduce diagnostics on the last step */
+#define LBM_STEP_MACRO 2     /* write rho/u/T planes on the last step */
+#define LBM_STEP_RESIDUAL 4  /* residual vs UPREV on the last step, then UPREV = u */
+
+typedef struct lbm_handle lbm_handle;
+
+LBM_API int32_t lbm_abi_version(void);
+LBM_API const char* lbm_last_error(void);
+
+/* Bytes the caller must allocate for field `field` under `desc`.
+ * Replaces the Taichi field declarations of src/LBM/LBM2D/_core.py:45-49
+ * (3D: src/LBM/LBM3D/_core.py:46-50). */
+LBM_API int32_t lbm_required_bytes(const lbm_desc* desc, int32_t field, size_t* bytes);
+
+/* Validate `desc` and create a handle.  Replaces LBM2D_BASE.__init__
+ * (src/LBM/LBM2D/_core.py:11-101) minus the field allocation. */
+LBM_API int32_t lbm_create(const lbm_desc* desc, lbm_handle** out);
+LBM_API int32_t lbm_destroy(lbm_handle* h);
+
+/* Hand a caller-owned device buffer to the handle. */
+LBM_API int32_t lbm_bind(lbm_handle* h, int32_t field, void* dev_ptr, size_t bytes);
+
+/* Replace the per-side boundary values (v, rho, T) without re-creating the
+ * handle; `host_sides` points to 6 lbm_side_desc in host memory (pinned for an
+ * asynchronous copy).  Replaces set_v_BC_value / set_rho_BC_value /
+ * set_TF_BC_value (src/LBM/LBM2D/_io.py:413-458) between steps. */
+LBM_API int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stream);
+
+/* Equilibrium initialisation from device planes rho[N], u[3N], T[N] (T may be
+ * NULL without thermal), alpha[N] (may be NULL without pyrolysis), all
+ * float32.  The solid mask must be bound first.  Replaces init_simulation /
+ * init_kernel (src/LBM/LBM2D/_initialize.py:16-65, LBM3D/_initialize.py:17-77).
+ * Resets the step counter. */
+LBM_API int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,
+                             const float* alpha, void* stream);
+
+/* Advance n lattice steps.  Replaces step() / step_kernel()
+ * (src/LBM/LBM2D/_evolution.py:12-25, src/LBM/LBM3D/_evolution.py:11-25). */
+LBM_API int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream);
+
+/* Recompute, without advancing or modifying the lattice, the outputs that
+ * `flags` (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL) ask for, for the
+ * state after the last step (rho/u/T planes, diagnostics).  Needs at least one
+ * step since lbm_init_equilibrium.  Replaces the field reads behind
+ * export_VTK_pyvista / log_info (src/LBM/LBM2D/_io.py:580-683). */
+LBM_API int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream);
+
+/* Copy the diagnostics reduced by the last LBM_STEP_DIAG step into *out
+ * (synchronises `stream`).  Replaces get_max_v / get_min_T / get_max_T
+ * (src/LBM/LBM2D/_io.py:538-579) and adds mass, energy, residual and the
+ * solid-mass integral.  Returns LBM_ERR_NONFINITE if NaN/Inf was seen. */
+LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
+
+/* Lattice steps taken since lbm_init_equilibrium (tLattice counter,
+ * src/LBM/LBM2D/_evolution.py:15). */
+LBM_API int64_t lbm_step_count(const lbm_handle* h);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* LBM_B200_H */

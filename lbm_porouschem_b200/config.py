@@ -1,0 +1,150 @@
+"""Lattice descriptor on the Python side, converted to ``lbm_desc`` for the C ABI.
+
+The enums mirror the reference's switches (src/LBM/util/flag.py:10-110); the
+side table mirrors ``set_BC`` (src/LBM/LBM2D/_io.py:385-402): an ``inlet``
+fixes velocity and extrapolates density, an ``outlet`` fixes density and
+extrapolates velocity, a ``wall`` fixes velocity to zero.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+from dataclasses import dataclass, field
+
+from . import _native as N
+
+PERIODIC, ZERO_GRADIENT, FIXED_VALUE = N.LBM_BC_PERIODIC, N.LBM_BC_ZEROGRADIENT, N.LBM_BC_FIXEDVALUE
+
+# d'Humieres et al. (2002) rates for D3Q19: e, eps, q, pi, m (viscous rows use 1/tau)
+MRT_RATES_3D = {1: 1.19, 2: 1.4, 4: 1.2, 6: 1.2, 8: 1.2, 10: 1.4, 12: 1.4, 16: 1.98, 17: 1.98, 18: 1.98}
+# Lallemand & Luo (2000) rates for D2Q9: e, eps, q
+MRT_RATES_2D = {1: 1.64, 2: 1.54, 4: 1.9, 6: 1.9}
+
+GAS_CONSTANT = 8.314441  # src/LBM/util/constant.py:17
+
+
+@dataclass
+class SideBC:
+    """One domain side.  ``active`` False keeps the side periodic."""
+    active: bool = False
+    v_type: int = PERIODIC
+    rho_type: int = PERIODIC
+    T_type: int = PERIODIC
+    v: tuple = (0.0, 0.0, 0.0)
+    rho: float = 1.0
+    T: float = 0.0
+
+    @staticmethod
+    def inlet(v, T_type=PERIODIC, T=0.0) -> "SideBC":
+        return SideBC(True, FIXED_VALUE, ZERO_GRADIENT, T_type, tuple(v), 1.0, T)
+
+    @staticmethod
+    def outlet(rho, T_type=PERIODIC, T=0.0) -> "SideBC":
+        return SideBC(True, ZERO_GRADIENT, FIXED_VALUE, T_type, (0.0, 0.0, 0.0), rho, T)
+
+    @staticmethod
+    def pressure(rho, T_type=PERIODIC, T=0.0) -> "SideBC":
+        """Fixed density with extrapolated velocity (an ``outlet`` used as a pressure inlet)."""
+        return SideBC.outlet(rho, T_type, T)
+
+    @staticmethod
+    def wall(T_type=PERIODIC, T=0.0) -> "SideBC":
+        return SideBC(True, FIXED_VALUE, ZERO_GRADIENT, T_type, (0.0, 0.0, 0.0), 1.0, T)
+
+
+@dataclass
+class LatticeConfig:
+    dim: int
+    nx: int
+    ny: int
+    nz: int = 1
+    collision: str = "bgk"          # "bgk" | "mrt"
+    precision: str = "fp32"         # "fp32" | "fp16" | "fp64"
+    eos: str = "ideal_gas"          # "ideal_gas" | "incompressible"
+    nu: float = 0.1                 # lattice viscosity; tau = 3 nu/rho + 1/2 (ideal gas)
+    force: tuple = (0.0, 0.0, 0.0)  # body acceleration (lattice units)
+    half_force_velocity: bool = False
+    thermal: str = "none"           # "none" | "conjugate"
+    tauT_fluid: float = 0.6
+    tauT_solid: float = 0.9
+    pyro: bool = False
+    pyro_A: float = 1e8             # 1/s
+    pyro_b: float = 0.0
+    pyro_Ea: float = 1.25e5         # J/mol
+    pyro_Tmin: float = 0.0          # K
+    T_ref: float = 300.0            # K at T = 0
+    T_scale: float = 500.0          # K per unit T
+    dt_phys: float = 1e-4           # s per lattice step
+    heat_norm: float = 0.8          # dH/(c_s T_scale) = 4e5/(1000*500)
+    gas_coef: float = 0.75          # (1 - char yield) * rho_s, rho_s = 1 lattice unit
+    alpha_flip: float = 0.01
+    mrt_rates: dict = field(default_factory=dict)
+    rho0: float = 1.0
+    T0: float = 0.0
+    sides: list = field(default_factory=lambda: [SideBC() for _ in range(6)])
+
+    @property
+    def shape(self) -> tuple:
+        return (self.nx, self.ny, self.nz)
+
+    @property
+    def ncells(self) -> int:
+        return self.nx * self.ny * self.nz
+
+    @property
+    def Q(self) -> int:
+        return 9 if self.dim == 2 else 19
+
+    @property
+    def QT(self) -> int:
+        return 5 if self.dim == 2 else 7
+
+    def replace(self, **kw) -> "LatticeConfig":
+        c = dataclasses.replace(self, **kw)
+        c.sides = [dataclasses.replace(s) for s in (kw.get("sides") or self.sides)]
+        return c
+
+    def tau(self, rho: float = 1.0) -> float:
+        nu = self.nu / rho if self.eos == "ideal_gas" else self.nu
+        return 3.0 * nu + 0.5
+
+    def mrt_s(self) -> list:
+        base = MRT_RATES_2D if self.dim == 2 else MRT_RATES_3D
+        s = [0.0] * 19
+        for r, v in base.items():
+            s[r] = v
+        for r, v in self.mrt_rates.items():
+            s[int(r)] = float(v)
+        return s
+
+    def to_desc(self) -> N.lbm_desc:
+        d = N.lbm_desc()
+        d.struct_size = ctypes.sizeof(N.lbm_desc)
+        d.dim, d.nx, d.ny, d.nz = self.dim, self.nx, self.ny, (1 if self.dim == 2 else self.nz)
+        d.collision = {"bgk": N.LBM_COLL_BGK, "mrt": N.LBM_COLL_MRT}[self.collision]
+        d.precision = {"fp32": N.LBM_PREC_FP32, "fp16": N.LBM_PREC_FP16, "fp64": N.LBM_PREC_FP64}[self.precision]
+        d.eos = {"ideal_gas": N.LBM_EOS_IDEAL_GAS, "incompressible": N.LBM_EOS_INCOMPRESSIBLE}[self.eos]
+        d.thermal = {"none": N.LBM_THERMAL_NONE, "conjugate": N.LBM_THERMAL_CONJUGATE}[self.thermal]
+        d.pyro = int(self.pyro)
+        d.half_force_velocity = int(self.half_force_velocity)
+        d.nu = self.nu
+        for i in range(3):
+            d.force[i] = float(self.force[i])
+        d.tauT_fluid, d.tauT_solid = self.tauT_fluid, self.tauT_solid
+        d.pyro_A, d.pyro_b, d.pyro_Ea, d.pyro_Tmin = self.pyro_A, self.pyro_b, self.pyro_Ea, self.pyro_Tmin
+        d.T_ref, d.T_scale, d.dt_phys = self.T_ref, self.T_scale, self.dt_phys
+        d.heat_norm, d.gas_coef, d.alpha_flip = self.heat_norm, self.gas_coef, self.alpha_flip
+        for r, v in enumerate(self.mrt_s()):
+            d.mrt_s[r] = v
+        d.rho0, d.T0 = self.rho0, self.T0
+        fill_sides(d.side, self.sides)
+        return d
+
+
+def fill_sides(arr, sides) -> None:
+    for i, s in enumerate(sides):
+        arr[i].active = int(bool(s.active))
+        arr[i].v_type, arr[i].rho_type, arr[i].T_type = int(s.v_type), int(s.rho_type), int(s.T_type)
+        for k in range(3):
+            arr[i].v[k] = float(s.v[k])
+        arr[i].rho, arr[i].T = float(s.rho), float(s.T)

@@ -1,0 +1,165 @@
+// capi_internal.cuh -- handle layout and launch templates shared by the C-ABI
+// translation unit and the per-(lattice, precision) instantiation units.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+
+#include "step_kernels.cuh"
+
+namespace lbm {
+namespace capi {
+
+int fail(int code, const std::string& msg);
+
+#define LBM_CUDA_TRY(expr)                                                         \
+  do {                                                                             \
+    cudaError_t e__ = (expr);                                                      \
+    if (e__ != cudaSuccess)                                                        \
+      return ::lbm::capi::fail(LBM_ERR_CUDA, std::string(#expr) + ": " + cudaGetErrorString(e__)); \
+  } while (0)
+
+constexpr int kCtrlBytes = 6 * (int)sizeof(lbm_side_desc);
+
+inline size_t storage_bytes(int prec) { return prec == LBM_PREC_FP16 ? 2 : (prec == LBM_PREC_FP64 ? 8 : 4); }
+inline size_t compute_bytes(int prec) { return prec == LBM_PREC_FP64 ? 8 : 4; }
+inline int lat_q(int dim) { return dim == 2 ? 9 : 19; }
+inline int lat_qt(int dim) { return dim == 2 ? 5 : 7; }
+
+struct Launch {
+  int tx;             // threads per block along x (bulk kernel)
+  dim3 grid, block;   // bulk
+  int nfaces;         // active faces
+  int faces[6];
+  int bc_threads;
+  dim3 bc_grid;
+  int bulk_blocks, bc_blocks;
+};
+
+inline Launch plan(const lbm_desc& d, int tx) {
+  Launch L{};
+  L.tx = tx;
+  L.block = dim3(tx, 1, 1);
+  L.grid = dim3((d.nx + tx - 1) / tx, d.ny, d.nz);
+  L.bulk_blocks = (int)(L.grid.x * L.grid.y * L.grid.z);
+  L.nfaces = 0;
+  int maxcells = 0;
+  for (int s = 0; s < 6; ++s) {
+    if (!d.side[s].active) continue;
+    L.faces[L.nfaces++] = s;
+    const int cells = s < 2 ? d.ny * d.nz : (s < 4 ? d.nx * d.nz : d.nx * d.ny);
+    if (cells > maxcells) maxcells = cells;
+  }
+  for (int s = L.nfaces; s < 6; ++s) L.faces[s] = -1;
+  L.bc_threads = 128;
+  L.bc_grid = dim3((maxcells + L.bc_threads - 1) / L.bc_threads, L.nfaces > 0 ? L.nfaces : 1, 1);
+  L.bc_blocks = L.nfaces > 0 ? (int)(L.bc_grid.x * L.bc_grid.y) : 0;
+  return L;
+}
+
+inline int default_tx(const lbm_desc& d) {
+  if (d.dim == 2) return d.nx >= 64 ? 64 : 32;
+  return d.nx >= 128 ? 128 : (d.nx >= 64 ? 64 : 32);
+}
+
+}  // namespace capi
+}  // namespace lbm
+
+struct lbm_handle {
+  lbm_desc d;
+  size_t N;
+  void* ptr[LBM_NUM_FIELDS];
+  size_t bytes[LBM_NUM_FIELDS];
+  int64_t step;
+  lbm::capi::Launch L;
+  bool diag_valid;
+};
+
+namespace lbm {
+namespace capi {
+
+inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
+inline lbm_side_desc* scratch_sides(lbm_handle* h) {
+  const size_t rows = (size_t)(h->L.bulk_blocks + h->L.bc_blocks + 1) * kNumDiag * sizeof(double);
+  const size_t off = (rows + 255) / 256 * 256;
+  return (lbm_side_desc*)((char*)h->ptr[LBM_FIELD_SCRATCH] + off);
+}
+inline double* scratch_final(lbm_handle* h) {
+  return scratch_partials(h) + (size_t)(h->L.bulk_blocks + h->L.bc_blocks) * kNumDiag;
+}
+
+template <class S>
+StepParams<S> make_params(lbm_handle* h, int buf) {
+  using C = typename Store<S>::C;
+  const lbm_desc& d = h->d;
+  StepParams<S> p{};
+  p.nx = d.nx; p.ny = d.ny; p.nz = d.nz; p.N = h->N;
+  const int Q = lat_q(d.dim), QT = lat_qt(d.dim);
+  S* f = (S*)h->ptr[LBM_FIELD_F];
+  S* g = (S*)h->ptr[LBM_FIELD_G];
+  p.fA = f + (size_t)buf * Q * h->N;
+  p.fB = f + (size_t)(buf ^ 1) * Q * h->N;
+  if (g) { p.gA = g + (size_t)buf * QT * h->N; p.gB = g + (size_t)(buf ^ 1) * QT * h->N; }
+  p.mask = (uint8_t*)h->ptr[LBM_FIELD_MASK];
+  p.alpha = (float*)h->ptr[LBM_FIELD_ALPHA];
+  float* rel = (float*)h->ptr[LBM_FIELD_REL];
+  if (rel) { p.relA = rel + (size_t)buf * h->N; p.relB = rel + (size_t)(buf ^ 1) * h->N; }
+  p.par = buf;
+  p.eos = d.eos;
+  p.half_force = d.half_force_velocity;
+  p.has_force = (d.force[0] != 0 || d.force[1] != 0 || d.force[2] != 0);
+  p.nu = (C)d.nu; p.Fx = (C)d.force[0]; p.Fy = (C)d.force[1]; p.Fz = (C)d.force[2];
+  for (int r = 0; r < 19; ++r) {
+    double n2 = 0;
+    if (r < Q) {
+      for (int k = 0; k < Q; ++k) {
+        const double m = d.dim == 2 ? Lattice<2>::mrt(r, k) : Lattice<3>::mrt(r, k);
+        n2 += m * m;
+      }
+    }
+    p.mrt_sn[r] = n2 > 0 ? (C)(d.mrt_s[r] / n2) : (C)0;
+  }
+  p.itauT_f = d.thermal ? (C)1 / (C)d.tauT_fluid : (C)0;
+  p.itauT_s = d.thermal ? (C)1 / (C)d.tauT_solid : (C)0;
+  p.rho0 = (C)d.rho0; p.T0 = (C)d.T0;
+  p.pyA = (C)d.pyro_A; p.pyb = (C)d.pyro_b; p.pyEa = (C)d.pyro_Ea; p.pyTmin = (C)d.pyro_Tmin;
+  p.Tref = (C)d.T_ref; p.Tscale = (C)d.T_scale; p.dtp = (C)d.dt_phys;
+  p.heat_norm = (C)d.heat_norm; p.gas_coef = (C)d.gas_coef; p.alpha_flip = (C)d.alpha_flip;
+  p.active = 0;
+  for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
+  p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;
+  p.flags = 0;
+  p.partials = h->ptr[LBM_FIELD_SCRATCH] ? scratch_partials(h) : nullptr;
+  p.block_offset = 0;
+  p.rho_out = (C*)h->ptr[LBM_FIELD_RHO];
+  p.u_out = (C*)h->ptr[LBM_FIELD_U];
+  p.T_out = (C*)h->ptr[LBM_FIELD_T];
+  p.uprev = (float*)h->ptr[LBM_FIELD_UPREV];
+  return p;
+}
+
+// Launch one step (bulk + boundary) for handle h; defined per (lattice, storage)
+// in the inst_*.cu units.
+template <class Lt, class S>
+int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st);
+template <class Lt, class S>
+int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
+                  const float* alpha, int solid_bit, cudaStream_t st);
+
+#define LBM_EXTERN_INST(LT, ST)                                                                 \
+  extern template int dispatch_step<LT, ST>(lbm_handle*, StepParams<ST>, cudaStream_t);         \
+  extern template int dispatch_init<LT, ST>(lbm_handle*, StepParams<ST>, const float*, const float*, \
+                                            const float*, const float*, int, cudaStream_t);
+LBM_EXTERN_INST(Lattice<2>, float)
+LBM_EXTERN_INST(Lattice<3>, float)
+LBM_EXTERN_INST(Lattice<2>, __half)
+LBM_EXTERN_INST(Lattice<3>, __half)
+LBM_EXTERN_INST(Lattice<2>, double)
+LBM_EXTERN_INST(Lattice<3>, double)
+#undef LBM_EXTERN_INST
+
+}  // namespace capi
+}  // namespace lbm

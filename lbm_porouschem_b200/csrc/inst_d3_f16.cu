@@ -1,0 +1,55 @@
+// Explicit instantiation of the step/init launchers for one lattice and one
+// storage precision (split out so the kernels compile in parallel).
+#include "capi_internal.cuh"
+
+namespace lbm {
+namespace capi {
+
+template <class Lt, class S, int COLL, int THERM>
+static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
+  const Launch& L = h->L;
+  step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
+  if (L.nfaces > 0) {
+    p.block_offset = L.bulk_blocks;
+    const int4 f01 = make_int4(L.faces[0], L.faces[1], L.faces[2], L.faces[3]);
+    const int2 f2 = make_int2(L.faces[4], L.faces[5]);
+    step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, st>>>(p, f01, f2);
+  }
+}
+
+template <class Lt, class S>
+int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
+  const int coll = h->d.collision;
+  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
+#define LBM_CASE(C_, T_) \
+  if (coll == C_ && therm == T_) { launch_step<Lt, S, C_, T_>(h, p, st); return LBM_OK; }
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+#undef LBM_CASE
+  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
+}
+
+template <class Lt, class S>
+int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
+                  const float* alpha, int solid_bit, cudaStream_t st) {
+  const int coll = h->d.collision;
+  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
+  const int bs = 256;
+  const unsigned nb = (unsigned)((h->N + bs - 1) / bs);
+#define LBM_CASE(C_, T_)                                                                       \
+  if (coll == C_ && therm == T_) {                                                             \
+    init_equilibrium_kernel<Lt, S, C_, T_><<<nb, bs, 0, st>>>(p, rho, u, T, alpha, solid_bit); \
+    return LBM_OK;                                                                             \
+  }
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+#undef LBM_CASE
+  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
+}
+
+template int dispatch_step<Lattice<3>, __half>(lbm_handle*, StepParams<__half>, cudaStream_t);
+template int dispatch_init<Lattice<3>, __half>(lbm_handle*, StepParams<__half>, const float*, const float*, const float*,
+                                     const float*, int, cudaStream_t);
+
+}  // namespace capi
+}  // namespace lbm

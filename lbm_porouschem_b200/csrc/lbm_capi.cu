@@ -1,0 +1,271 @@
+// lbm_capi.cu -- host side of the C ABI declared in include/lbm_b200.h.
+//
+// Validates descriptors, keeps the caller's device buffers, and launches the
+// sm_100a kernels of step_kernels.cuh on the caller's stream.  No allocation
+// happens here: every buffer (including the reduction scratch) is bound by the
+// caller, sized by lbm_required_bytes().
+#include "capi_internal.cuh"
+
+using namespace lbm;
+using namespace lbm::capi;
+
+namespace lbm {
+namespace capi {
+thread_local std::string g_err;
+int fail(int code, const std::string& msg) {
+  g_err = msg;
+  return code;
+}
+}  // namespace capi
+}  // namespace lbm
+
+static int validate(const lbm_desc* d) {
+  if (!d) return fail(LBM_ERR_ARG, "desc is NULL");
+  if (d->struct_size != (int32_t)sizeof(lbm_desc))
+    return fail(LBM_ERR_ARG, "desc.struct_size mismatch (ABI drift)");
+  if (d->dim != 2 && d->dim != 3) return fail(LBM_ERR_ARG, "dim must be 2 or 3");
+  if (d->nx < 3 || d->ny < 3) return fail(LBM_ERR_ARG, "nx and ny must be >= 3");
+  if (d->dim == 2 && d->nz != 1) return fail(LBM_ERR_ARG, "nz must be 1 for dim 2");
+  if (d->dim == 3 && d->nz < 3) return fail(LBM_ERR_ARG, "nz must be >= 3 for dim 3");
+  const double N = (double)d->nx * d->ny * d->nz;
+  if (N * lat_q(d->dim) >= 2147483647.0)
+    return fail(LBM_ERR_SIZE, "nx*ny*nz*Q must stay below 2^31 (32-bit cell indices)");
+  if (d->collision != LBM_COLL_BGK && d->collision != LBM_COLL_MRT)
+    return fail(LBM_ERR_ARG, "unknown collision");
+  if (d->precision < LBM_PREC_FP32 || d->precision > LBM_PREC_FP64)
+    return fail(LBM_ERR_ARG, "unknown precision");
+  if (d->eos != LBM_EOS_IDEAL_GAS && d->eos != LBM_EOS_INCOMPRESSIBLE)
+    return fail(LBM_ERR_ARG, "unknown eos");
+  if (d->thermal != LBM_THERMAL_NONE && d->thermal != LBM_THERMAL_CONJUGATE)
+    return fail(LBM_ERR_ARG, "unknown thermal mode");
+  if (d->pyro && d->thermal == LBM_THERMAL_NONE)
+    return fail(LBM_ERR_ARG, "pyrolysis needs the thermal field");
+  if (!(d->nu > 0)) return fail(LBM_ERR_ARG, "nu must be > 0");
+  if (d->thermal && !(d->tauT_fluid > 0.5 && d->tauT_solid > 0.5))
+    return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");
+  for (int s = 0; s < 6; ++s) {
+    const lbm_side_desc& sd = d->side[s];
+    if (!sd.active) continue;
+    if (d->dim == 2 && s >= 4) return fail(LBM_ERR_ARG, "z sides cannot be active in 2D");
+    const int types[3] = {sd.v_type, sd.rho_type, sd.T_type};
+    for (int t : types)
+      if (t < LBM_BC_PERIODIC || t > LBM_BC_FIXEDVALUE) return fail(LBM_ERR_ARG, "bad side bc type");
+  }
+  if ((d->side[0].active && d->side[1].active && d->nx < 4) ||
+      (d->side[2].active && d->side[3].active && d->ny < 4) ||
+      (d->side[4].active && d->side[5].active && d->nz < 4))
+    return fail(LBM_ERR_ARG, "two active opposite sides need at least 4 cells between them");
+  return LBM_OK;
+}
+
+extern "C" {
+
+int32_t lbm_abi_version(void) { return LBM_ABI_VERSION; }
+const char* lbm_last_error(void) { return g_err.c_str(); }
+
+int32_t lbm_required_bytes(const lbm_desc* d, int32_t field, size_t* bytes) {
+  int rc = validate(d);
+  if (rc) return rc;
+  if (!bytes) return fail(LBM_ERR_ARG, "bytes is NULL");
+  const size_t N = (size_t)d->nx * d->ny * d->nz;
+  const size_t s = storage_bytes(d->precision), cb = compute_bytes(d->precision);
+  switch (field) {
+    case LBM_FIELD_F: *bytes = 2 * (size_t)lat_q(d->dim) * N * s; break;
+    case LBM_FIELD_G: *bytes = d->thermal ? 2 * (size_t)lat_qt(d->dim) * N * s : 0; break;
+    case LBM_FIELD_MASK: *bytes = N; break;
+    case LBM_FIELD_ALPHA: *bytes = d->pyro ? N * 4 : 0; break;
+    case LBM_FIELD_REL: *bytes = d->pyro ? 2 * N * 4 : 0; break;
+    case LBM_FIELD_RHO: *bytes = N * cb; break;
+    case LBM_FIELD_U: *bytes = 3 * N * cb; break;
+    case LBM_FIELD_T: *bytes = d->thermal ? N * cb : 0; break;
+    case LBM_FIELD_UPREV: *bytes = 3 * N * 4; break;
+    case LBM_FIELD_SCRATCH: {
+      const Launch L = plan(*d, default_tx(*d));
+      *bytes = (size_t)(L.bulk_blocks + L.bc_blocks + 1) * kNumDiag * sizeof(double) + kCtrlBytes + 256;
+      break;
+    }
+    default: return fail(LBM_ERR_ARG, "unknown field id");
+  }
+  return LBM_OK;
+}
+
+int32_t lbm_create(const lbm_desc* d, lbm_handle** out) {
+  int rc = validate(d);
+  if (rc) return rc;
+  if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+  lbm_handle* h = new lbm_handle();
+  h->d = *d;
+  h->N = (size_t)d->nx * d->ny * d->nz;
+  for (int i = 0; i < LBM_NUM_FIELDS; ++i) { h->ptr[i] = nullptr; h->bytes[i] = 0; }
+  h->step = 0;
+  h->L = plan(*d, default_tx(*d));
+  h->diag_valid = false;
+  *out = h;
+  return LBM_OK;
+}
+
+int32_t lbm_destroy(lbm_handle* h) {
+  delete h;
+  return LBM_OK;
+}
+
+int32_t lbm_bind(lbm_handle* h, int32_t field, void* ptr, size_t bytes) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  if (field < 0 || field >= LBM_NUM_FIELDS) return fail(LBM_ERR_ARG, "unknown field id");
+  size_t need = 0;
+  int rc = lbm_required_bytes(&h->d, field, &need);
+  if (rc) return rc;
+  if (bytes < need)
+    return fail(LBM_ERR_ARG, "buffer for field " + std::to_string(field) + " too small: " +
+                                 std::to_string(bytes) + " < " + std::to_string(need));
+  if (need > 0 && !ptr) return fail(LBM_ERR_ARG, "NULL device pointer");
+  if (ptr && ((uintptr_t)ptr % 16) != 0) return fail(LBM_ERR_ARG, "device pointer not 16-byte aligned");
+  h->ptr[field] = ptr;
+  h->bytes[field] = bytes;
+  return LBM_OK;
+}
+
+int64_t lbm_step_count(const lbm_handle* h) { return h ? h->step : -1; }
+
+}  // extern "C"
+
+// Calls fn.template operator()<Lattice, Storage>() for the handle's dim/precision.
+template <class Fn>
+static int with_types(lbm_handle* h, Fn&& fn) {
+  const int dim = h->d.dim, prec = h->d.precision;
+  if (dim == 2 && prec == LBM_PREC_FP32) return fn(Lattice<2>{}, float{});
+  if (dim == 3 && prec == LBM_PREC_FP32) return fn(Lattice<3>{}, float{});
+  if (dim == 2 && prec == LBM_PREC_FP16) return fn(Lattice<2>{}, __half{});
+  if (dim == 3 && prec == LBM_PREC_FP16) return fn(Lattice<3>{}, __half{});
+  if (dim == 2 && prec == LBM_PREC_FP64) return fn(Lattice<2>{}, double{});
+  if (dim == 3 && prec == LBM_PREC_FP64) return fn(Lattice<3>{}, double{});
+  return fail(LBM_ERR_ARG, "unsupported dim/precision");
+}
+
+static int check_bound(lbm_handle* h) {
+  const int need[] = {LBM_FIELD_F, LBM_FIELD_MASK, LBM_FIELD_SCRATCH};
+  for (int f : need)
+    if (!h->ptr[f]) return fail(LBM_ERR_UNBOUND, "field " + std::to_string(f) + " is not bound");
+  if (h->d.thermal && !h->ptr[LBM_FIELD_G]) return fail(LBM_ERR_UNBOUND, "field G is not bound");
+  if (h->d.pyro && (!h->ptr[LBM_FIELD_ALPHA] || !h->ptr[LBM_FIELD_REL]))
+    return fail(LBM_ERR_UNBOUND, "pyrolysis needs ALPHA and REL bound");
+  return LBM_OK;
+}
+
+extern "C" {
+
+int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stream) {
+  if (!h || !host_sides) return fail(LBM_ERR_ARG, "NULL argument");
+  if (!h->ptr[LBM_FIELD_SCRATCH]) return fail(LBM_ERR_UNBOUND, "scratch is not bound");
+  for (int s = 0; s < 6; ++s) {
+    const lbm_side_desc& a = h->d.side[s];
+    const lbm_side_desc& b = host_sides[s];
+    if (a.active != b.active || a.v_type != b.v_type || a.rho_type != b.rho_type || a.T_type != b.T_type)
+      return fail(LBM_ERR_ARG, "lbm_set_sides may change values only, not side types");
+  }
+  memcpy(h->d.side, host_sides, sizeof(h->d.side));
+  LBM_CUDA_TRY(cudaMemcpyAsync(scratch_sides(h), host_sides, kCtrlBytes, cudaMemcpyHostToDevice,
+                               (cudaStream_t)stream));
+  return LBM_OK;
+}
+
+int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,
+                             const float* alpha, void* stream) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if (!rho || !u) return fail(LBM_ERR_ARG, "rho and u are required");
+  if (h->d.thermal && !T) return fail(LBM_ERR_ARG, "T is required with the thermal field");
+  cudaStream_t st = (cudaStream_t)stream;
+  LBM_CUDA_TRY(cudaMemcpyAsync(scratch_sides(h), h->d.side, kCtrlBytes, cudaMemcpyHostToDevice, st));
+  const int solid_bit = (int)(h->step & 1);
+  rc = with_types(h, [&](auto lat, auto s) -> int {
+    using Lt = decltype(lat);
+    using S = decltype(s);
+    StepParams<S> p = make_params<S>(h, 0);
+    return dispatch_init<Lt, S>(h, p, rho, u, T, alpha, solid_bit, st);
+  });
+  if (rc) return rc;
+  LBM_CUDA_TRY(cudaGetLastError());
+  h->step = 0;
+  h->diag_valid = false;
+  return LBM_OK;
+}
+
+int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  if (n < 0) return fail(LBM_ERR_ARG, "n must be >= 0");
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if ((flags & LBM_STEP_MACRO) && (!h->ptr[LBM_FIELD_RHO] || !h->ptr[LBM_FIELD_U] ||
+                                   (h->d.thermal && !h->ptr[LBM_FIELD_T])))
+    return fail(LBM_ERR_UNBOUND, "LBM_STEP_MACRO needs RHO, U (and T) bound");
+  if ((flags & LBM_STEP_RESIDUAL) && !h->ptr[LBM_FIELD_UPREV])
+    return fail(LBM_ERR_UNBOUND, "LBM_STEP_RESIDUAL needs UPREV bound");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int i = 0; i < n; ++i) {
+    const int buf = (int)(h->step & 1);
+    const int fl = (i == n - 1) ? flags : 0;
+    rc = with_types(h, [&](auto lat, auto s) -> int {
+      using Lt = decltype(lat);
+      using S = decltype(s);
+      StepParams<S> p = make_params<S>(h, buf);
+      p.flags = fl;
+      return dispatch_step<Lt, S>(h, p, st);
+    });
+    if (rc) return rc;
+    if (fl) {
+      finalize_diag<<<1, 1024, 0, st>>>(scratch_partials(h), h->L.bulk_blocks + h->L.bc_blocks,
+                                       scratch_final(h));
+      h->diag_valid = true;
+    }
+    h->step += 1;
+  }
+  LBM_CUDA_TRY(cudaGetLastError());
+  return LBM_OK;
+}
+
+int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  if (h->step < 1) return fail(LBM_ERR_ARG, "no step taken yet: the initial fields are the state");
+  if (flags & ~(LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) return fail(LBM_ERR_ARG, "bad flags");
+  if (!flags) return LBM_OK;
+  int rc = check_bound(h);
+  if (rc) return rc;
+  if ((flags & LBM_STEP_MACRO) && (!h->ptr[LBM_FIELD_RHO] || !h->ptr[LBM_FIELD_U] ||
+                                   (h->d.thermal && !h->ptr[LBM_FIELD_T])))
+    return fail(LBM_ERR_UNBOUND, "LBM_STEP_MACRO needs RHO, U (and T) bound");
+  if ((flags & LBM_STEP_RESIDUAL) && !h->ptr[LBM_FIELD_UPREV])
+    return fail(LBM_ERR_UNBOUND, "LBM_STEP_RESIDUAL needs UPREV bound");
+  cudaStream_t st = (cudaStream_t)stream;
+  const int buf = (int)((h->step - 1) & 1);
+  rc = with_types(h, [&](auto lat, auto s) -> int {
+    using Lt = decltype(lat);
+    using S = decltype(s);
+    StepParams<S> p = make_params<S>(h, buf);
+    p.flags = flags | kStepPeek;
+    return dispatch_step<Lt, S>(h, p, st);
+  });
+  if (rc) return rc;
+  finalize_diag<<<1, 1024, 0, st>>>(scratch_partials(h), h->L.bulk_blocks + h->L.bc_blocks, scratch_final(h));
+  h->diag_valid = true;
+  LBM_CUDA_TRY(cudaGetLastError());
+  return LBM_OK;
+}
+
+int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
+  if (!h || !out) return fail(LBM_ERR_ARG, "NULL argument");
+  if (!h->diag_valid) return fail(LBM_ERR_ARG, "no diagnostics: call lbm_step with LBM_STEP_DIAG");
+  double v[kNumDiag];
+  cudaStream_t st = (cudaStream_t)stream;
+  LBM_CUDA_TRY(cudaMemcpyAsync(v, scratch_final(h), sizeof(v), cudaMemcpyDeviceToHost, st));
+  LBM_CUDA_TRY(cudaStreamSynchronize(st));
+  out->mass = v[0]; out->energy = v[1]; out->solid_alpha = v[2]; out->umax = v[3];
+  out->Tmin = v[4]; out->Tmax = v[5]; out->nonfinite = v[6]; out->nfluid = v[7];
+  out->res_num = v[8]; out->res_den = v[9];
+  out->step = h->step;
+  if (v[6] > 0) return fail(LBM_ERR_NONFINITE, "diagnostics saw NaN/Inf");
+  return LBM_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,211 @@
+"""Device-resident lattice driven through the C ABI.
+
+``Lattice`` owns the device buffers (torch tensors used purely as memory),
+binds them to a native handle and exposes init / step / diagnostics / field
+read-back.  It is the layer the reference-shaped solver classes in
+``solver.py`` sit on.  There is no CPU path: constructing a ``Lattice``
+without CUDA or without the built library raises.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional
+
+import numpy as np
+import torch
+
+from . import _native as N
+from .config import LatticeConfig, fill_sides
+from .geometry import fortran_flat, from_flat, mask_bytes
+
+_STORE_DTYPE = {"fp32": torch.float32, "fp16": torch.float16, "fp64": torch.float64}
+_COMPUTE_DTYPE = {"fp32": torch.float32, "fp16": torch.float32, "fp64": torch.float64}
+
+
+def _stream_handle(stream: Optional[torch.cuda.Stream]) -> int:
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return int(s.cuda_stream)
+
+
+class Lattice:
+    """One lattice instance on one GPU."""
+
+    def __init__(self, cfg: LatticeConfig, device: str | torch.device = "cuda",
+                 stream: Optional[torch.cuda.Stream] = None):
+        if not torch.cuda.is_available():
+            raise RuntimeError("the CUDA lattice update needs a GPU (no CPU fallback)")
+        self.lib = N.load()
+        self.cfg = cfg
+        self.device = torch.device(device)
+        self.stream = stream
+        self._desc = cfg.to_desc()
+        h = ctypes.c_void_p()
+        N.check(self.lib.lbm_create(ctypes.byref(self._desc), ctypes.byref(h)))
+        self._h = h
+        self.buf: dict[int, torch.Tensor] = {}
+        with torch.cuda.device(self.device):
+            for fid in range(N.LBM_NUM_FIELDS):
+                nbytes = ctypes.c_size_t()
+                N.check(self.lib.lbm_required_bytes(ctypes.byref(self._desc), fid, ctypes.byref(nbytes)))
+                if nbytes.value == 0:
+                    continue
+                t = torch.zeros(nbytes.value, dtype=torch.uint8, device=self.device)
+                N.check(self.lib.lbm_bind(self._h, fid, ctypes.c_void_p(t.data_ptr()), nbytes.value))
+                self.buf[fid] = t
+        self._init_fields: Optional[dict] = None
+        # pinned host staging for per-step boundary values (asynchronous H2D copy)
+        nb = ctypes.sizeof(N.lbm_side_desc) * 6
+        self._sides_pinned = torch.empty(nb, dtype=torch.uint8, pin_memory=True)
+        self._host_sides = (N.lbm_side_desc * 6).from_address(self._sides_pinned.data_ptr())
+        self._sides_evt: Optional[torch.cuda.Event] = None
+
+    # ----------------------------------------------------------- views
+    def _view(self, fid: int, dtype: torch.dtype) -> torch.Tensor:
+        return self.buf[fid].view(dtype)
+
+    @property
+    def f(self) -> torch.Tensor:
+        """Flow populations [2, Q, N] in storage precision (A/B buffers)."""
+        return self._view(N.LBM_FIELD_F, _STORE_DTYPE[self.cfg.precision]).view(2, self.cfg.Q, -1)
+
+    @property
+    def mask(self) -> torch.Tensor:
+        return self.buf[N.LBM_FIELD_MASK]
+
+    @property
+    def nsteps(self) -> int:
+        return int(self.lib.lbm_step_count(self._h))
+
+    def _s(self) -> ctypes.c_void_p:
+        return ctypes.c_void_p(_stream_handle(self.stream))
+
+    # ------------------------------------------------------- set-up
+    def set_geometry(self, solid: np.ndarray, reactive: Optional[np.ndarray] = None) -> None:
+        """Solid mask in the reference's (nx, ny[, nz]) numpy layout (True = solid)."""
+        m = mask_bytes(np.asarray(solid), None if reactive is None else np.asarray(reactive))
+        if m.size != self.cfg.ncells:
+            raise ValueError("mask shape does not match the lattice")
+        with self._on_stream():
+            self.mask.copy_(torch.from_numpy(m).to(self.device))
+
+    def _on_stream(self):
+        """Issue torch work on the lattice's stream so it orders with the kernels."""
+        return torch.cuda.stream(self.stream) if self.stream is not None else torch.cuda.stream(
+            torch.cuda.current_stream())
+
+    def _plane(self, v, ncomp: int = 1) -> torch.Tensor:
+        n = self.cfg.ncells
+        if np.isscalar(v):
+            return torch.full((ncomp * n,), float(v), dtype=torch.float32, device=self.device)
+        a = np.asarray(v, dtype=np.float64)
+        if ncomp == 1:
+            flat = fortran_flat(a.reshape(self.cfg.shape))
+        else:
+            flat = np.concatenate([fortran_flat(a[i].reshape(self.cfg.shape)) for i in range(ncomp)])
+        return torch.from_numpy(flat.astype(np.float32)).to(self.device)
+
+    def init(self, rho=1.0, u=(0.0, 0.0, 0.0), T=0.0, alpha=None) -> None:
+        """Equilibrium initialisation (reference init_kernel) from scalars or (nx,ny,nz) arrays.
+
+        ``u`` is a 3-tuple of scalars or an array shaped (3, nx, ny, nz)."""
+        with self._on_stream():
+            self._init(rho, u, T, alpha)
+
+    def _init(self, rho, u, T, alpha) -> None:
+        cfg = self.cfg
+        r = self._plane(rho)
+        if isinstance(u, (tuple, list)) and all(np.isscalar(x) for x in u):
+            uu = torch.cat([torch.full((cfg.ncells,), float(x), dtype=torch.float32, device=self.device)
+                            for x in u])
+        else:
+            uu = self._plane(u, 3)
+        tt = self._plane(T) if cfg.thermal != "none" else None
+        aa = self._plane(alpha) if (cfg.pyro and alpha is not None) else None
+        self._init_fields = {"rho": r, "u": uu, "T": tt}
+        N.check(self.lib.lbm_init_equilibrium(
+            self._h, ctypes.c_void_p(r.data_ptr()), ctypes.c_void_p(uu.data_ptr()),
+            ctypes.c_void_p(tt.data_ptr()) if tt is not None else None,
+            ctypes.c_void_p(aa.data_ptr()) if aa is not None else None, self._s()))
+        # macro planes start at the initial state (solid cells keep these values)
+        if N.LBM_FIELD_RHO in self.buf:
+            cd = _COMPUTE_DTYPE[cfg.precision]
+            self._view(N.LBM_FIELD_RHO, cd).copy_(r.to(cd))
+            self._view(N.LBM_FIELD_U, cd).copy_(uu.to(cd))
+            if tt is not None:
+                self._view(N.LBM_FIELD_T, cd).copy_(tt.to(cd))
+        if N.LBM_FIELD_UPREV in self.buf:
+            self._view(N.LBM_FIELD_UPREV, torch.float32).zero_()
+
+    def set_sides(self, sides) -> None:
+        """Change boundary values (not types) between steps; a pinned host->device copy."""
+        if self._sides_evt is not None:
+            self._sides_evt.synchronize()      # the previous copy has read the staging buffer
+        fill_sides(self._host_sides, sides)
+        N.check(self.lib.lbm_set_sides(self._h, self._host_sides, self._s()))
+        self._sides_evt = torch.cuda.Event()
+        self._sides_evt.record(self.stream if self.stream is not None else torch.cuda.current_stream())
+        self.cfg.sides = list(sides)
+
+    # ------------------------------------------------------- stepping
+    def step(self, n: int = 1, diag: bool = False, macro: bool = False, residual: bool = False) -> None:
+        flags = (N.LBM_STEP_DIAG if diag else 0) | (N.LBM_STEP_MACRO if macro else 0) | \
+                (N.LBM_STEP_RESIDUAL if residual else 0)
+        N.check(self.lib.lbm_step(self._h, int(n), flags, self._s()))
+
+    def compute(self, diag: bool = True, macro: bool = False, residual: bool = False) -> None:
+        """Recompute outputs for the current state without advancing it."""
+        flags = (N.LBM_STEP_DIAG if diag else 0) | (N.LBM_STEP_MACRO if macro else 0) | \
+                (N.LBM_STEP_RESIDUAL if residual else 0)
+        N.check(self.lib.lbm_compute_macro(self._h, flags, self._s()))
+
+    def read_diag(self) -> dict:
+        d = N.lbm_diag()
+        rc = self.lib.lbm_read_diag(self._h, ctypes.byref(d), self._s())
+        out = {k: getattr(d, k) for k, _ in N.lbm_diag._fields_}
+        if rc == N.LBM_ERR_NONFINITE:
+            out["nonfinite"] = max(out["nonfinite"], 1.0)
+            return out
+        N.check(rc)
+        return out
+
+    def diagnostics(self) -> dict:
+        """Diagnostics of the current state (recomputed if needed)."""
+        if self.nsteps == 0:
+            raise RuntimeError("no step taken yet")
+        self.compute(diag=True)
+        return self.read_diag()
+
+    def fields(self) -> dict:
+        """rho, u (3,nx,ny,nz) and T of the current state as numpy arrays (reference layout)."""
+        cfg = self.cfg
+        cd = _COMPUTE_DTYPE[cfg.precision]
+        if self.nsteps > 0:
+            self.compute(diag=True, macro=True)
+        torch.cuda.current_stream().synchronize() if self.stream is None else self.stream.synchronize()
+        rho = from_flat(self._view(N.LBM_FIELD_RHO, cd).cpu().numpy(), cfg.shape)
+        uf = self._view(N.LBM_FIELD_U, cd).cpu().numpy()
+        n = cfg.ncells
+        u = np.stack([from_flat(uf[i * n:(i + 1) * n], cfg.shape) for i in range(3)])
+        out = {"rho": rho, "u": u}
+        if cfg.thermal != "none":
+            out["T"] = from_flat(self._view(N.LBM_FIELD_T, cd).cpu().numpy(), cfg.shape)
+        if cfg.pyro:
+            out["alpha"] = from_flat(self._view(N.LBM_FIELD_ALPHA, torch.float32).cpu().numpy(), cfg.shape)
+        par = self.nsteps & 1
+        m = self.mask.cpu().numpy()
+        out["solid"] = from_flat(((m >> par) & 1).astype(bool), cfg.shape)
+        return out
+
+    def close(self) -> None:
+        if getattr(self, "buf", None):
+            (self.stream or torch.cuda.current_stream()).synchronize()
+        if getattr(self, "_h", None) is not None and self._h.value:
+            self.lib.lbm_destroy(self._h)
+            self._h = ctypes.c_void_p()
+        self.buf.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -1,0 +1,554 @@
+/*
+ * lbm_oracle.c -- CPU restatement of LBM_porousChem's per-timestep lattice update.
+ *
+ * TEST INFRASTRUCTURE ONLY.  This file is the checker for the CUDA path: the
+ * tests, the smoke entry and the bench's CPU-baseline leg call it.  Nothing in
+ * the product links or executes it.
+ *
+ * PARITY UNPINNED: the reference (Python + Taichi 1.7.4) cannot run in this
+ * environment (Taichi is not installed and there is no network) and its own
+ * tests pin no lattice numbers.  This restatement follows the reference's code
+ * line by line where the reference defines the behaviour, and defines the new
+ * behaviour (body force, conjugate heat, pyrolysis with cell flip, MRT,
+ * reductions) where the reference has none.  It is pinned instead by analytic
+ * known answers (Poiseuille, mass conservation, equilibrium fixed point, the
+ * single-cell Arrhenius ODE) in tests/test_oracle_*.py.
+ *
+ * Structure mirrors the reference's push scheme:
+ *   step():  collision_source_streaming (push, halfway bounce-back)
+ *            -> macro (moments, sources, pyrolysis, flips)
+ *            -> non-equilibrium-extrapolation boundaries (NEE)
+ *   src/LBM/LBM2D/_evolution.py:12-25   (step / step_kernel)
+ *   src/LBM/LBM2D/_evolution.py:26-115  (collision_source_streaming)
+ *   src/LBM/LBM2D/_evolution.py:118-202 (macro)
+ *   src/LBM/LBM2D/_boundary.py:17-101   (Boundary_condition_NEE, flow sides)
+ *   src/LBM/LBM2D/_scalarField.py:83-122 (scalar NEE)
+ *   3D twins: src/LBM/LBM3D/_evolution.py:11-195, LBM3D/_boundary.py:15-142,
+ *             LBM3D/_scalarField.py:83-140.
+ *
+ * Build twice: -DREAL=float (FP32 oracle) and -DREAL=double (FP64 oracle).
+ * Cell index: c = x + nx*(y + ny*z).  Distribution storage: f[c*Q + k].
+ */
+#include <math.h>
+#include <stdint.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#ifndef REAL
+#define REAL double
+#endif
+
+/* ---------------------------------------------------------------- lattices */
+/* D2Q9 / D2Q5: src/LBM/LBM2D/_initialize.py:25-35, opposite table _core.py:35 */
+static const int E9[9][3] = {{0,0,0},{1,0,0},{0,1,0},{-1,0,0},{0,-1,0},
+                             {1,1,0},{-1,1,0},{-1,-1,0},{1,-1,0}};
+static const int OPP9[9] = {0,3,4,1,2,7,8,5,6};
+/* D3Q19 / D3Q7: src/LBM/LBM3D/_initialize.py:25-43, opposite table _core.py:36 */
+static const int E19[19][3] = {{0,0,0},{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1},{0,0,-1},
+                               {1,1,0},{-1,1,0},{1,-1,0},{-1,-1,0},
+                               {1,0,1},{-1,0,1},{1,0,-1},{-1,0,-1},
+                               {0,1,1},{0,-1,1},{0,1,-1},{0,-1,-1}};
+static const int OPP19[19] = {0,2,1,4,3,6,5,10,9,8,7,14,13,12,11,18,17,16,15};
+
+/* ------------------------------------------------------------------ config */
+enum { ORC_BC_PERIODIC = 0, ORC_BC_ZEROGRAD = 1, ORC_BC_FIXED = 2 };
+
+typedef struct orc_side {
+    int active;      /* 1: NEE applied on this side (reference BC_MODEL.NEE) */
+    int v_type;      /* ORC_BC_* for velocity  (LBM2D/_io.py:385-402 set_BC mapping) */
+    int rho_type;    /* ORC_BC_* for density */
+    int T_type;      /* ORC_BC_* for the temperature distribution */
+    double v[3];
+    double rho;
+    double T;
+} orc_side;
+
+typedef struct orc_cfg {
+    int dim, nx, ny, nz;
+    int collision;           /* 0 BGK, 1 MRT */
+    int eos;                 /* 0 IDEAL_GAS (tau = 3 nu/rho + 1/2), 1 INCOMPRESSIBLE */
+    double nu;               /* lattice viscosity (visco*dt/dx^2), _evolution.py:227-249 */
+    double force[3];         /* body acceleration (new; reference volume_force = 0) */
+    int half_force_velocity; /* 1: u = (sum e f + F/2)/rho.  Reference: 0 (_evolution.py:123-130) */
+    int thermal;             /* 0 none, 1 conjugate single field */
+    double tauT_fluid, tauT_solid;
+    int pyro;
+    double pyro_A, pyro_b, pyro_Ea, pyro_Tmin;  /* Arrhenius, LBM2D/_chemical.py:198-212 */
+    double T_ref, T_scale;   /* T_phys = T*T_scale + T_ref, _scalarField.py:39-42 */
+    double dt_phys;          /* seconds per lattice step */
+    double heat_norm;        /* dH/(c_s*T_scale): normalised temperature drop per unit dalpha */
+    double gas_coef;         /* (1-char_yield)*rho_s: gas mass released per unit dalpha */
+    double alpha_flip;       /* reactive fraction below which a solid cell turns fluid */
+    double mrt_s[19];        /* MRT relaxation rates per moment (viscous ones overwritten by 1/tau) */
+    orc_side side[6];        /* 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+ */
+} orc_cfg;
+
+/* mask bits */
+#define ORC_SOLID 1u
+#define ORC_REACTIVE 4u
+
+typedef struct orc {
+    orc_cfg c;
+    int Q, QT;
+    long N;
+    int e[19][3];
+    int opp[19];
+    REAL w[19], wt[7];
+    REAL ta, tb, tc;          /* thermal equilibrium coefficients (3,4.5,1.5) / (4,8,2) */
+    double M[19][19];         /* MRT moment matrix (rows orthogonal) */
+    double Mn[19];            /* squared row norms */
+    int visc_row[19];         /* 1 if the moment relaxes with 1/tau */
+    int cons_row[19];         /* 1 if the moment is conserved (rho, j): never relaxed */
+    REAL *f, *F, *g, *G;
+    REAL *rho, *u, *T, *dS, *alpha, *rel;
+    uint8_t *mask, *mask_next;
+} orc;
+
+/* ------------------------------------------------------------ MRT basis */
+/* D3Q19 moment basis of d'Humieres, Ginzburg, Krafczyk, Lallemand & Luo,
+ * Phil. Trans. R. Soc. A 360 (2002) 437: rho, e, eps, jx, qx, jy, qy, jz, qz,
+ * 3pxx, 3pixx, pww, piww, pxy, pyz, pxz, mx, my, mz.  D2Q9 basis of Lallemand &
+ * Luo, Phys. Rev. E 61 (2000) 6546: rho, e, eps, jx, qx, jy, qy, pxx, pxy.  The
+ * reference has no MRT; this is new behaviour. */
+static double mrt_poly(int dim, int r, int cx, int cy, int cz) {
+    double c2 = cx*cx + cy*cy + cz*cz;
+    if (dim == 2) {
+        switch (r) {
+        case 0: return 1;
+        case 1: return -4 + 3*c2;
+        case 2: return 4 - 10.5*c2 + 4.5*c2*c2;
+        case 3: return cx;
+        case 4: return (-5 + 3*c2)*cx;
+        case 5: return cy;
+        case 6: return (-5 + 3*c2)*cy;
+        case 7: return cx*cx - cy*cy;
+        case 8: return cx*cy;
+        }
+        return 0;
+    }
+    switch (r) {
+    case 0: return 1;
+    case 1: return 19*c2 - 30;
+    case 2: return (21*c2*c2 - 53*c2 + 24)/2.0;
+    case 3: return cx;
+    case 4: return (5*c2 - 9)*cx;
+    case 5: return cy;
+    case 6: return (5*c2 - 9)*cy;
+    case 7: return cz;
+    case 8: return (5*c2 - 9)*cz;
+    case 9: return 3*cx*cx - c2;
+    case 10: return (3*c2 - 5)*(3*cx*cx - c2);
+    case 11: return cy*cy - cz*cz;
+    case 12: return (3*c2 - 5)*(cy*cy - cz*cz);
+    case 13: return cx*cy;
+    case 14: return cy*cz;
+    case 15: return cx*cz;
+    case 16: return (cy*cy - cz*cz)*cx;
+    case 17: return (cz*cz - cx*cx)*cy;
+    case 18: return (cx*cx - cy*cy)*cz;
+    }
+    return 0;
+}
+
+/* ---------------------------------------------------------------- helpers */
+static inline long cidx(const orc* o, int x, int y, int z) {
+    return (long)x + (long)o->c.nx * ((long)y + (long)o->c.ny * z);
+}
+/* src/LBM/LBM2D/_evolution.py:205-212 periodic_index (3D: LBM3D/_evolution.py:200-210) */
+static inline int wrap(int v, int n) { return v < 0 ? n - 1 : (v > n - 1 ? 0 : v); }
+static inline long nbr(const orc* o, long c, int k, int sign) {
+    int nx = o->c.nx, ny = o->c.ny;
+    int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((long)nx * ny));
+    x = wrap(x + sign*o->e[k][0], o->c.nx);
+    y = wrap(y + sign*o->e[k][1], o->c.ny);
+    z = wrap(z + sign*o->e[k][2], o->c.nz);
+    return cidx(o, x, y, z);
+}
+static inline int is_solid(const uint8_t* m, long c) { return (m[c] & ORC_SOLID) != 0; }
+
+/* feq9 / feq19: src/LBM/LBM2D/_evolution.py:213-225, eps = 1 - solid = 1 for fluid cells */
+static inline REAL feq(const orc* o, int k, REAL rho, const REAL* u) {
+    REAL eu = (REAL)o->e[k][0]*u[0] + (REAL)o->e[k][1]*u[1] + (REAL)o->e[k][2]*u[2];
+    REAL uv = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
+    REAL eps = (REAL)1.0 + (REAL)1e-12;
+    if (o->c.eos == 1)
+        return o->w[k]*(rho + (REAL)3.0*eu + (REAL)4.5*eu*eu/eps - (REAL)1.5*uv/eps);
+    return o->w[k]*rho*((REAL)1.0 + (REAL)3.0*eu + (REAL)4.5*eu*eu/eps - (REAL)1.5*uv/eps);
+}
+/* TemperatureFluid.geq5 / geq7: src/LBM/LBM2D/_thermal.py:54-61, LBM3D/_thermal.py:54-61 */
+static inline REAL geq_fluid(const orc* o, int k, REAL T, const REAL* u) {
+    REAL eu = (REAL)o->e[k][0]*u[0] + (REAL)o->e[k][1]*u[1] + (REAL)o->e[k][2]*u[2];
+    REAL uv = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
+    return o->wt[k]*T*((REAL)1.0 + o->ta*eu + o->tb*eu*eu - o->tc*uv);
+}
+/* tau: src/LBM/LBM2D/_evolution.py:241-249 (IDEAL_GAS divides viscosity by rho) */
+static inline REAL tau_flow(const orc* o, REAL rho) {
+    REAL nu = (REAL)o->c.nu;
+    if (o->c.eos == 0) nu = nu / rho;
+    return (REAL)3*nu + (REAL)0.5;
+}
+/* forceTermGuo: src/LBM/LBM2D/_evolution.py:284-298 */
+static inline REAL guo(const orc* o, int k, REAL rho, const REAL* u, REAL tau) {
+    REAL Fx = (REAL)o->c.force[0], Fy = (REAL)o->c.force[1], Fz = (REAL)o->c.force[2];
+    if (Fx == 0 && Fy == 0 && Fz == 0) return 0;
+    REAL eps = (REAL)1.0 + (REAL)1e-12;
+    REAL ex = (REAL)o->e[k][0], ey = (REAL)o->e[k][1], ez = (REAL)o->e[k][2];
+    REAL t1 = (ex - u[0]/eps)*Fx + (ey - u[1]/eps)*Fy + (ez - u[2]/eps)*Fz;
+    REAL eu = ex*u[0] + ey*u[1] + ez*u[2];
+    REAL eF = ex*Fx + ey*Fy + ez*Fz;
+    REAL pre = (REAL)1.0 - (REAL)1.0/(REAL)2.0/tau;
+    if (o->c.eos == 1)
+        return pre*o->w[k]*((REAL)3.0*t1 + (REAL)9.0*eu*eF/eps);
+    return pre*rho*o->w[k]*((REAL)3.0*t1 + (REAL)9.0*eu*eF/eps);
+}
+
+/* Post-collision flow populations of a fluid cell (BGK: _evolution.py:33; MRT new). */
+static void collide_flow(const orc* o, const REAL* fin, REAL rho, const REAL* u, REAL* fout) {
+    int Q = o->Q;
+    REAL tau = tau_flow(o, rho);
+    REAL fe[19];
+    for (int k = 0; k < Q; ++k) fe[k] = feq(o, k, rho, u);
+    if (o->c.collision == 0) {
+        for (int k = 0; k < Q; ++k)
+            fout[k] = fin[k] - (REAL)1/tau*(fin[k] - fe[k]) + guo(o, k, rho, u, tau);
+        return;
+    }
+    REAL mneq[19];
+    for (int r = 0; r < Q; ++r) {
+        if (o->cons_row[r]) { mneq[r] = 0; continue; }
+        REAL s = o->visc_row[r] ? (REAL)1/tau : (REAL)o->c.mrt_s[r];
+        REAL acc = 0;
+        for (int k = 0; k < Q; ++k) acc += (REAL)o->M[r][k]*(fin[k] - fe[k]);
+        mneq[r] = s*acc/(REAL)o->Mn[r];
+    }
+    for (int k = 0; k < Q; ++k) {
+        REAL acc = 0;
+        for (int r = 0; r < Q; ++r) if (!o->cons_row[r]) acc += (REAL)o->M[r][k]*mneq[r];
+        fout[k] = fin[k] - acc + guo(o, k, rho, u, tau);
+    }
+}
+
+/* ------------------------------------------------------------- lifecycle */
+orc* orc_create(const orc_cfg* cfg) {
+    orc* o = (orc*)calloc(1, sizeof(orc));
+    o->c = *cfg;
+    if (o->c.dim == 2) o->c.nz = 1;
+    o->N = (long)o->c.nx * o->c.ny * o->c.nz;
+    if (o->c.dim == 2) {
+        o->Q = 9; o->QT = 5;
+        for (int k = 0; k < 9; ++k) { memcpy(o->e[k], E9[k], sizeof(E9[k])); o->opp[k] = OPP9[k]; }
+        o->w[0] = (REAL)(4.0/9.0);
+        for (int k = 1; k < 5; ++k) o->w[k] = (REAL)(1.0/9.0);
+        for (int k = 5; k < 9; ++k) o->w[k] = (REAL)(1.0/36.0);
+        o->wt[0] = (REAL)(1.0/3.0);
+        for (int k = 1; k < 5; ++k) o->wt[k] = (REAL)(1.0/6.0);
+        o->ta = 3.0; o->tb = 4.5; o->tc = 1.5;
+    } else {
+        o->Q = 19; o->QT = 7;
+        for (int k = 0; k < 19; ++k) { memcpy(o->e[k], E19[k], sizeof(E19[k])); o->opp[k] = OPP19[k]; }
+        o->w[0] = (REAL)(1.0/3.0);
+        for (int k = 1; k < 7; ++k) o->w[k] = (REAL)(1.0/18.0);
+        for (int k = 7; k < 19; ++k) o->w[k] = (REAL)(1.0/36.0);
+        o->wt[0] = (REAL)(1.0/4.0);
+        for (int k = 1; k < 7; ++k) o->wt[k] = (REAL)(1.0/8.0);
+        o->ta = 4.0; o->tb = 8.0; o->tc = 2.0;
+    }
+    for (int r = 0; r < o->Q; ++r) {
+        double n2 = 0;
+        for (int k = 0; k < o->Q; ++k) {
+            o->M[r][k] = mrt_poly(o->c.dim, r, o->e[k][0], o->e[k][1], o->e[k][2]);
+            n2 += o->M[r][k]*o->M[r][k];
+        }
+        o->Mn[r] = n2;
+        o->visc_row[r] = o->c.dim == 2 ? (r == 7 || r == 8)
+                                       : (r == 9 || r == 11 || r == 13 || r == 14 || r == 15);
+        o->cons_row[r] = o->c.dim == 2 ? (r == 0 || r == 3 || r == 5)
+                                       : (r == 0 || r == 3 || r == 5 || r == 7);
+    }
+    long N = o->N;
+    o->f = (REAL*)calloc(N*o->Q, sizeof(REAL));
+    o->F = (REAL*)calloc(N*o->Q, sizeof(REAL));
+    o->g = (REAL*)calloc(N*o->QT, sizeof(REAL));
+    o->G = (REAL*)calloc(N*o->QT, sizeof(REAL));
+    o->rho = (REAL*)calloc(N, sizeof(REAL));
+    o->u = (REAL*)calloc(3*N, sizeof(REAL));
+    o->T = (REAL*)calloc(N, sizeof(REAL));
+    o->dS = (REAL*)calloc(N, sizeof(REAL));
+    o->alpha = (REAL*)calloc(N, sizeof(REAL));
+    o->rel = (REAL*)calloc(N, sizeof(REAL));
+    o->mask = (uint8_t*)calloc(N, 1);
+    o->mask_next = (uint8_t*)calloc(N, 1);
+    return o;
+}
+
+void orc_destroy(orc* o) {
+    if (!o) return;
+    free(o->f); free(o->F); free(o->g); free(o->G); free(o->rho); free(o->u); free(o->T);
+    free(o->dS); free(o->alpha); free(o->rel); free(o->mask); free(o->mask_next); free(o);
+}
+
+int orc_Q(const orc* o) { return o->Q; }
+int orc_QT(const orc* o) { return o->QT; }
+double orc_M(const orc* o, int r, int k) { return o->M[r][k]; }
+
+/* init_kernel: f = F = feq(rho,u), g = G = geq(T,u)  (src/LBM/LBM2D/_initialize.py:37-65).
+ * Inputs are planar: u[d*N + c].  mask bit0 = solid, bit2 = reactive. */
+void orc_init(orc* o, const double* rho, const double* u, const double* T,
+              const uint8_t* mask, const double* alpha) {
+    long N = o->N;
+    for (long c = 0; c < N; ++c) {
+        o->mask[c] = mask[c] & (ORC_SOLID | ORC_REACTIVE);
+        o->rho[c] = (REAL)rho[c];
+        for (int d = 0; d < 3; ++d) o->u[c*3 + d] = (REAL)u[d*N + c];
+        o->T[c] = T ? (REAL)T[c] : 0;
+        o->alpha[c] = alpha ? (REAL)alpha[c] : 0;
+        o->dS[c] = 0;
+        o->rel[c] = 0;
+        if (is_solid(o->mask, c)) { o->u[c*3] = o->u[c*3+1] = o->u[c*3+2] = 0; }
+        for (int k = 0; k < o->Q; ++k) {
+            REAL v = is_solid(o->mask, c) ? 0 : feq(o, k, o->rho[c], &o->u[c*3]);
+            o->f[c*o->Q + k] = v;
+            o->F[c*o->Q + k] = v;
+        }
+        for (int k = 0; k < o->QT; ++k) {
+            REAL v = is_solid(o->mask, c) ? o->wt[k]*o->T[c] : geq_fluid(o, k, o->T[c], &o->u[c*3]);
+            o->g[c*o->QT + k] = v;
+            o->G[c*o->QT + k] = v;
+        }
+    }
+}
+
+/* --------------------------------------------------------------- the step */
+
+/* collision_source_streaming: src/LBM/LBM2D/_evolution.py:26-115 */
+static void collide_stream(orc* o) {
+    int Q = o->Q, QT = o->QT;
+    long N = o->N;
+    #pragma omp parallel for schedule(static)
+    for (long c = 0; c < N; ++c) {
+        REAL fo[19], go[7];
+        int solid = is_solid(o->mask, c);
+        if (!solid) {
+            collide_flow(o, &o->f[c*Q], o->rho[c], &o->u[c*3], fo);
+            for (int k = 0; k < Q; ++k) {
+                long ip = nbr(o, c, k, +1);
+                if (!is_solid(o->mask, ip)) o->F[ip*Q + k] = fo[k];      /* :69-70 */
+                else o->F[c*Q + o->opp[k]] = fo[k];                      /* :78-79 halfway bounce-back */
+            }
+        }
+        if (o->c.thermal == 1) {
+            /* conjugate single field: fluid geq advects (TF.geq), solid geq = w T (TS.geq,
+             * LBM2D/_thermal.py:162-166); the source enters as geq(dS) (_evolution.py:54-58) */
+            REAL tauT = solid ? (REAL)o->c.tauT_solid : (REAL)o->c.tauT_fluid;
+            for (int k = 0; k < QT; ++k) {
+                REAL gk = o->g[c*QT + k];
+                REAL ge = solid ? o->wt[k]*o->T[c] : geq_fluid(o, k, o->T[c], &o->u[c*3]);
+                REAL src = o->wt[k]*o->dS[c];
+                go[k] = gk - (REAL)1/tauT*(gk - ge) + src;
+            }
+            for (int k = 0; k < QT; ++k) o->G[nbr(o, c, k, +1)*QT + k] = go[k];
+        }
+    }
+    /* pyrolysis gas release: a reacting solid cell pushes rel*w_k into each fluid
+     * neighbour along e_k (new behaviour; no reference counterpart) */
+    if (o->c.pyro) {
+        #pragma omp parallel for schedule(static)
+        for (long y = 0; y < N; ++y) {
+            if (is_solid(o->mask, y)) continue;
+            for (int k = 1; k < Q; ++k) {
+                long x = nbr(o, y, k, -1);
+                if (is_solid(o->mask, x) && o->rel[x] != 0)
+                    o->F[y*Q + k] += o->rel[x]*o->w[k];
+            }
+        }
+    }
+}
+
+/* macro: src/LBM/LBM2D/_evolution.py:118-202, plus pyrolysis and the cell flip */
+static void macro(orc* o) {
+    int Q = o->Q, QT = o->QT;
+    long N = o->N;
+    #pragma omp parallel for schedule(static)
+    for (long c = 0; c < N; ++c) {
+        o->mask_next[c] = o->mask[c];
+        if (!is_solid(o->mask, c)) {
+            REAL r = 0, j[3] = {0, 0, 0};
+            for (int k = 0; k < Q; ++k) {
+                REAL Fk = o->F[c*Q + k];
+                o->f[c*Q + k] = Fk;
+                r += Fk;
+                for (int d = 0; d < 3; ++d) j[d] += (REAL)o->e[k][d]*Fk;
+            }
+            if (o->c.half_force_velocity)
+                for (int d = 0; d < 3; ++d) j[d] += (REAL)0.5*(REAL)o->c.force[d]*(o->c.eos == 0 ? r : (REAL)1);
+            if (o->c.eos == 0) for (int d = 0; d < 3; ++d) j[d] /= r;
+            o->rho[c] = r;
+            for (int d = 0; d < 3; ++d) o->u[c*3 + d] = j[d];
+        }
+        if (o->c.thermal == 1) {
+            REAL Tc = 0;
+            for (int k = 0; k < QT; ++k) { Tc += o->G[c*QT + k]; o->g[c*QT + k] = o->G[c*QT + k]; }
+            o->T[c] = Tc;
+            o->dS[c] = 0;
+        }
+        o->rel[c] = 0;
+        if (o->c.pyro && is_solid(o->mask, c) && (o->mask[c] & ORC_REACTIVE)) {
+            /* Arrhenius rate, src/LBM/LBM2D/_chemical.py:198-212 with T = T_s */
+            REAL a = o->alpha[c];
+            REAL TK = o->T[c]*(REAL)o->c.T_scale + (REAL)o->c.T_ref;
+            REAL k = 0;
+            if (TK > (REAL)o->c.pyro_Tmin)
+                k = (REAL)o->c.pyro_A*(REAL)pow((double)(TK + (REAL)1e-6), o->c.pyro_b)
+                    *(REAL)exp(-(double)((REAL)o->c.pyro_Ea/(TK + (REAL)1e-6)/(REAL)8.314441));
+            REAL da = k*a*(REAL)o->c.dt_phys;
+            REAL an = a - da;
+            o->alpha[c] = an;
+            o->dS[c] = -(REAL)o->c.heat_norm*da;
+            REAL mg = (REAL)o->c.gas_coef*da;
+            REAL W = 0;
+            for (int q = 1; q < Q; ++q) if (!is_solid(o->mask, nbr(o, c, q, +1))) W += o->w[q];
+            o->rel[c] = W > 0 ? mg/W : 0;
+            if (an < (REAL)o->c.alpha_flip) o->mask_next[c] = o->mask[c] & ~ORC_SOLID;
+        }
+    }
+    /* cell flip: a spent cell turns fluid at the mean rho,u of its fluid neighbours */
+    for (long c = 0; c < N; ++c) {
+        if (!(is_solid(o->mask, c) && !is_solid(o->mask_next, c))) continue;
+        REAL rs = 0, us[3] = {0, 0, 0};
+        int n = 0;
+        for (int q = 1; q < Q; ++q) {
+            long nb = nbr(o, c, q, +1);
+            if (is_solid(o->mask, nb)) continue;
+            rs += o->rho[nb];
+            for (int d = 0; d < 3; ++d) us[d] += o->u[nb*3 + d];
+            ++n;
+        }
+        REAL rb = n ? rs/(REAL)n : (REAL)1;
+        REAL ub[3];
+        for (int d = 0; d < 3; ++d) ub[d] = n ? us[d]/(REAL)n : 0;
+        o->rho[c] = rb;
+        for (int d = 0; d < 3; ++d) o->u[c*3 + d] = ub[d];
+        for (int k = 0; k < Q; ++k) o->f[c*Q + k] = feq(o, k, rb, ub);
+        o->rel[c] = 0;
+    }
+    memcpy(o->mask, o->mask_next, (size_t)N);
+}
+
+/* Non-equilibrium extrapolation on one boundary cell b with inner neighbour i.
+ * Flow: src/LBM/LBM2D/_boundary.py:54-101 (3D: LBM3D/_boundary.py:71-142).
+ * Scalar: src/LBM/LBM2D/_scalarField.py:83-122. */
+static void nee_cell(orc* o, const orc_side* s, long b, long i) {
+    int Q = o->Q, QT = o->QT;
+    REAL* ub = &o->u[b*3];
+    const REAL* ui = &o->u[i*3];
+    if (s->v_type == ORC_BC_FIXED) for (int d = 0; d < 3; ++d) ub[d] = (REAL)s->v[d];
+    else if (s->v_type == ORC_BC_ZEROGRAD) for (int d = 0; d < 3; ++d) ub[d] = ui[d];
+    if (s->rho_type == ORC_BC_FIXED) o->rho[b] = (REAL)s->rho;
+    else if (s->rho_type == ORC_BC_ZEROGRAD) o->rho[b] = o->rho[i];
+    for (int k = 0; k < Q; ++k)
+        o->f[b*Q + k] = feq(o, k, o->rho[b], ub) + (o->f[i*Q + k] - feq(o, k, o->rho[i], ui));
+    if (o->c.thermal == 1) {
+        if (s->T_type == ORC_BC_FIXED) o->T[b] = (REAL)s->T;
+        else if (s->T_type == ORC_BC_ZEROGRAD) o->T[b] = o->T[i];
+        for (int k = 0; k < QT; ++k) {
+            o->G[b*QT + k] = geq_fluid(o, k, o->T[b], ub) + (o->G[i*QT + k] - geq_fluid(o, k, o->T[i], ui));
+            o->g[b*QT + k] = o->G[b*QT + k];
+        }
+    }
+}
+
+/* Boundary_condition_NEE: x sides first (loop over j,k), then y sides (i,k), then z (i,j).
+ * src/LBM/LBM2D/_boundary.py:17-52, LBM3D/_boundary.py:15-68. */
+static void nee(orc* o) {
+    int nx = o->c.nx, ny = o->c.ny, nz = o->c.nz;
+    const orc_side* S = o->c.side;
+    for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) {
+        if (S[0].active) nee_cell(o, &S[0], cidx(o, 0, y, z), cidx(o, 1, y, z));
+        if (S[1].active) nee_cell(o, &S[1], cidx(o, nx-1, y, z), cidx(o, nx-2, y, z));
+    }
+    for (int z = 0; z < nz; ++z) for (int x = 0; x < nx; ++x) {
+        if (S[2].active) nee_cell(o, &S[2], cidx(o, x, 0, z), cidx(o, x, 1, z));
+        if (S[3].active) nee_cell(o, &S[3], cidx(o, x, ny-1, z), cidx(o, x, ny-2, z));
+    }
+    if (o->c.dim == 3)
+        for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
+            if (S[4].active) nee_cell(o, &S[4], cidx(o, x, y, 0), cidx(o, x, y, 1));
+            if (S[5].active) nee_cell(o, &S[5], cidx(o, x, y, nz-1), cidx(o, x, y, nz-2));
+        }
+}
+
+/* step: src/LBM/LBM2D/_evolution.py:12-25 */
+void orc_step(orc* o, int n) {
+    for (int i = 0; i < n; ++i) {
+        collide_stream(o);
+        macro(o);
+        nee(o);
+    }
+}
+
+/* Read back macroscopic fields (planar u) and the current mask / reactive fraction. */
+void orc_get(const orc* o, double* rho, double* u, double* T, uint8_t* mask, double* alpha) {
+    long N = o->N;
+    for (long c = 0; c < N; ++c) {
+        if (rho) rho[c] = o->rho[c];
+        if (u) for (int d = 0; d < 3; ++d) u[d*N + c] = o->u[c*3 + d];
+        if (T) T[c] = o->T[c];
+        if (mask) mask[c] = o->mask[c];
+        if (alpha) alpha[c] = o->alpha[c];
+    }
+}
+
+/* Post-stream distributions (f after macro/NEE), planar: out[k*N + c]. */
+void orc_get_dist(const orc* o, double* f, double* g) {
+    long N = o->N;
+    for (long c = 0; c < N; ++c) {
+        if (f) for (int k = 0; k < o->Q; ++k) f[k*N + c] = o->f[c*o->Q + k];
+        if (g) for (int k = 0; k < o->QT; ++k) g[k*N + c] = o->g[c*o->QT + k];
+    }
+}
+
+/* Diagnostics over the current state (new: the reference only has max|v|, min/max T,
+ * src/LBM/LBM2D/_io.py:565-588).  out: [0] mass (sum rho, fluid), [1] energy (sum T,
+ * all cells), [2] reactive solid fraction sum, [3] max |u| (fluid), [4] min T, [5] max T,
+ * [6] non-finite count, [7] fluid cell count. */
+void orc_diag(const orc* o, double* out) {
+    double mass = 0, en = 0, sm = 0, umax2 = 0, tmin = 1e300, tmax = -1e300, nan = 0, nf = 0;
+    for (long c = 0; c < o->N; ++c) {
+        double T = o->c.thermal ? (double)o->T[c] : 0;
+        if (!isfinite(T)) nan += 1;
+        en += T;
+        if (T < tmin) tmin = T;
+        if (T > tmax) tmax = T;
+        if (is_solid(o->mask, c)) {
+            if (o->mask[c] & ORC_REACTIVE) sm += o->alpha[c];
+            continue;
+        }
+        double r = o->rho[c];
+        if (!isfinite(r)) nan += 1;
+        mass += r;
+        nf += 1;
+        double u2 = 0;
+        for (int d = 0; d < 3; ++d) u2 += (double)o->u[c*3+d]*(double)o->u[c*3+d];
+        if (u2 > umax2) umax2 = u2;
+    }
+    out[0] = mass; out[1] = en; out[2] = sm; out[3] = sqrt(umax2);
+    out[4] = tmin; out[5] = tmax; out[6] = nan; out[7] = nf;
+}
+
+int orc_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+void orc_set_threads(int n) {
+#ifdef _OPENMP
+    if (n > 0) omp_set_num_threads(n);
+#else
+    (void)n;
+#endif
+}

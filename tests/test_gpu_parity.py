@@ -1,0 +1,161 @@
+"""Parity of the CUDA lattice update (called through the C ABI) with the C oracle.
+
+Tolerances (relative L2 over the compared cells):
+  - FP64 storage vs the FP64 oracle: 1e-10 for rho, u, T; the solid mask and
+    the flip steps are identical.  This is the strict algorithmic check.
+  - FP32 storage vs the FP32 oracle: 1e-5 for rho and T; for u, 1e-5 relative
+    to the velocity scale max|u| (the oracle and the kernel round differently,
+    the kernel fuses multiply-adds); flip steps within +-1.
+  - FP16 deviation storage vs the FP64 oracle: 1e-2 for u, 1e-4 for rho and T.
+"""
+import numpy as np
+import pytest
+
+from lbm_porouschem_b200 import workloads
+from lbm_porouschem_b200.config import LatticeConfig
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b, mask=None):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    if mask is not None:
+        a, b = a[..., mask], b[..., mask]
+    den = np.linalg.norm(b)
+    return np.linalg.norm(a - b) / (den if den > 0 else 1.0)
+
+
+def _run_pair(oracle_mod, w, n, real, prec=None):
+    from lbm_porouschem_b200.lattice import Lattice
+    cfg = w.cfg if prec is None else w.cfg.replace(precision=prec)
+    lat = Lattice(cfg)
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    o = oracle_mod.Oracle(cfg, real=real)
+    o.init(w.solid, w.reactive, **w.init)
+    lat.step(n)
+    o.step(n)
+    return lat, o
+
+
+def _compare(lat, o, tol_rho, tol_T, tol_u, u_scale_rel=False):
+    g, r = lat.fields(), o.fields()
+    assert np.array_equal(g["solid"], r["solid"])
+    fl = ~r["solid"]
+    e_rho = _rel(g["rho"], r["rho"], fl)
+    if u_scale_rel:
+        scale = np.abs(r["u"][:, fl]).max()
+        e_u = np.sqrt(np.mean((g["u"][:, fl] - r["u"][:, fl]) ** 2)) / scale
+    else:
+        e_u = _rel(g["u"], r["u"], fl)
+    assert e_rho < tol_rho, e_rho
+    assert e_u < tol_u, e_u
+    if "T" in r:
+        e_T = _rel(g["T"], r["T"])
+        assert e_T < tol_T, e_T
+    return g, r
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_flow2d_fp64(oracle_mod, coll):
+    w = workloads.flow2d(64, 48, seed=1, collision=coll)
+    w.cfg.force = (1e-5, 0.0, 0.0)
+    lat, o = _run_pair(oracle_mod, w, 300, "f64", "fp64")
+    _compare(lat, o, 1e-10, 1e-10, 1e-10)
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_flow2d_fp32(oracle_mod, coll):
+    w = workloads.flow2d(64, 48, seed=1, collision=coll)
+    w.cfg.force = (1e-5, 0.0, 0.0)
+    lat, o = _run_pair(oracle_mod, w, 300, "f32")
+    _compare(lat, o, 1e-5, 1e-5, 1e-5, u_scale_rel=True)
+
+
+def _fast_pyro(w, A=3e10):
+    # hot start, faster rate and a milder heat sink so that cells convert within
+    # a short test (k dt ~ 0.02 per step at T = 1: conversion after ~220 steps)
+    w.cfg.pyro_A = A
+    w.cfg.heat_norm = 0.2
+    w.init["T"] = 1.0
+    return w
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_pyro2d_fp64_with_flips(oracle_mod, coll):
+    w = _fast_pyro(workloads.pyro2d(48, 32, seed=2, collision=coll))
+    lat, o = _run_pair(oracle_mod, w, 400, "f64", "fp64")
+    g, r = _compare(lat, o, 1e-10, 1e-10, 1e-10)
+    assert (w.solid & ~r["solid"]).any(), "the test case should convert some cells"
+    assert np.max(np.abs(g["alpha"] - r["alpha"])[r["solid"]]) < 1e-10
+
+
+def test_pyro2d_fp32(oracle_mod):
+    w = _fast_pyro(workloads.pyro2d(48, 32, seed=2))
+    lat, o = _run_pair(oracle_mod, w, 200, "f32")
+    _compare(lat, o, 1e-5, 1e-5, 1e-4, u_scale_rel=True)
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_pyro3d_fp64(oracle_mod, coll):
+    w = _fast_pyro(workloads.pyro3d(20, seed=3, collision=coll, ny=16, nz=12), A=8e10)
+    lat, o = _run_pair(oracle_mod, w, 120, "f64", "fp64")
+    g, r = _compare(lat, o, 1e-10, 1e-10, 1e-10)
+
+
+def test_pyro3d_fp32(oracle_mod):
+    w = _fast_pyro(workloads.pyro3d(20, seed=3, ny=16, nz=12), A=8e10)
+    lat, o = _run_pair(oracle_mod, w, 120, "f32")
+    _compare(lat, o, 1e-5, 1e-5, 1e-4, u_scale_rel=True)
+
+
+def test_pyro3d_fp16_vs_fp64_oracle(oracle_mod):
+    w = workloads.pyro3d(20, seed=3, ny=16, nz=12)
+    w.cfg.pyro_A = 5e10
+    lat, o = _run_pair(oracle_mod, w, 120, "f64", "fp16")
+    _compare(lat, o, 1e-4, 1e-3, 5e-2, u_scale_rel=True)
+
+
+def test_diagnostics_match_oracle(oracle_mod):
+    w = _fast_pyro(workloads.pyro2d(48, 32, seed=4))
+    lat, o = _run_pair(oracle_mod, w, 150, "f64", "fp64")
+    d, r = lat.diagnostics(), o.diag()
+    for k in ("mass", "energy", "solid_alpha", "umax", "Tmin", "Tmax", "nfluid"):
+        assert abs(d[k] - r[k]) <= 1e-9 * max(1.0, abs(r[k])), (k, d[k], r[k])
+    assert d["nonfinite"] == 0
+
+
+def test_fused_diag_equals_peek(oracle_mod):
+    w = _fast_pyro(workloads.pyro2d(48, 32, seed=5))
+    from lbm_porouschem_b200.lattice import Lattice
+    lat = Lattice(w.cfg.replace(precision="fp64"))
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    lat.step(60, diag=True)
+    fused = lat.read_diag()
+    peek = lat.diagnostics()
+    for k in ("mass", "energy", "solid_alpha", "umax", "nfluid"):
+        assert fused[k] == pytest.approx(peek[k], rel=1e-12, abs=1e-14), k
+
+
+def test_flip_steps_within_one(oracle_mod):
+    w = _fast_pyro(workloads.pyro2d(40, 24, seed=6))
+    from lbm_porouschem_b200.lattice import Lattice
+    lat = Lattice(w.cfg)
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    o = oracle_mod.Oracle(w.cfg, real="f32")
+    o.init(w.solid, w.reactive, **w.init)
+    fg = np.full(w.solid.shape, -1)
+    fo = np.full(w.solid.shape, -1)
+    for n in range(1, 301):
+        lat.step(1)
+        o.step(1)
+        sg = lat.fields()["solid"][..., 0]
+        so = o.fields()["solid"][..., 0]
+        fg[(fg < 0) & w.solid & ~sg] = n
+        fo[(fo < 0) & w.solid & ~so] = n
+    conv = fo > 0
+    assert conv.any()
+    assert np.all(np.abs(fg[conv] - fo[conv]) <= 1)
+    assert np.array_equal(fg > 0, conv)
