@@ -122,8 +122,8 @@ typedef struct lbm_diag {
 #define LBM_FIELD_F 0       /* flow populations, 2 x Q planes (A/B), storage precision */
 #define LBM_FIELD_G 1       /* temperature populations, 2 x QT planes */
 #define LBM_FIELD_MASK 2    /* uint8 per cell */
-#define LBM_FIELD_ALPHA 3   /* float32 reactive fraction per cell */
-#define LBM_FIELD_REL 4     /* float32 gas release per cell, 2 planes */
+#define LBM_FIELD_ALPHA 3   /* reactive fraction per cell (compute precision) */
+#define LBM_FIELD_REL 4     /* gas release per cell, 2 planes (compute precision) */
 #define LBM_FIELD_RHO 5     /* macro outputs: rho (compute precision) */
 #define LBM_FIELD_U 6       /* 3 planes */
 #define LBM_FIELD_T 7
@@ -161,8 +161,8 @@ LBM_API int32_t lbm_bind(lbm_handle* h, int32_t field, void* dev_ptr, size_t byt
 LBM_API int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stream);
 
 /* Equilibrium initialisation from device planes rho[N], u[3N], T[N] (T may be
- * NULL without thermal), alpha[N] (may be NULL without pyrolysis), all
- * float32.  The solid mask must be bound first.  Replaces init_simulation /
+ * NULL without thermal), alpha[N] (NULL: 1 on reactive cells), all float32.
+ * Compute precision is float32 for FP32/FP16 storage and float64 for FP64.  The solid mask must be bound first.  Replaces init_simulation /
  * init_kernel (src/LBM/LBM2D/_initialize.py:16-65, LBM3D/_initialize.py:17-77).
  * Resets the step counter. */
 LBM_API int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,

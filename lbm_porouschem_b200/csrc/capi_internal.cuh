@@ -5,6 +5,7 @@
 
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 
@@ -60,7 +61,13 @@ inline Launch plan(const lbm_desc& d, int tx) {
   return L;
 }
 
+// Threads per block along x for the bulk kernel.  LBM_BLOCK_X (32..256, a
+// multiple of 32) overrides the default for launch-shape sweeps.
 inline int default_tx(const lbm_desc& d) {
+  if (const char* e = getenv("LBM_BLOCK_X")) {
+    const int v = atoi(e);
+    if (v >= 32 && v <= 256 && v % 32 == 0) return v;
+  }
   if (d.dim == 2) return d.nx >= 64 ? 64 : 32;
   return d.nx >= 128 ? 128 : (d.nx >= 64 ? 64 : 32);
 }
@@ -81,14 +88,28 @@ struct lbm_handle {
 namespace lbm {
 namespace capi {
 
+// Scratch layout: partials [kNumDiag][rows] | stage-1 sums [kNumDiag][kStage1Blocks] |
+// final [kNumDiag] | (256-byte aligned) device copy of the 6 side records.
+inline int partial_rows(const Launch& L) { return L.bulk_blocks + L.bc_blocks; }
+inline size_t scratch_diag_doubles(const Launch& L) {
+  return (size_t)kNumDiag * (partial_rows(L) + kStage1Blocks + 1);
+}
+inline size_t scratch_bytes(const Launch& L) {
+  return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes;
+}
 inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
+inline double* scratch_stage1(lbm_handle* h) {
+  return scratch_partials(h) + (size_t)kNumDiag * partial_rows(h->L);
+}
+inline double* scratch_final(lbm_handle* h) { return scratch_stage1(h) + (size_t)kNumDiag * kStage1Blocks; }
 inline lbm_side_desc* scratch_sides(lbm_handle* h) {
-  const size_t rows = (size_t)(h->L.bulk_blocks + h->L.bc_blocks + 1) * kNumDiag * sizeof(double);
-  const size_t off = (rows + 255) / 256 * 256;
+  const size_t off = (scratch_diag_doubles(h->L) * sizeof(double) + 255) / 256 * 256;
   return (lbm_side_desc*)((char*)h->ptr[LBM_FIELD_SCRATCH] + off);
 }
-inline double* scratch_final(lbm_handle* h) {
-  return scratch_partials(h) + (size_t)(h->L.bulk_blocks + h->L.bc_blocks) * kNumDiag;
+// Two-stage deterministic reduction of the block partials into scratch_final().
+inline void launch_reduce(lbm_handle* h, cudaStream_t st) {
+  reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), partial_rows(h->L), scratch_stage1(h));
+  reduce_diag_stage2<<<1, 256, 0, st>>>(scratch_stage1(h), kStage1Blocks, scratch_final(h));
 }
 
 template <class S>
@@ -104,8 +125,8 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.fB = f + (size_t)(buf ^ 1) * Q * h->N;
   if (g) { p.gA = g + (size_t)buf * QT * h->N; p.gB = g + (size_t)(buf ^ 1) * QT * h->N; }
   p.mask = (uint8_t*)h->ptr[LBM_FIELD_MASK];
-  p.alpha = (float*)h->ptr[LBM_FIELD_ALPHA];
-  float* rel = (float*)h->ptr[LBM_FIELD_REL];
+  p.alpha = (C*)h->ptr[LBM_FIELD_ALPHA];
+  C* rel = (C*)h->ptr[LBM_FIELD_REL];
   if (rel) { p.relA = rel + (size_t)buf * h->N; p.relB = rel + (size_t)(buf ^ 1) * h->N; }
   p.par = buf;
   p.eos = d.eos;
@@ -133,6 +154,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;
   p.flags = 0;
   p.partials = h->ptr[LBM_FIELD_SCRATCH] ? scratch_partials(h) : nullptr;
+  p.partial_rows = partial_rows(h->L);
   p.block_offset = 0;
   p.rho_out = (C*)h->ptr[LBM_FIELD_RHO];
   p.u_out = (C*)h->ptr[LBM_FIELD_U];

@@ -134,4 +134,37 @@ __host__ __device__ constexpr double mrt_norm(int r) {
   return s;
 }
 
+// Opposite-direction pairs: pair p = (pk(p), opp(pk(p))) with pk(p) < opp(pk(p)).
+// Symmetric and antisymmetric combinations of a pair carry the even and odd
+// moments separately, which halves the equilibrium and MRT arithmetic.
+template <class L>
+__host__ __device__ constexpr int num_pairs() { return (L::Q - 1) / 2; }
+template <class L>
+__host__ __device__ constexpr int pk(int p) {
+  int n = 0;
+  for (int k = 1; k < L::Q; ++k)
+    if (k < L::opp(k)) {
+      if (n == p) return k;
+      ++n;
+    }
+  return -1;
+}
+template <class L, int QQ>
+__host__ __device__ constexpr int pkt(int p) {  // same for the thermal lattice (first QQ directions)
+  int n = 0;
+  for (int k = 1; k < QQ; ++k)
+    if (k < L::opp(k)) {
+      if (n == p) return k;
+      ++n;
+    }
+  return -1;
+}
+// True if MRT row r is even under velocity reversal (M[r][opp k] == M[r][k]).
+template <class L>
+__host__ __device__ constexpr bool mrt_even(int r) {
+  for (int k = 0; k < L::Q; ++k)
+    if (L::mrt(r, L::opp(k)) != L::mrt(r, k)) return false;
+  return true;
+}
+
 }  // namespace lbm

@@ -73,15 +73,15 @@ int32_t lbm_required_bytes(const lbm_desc* d, int32_t field, size_t* bytes) {
     case LBM_FIELD_F: *bytes = 2 * (size_t)lat_q(d->dim) * N * s; break;
     case LBM_FIELD_G: *bytes = d->thermal ? 2 * (size_t)lat_qt(d->dim) * N * s : 0; break;
     case LBM_FIELD_MASK: *bytes = N; break;
-    case LBM_FIELD_ALPHA: *bytes = d->pyro ? N * 4 : 0; break;
-    case LBM_FIELD_REL: *bytes = d->pyro ? 2 * N * 4 : 0; break;
+    case LBM_FIELD_ALPHA: *bytes = d->pyro ? N * cb : 0; break;
+    case LBM_FIELD_REL: *bytes = d->pyro ? 2 * N * cb : 0; break;
     case LBM_FIELD_RHO: *bytes = N * cb; break;
     case LBM_FIELD_U: *bytes = 3 * N * cb; break;
     case LBM_FIELD_T: *bytes = d->thermal ? N * cb : 0; break;
     case LBM_FIELD_UPREV: *bytes = 3 * N * 4; break;
     case LBM_FIELD_SCRATCH: {
       const Launch L = plan(*d, default_tx(*d));
-      *bytes = (size_t)(L.bulk_blocks + L.bc_blocks + 1) * kNumDiag * sizeof(double) + kCtrlBytes + 256;
+      *bytes = scratch_bytes(L);
       break;
     }
     default: return fail(LBM_ERR_ARG, "unknown field id");
@@ -115,6 +115,7 @@ int32_t lbm_bind(lbm_handle* h, int32_t field, void* ptr, size_t bytes) {
   size_t need = 0;
   int rc = lbm_required_bytes(&h->d, field, &need);
   if (rc) return rc;
+  if (field == LBM_FIELD_SCRATCH) need = scratch_bytes(h->L);  // the handle's own launch plan
   if (bytes < need)
     return fail(LBM_ERR_ARG, "buffer for field " + std::to_string(field) + " too small: " +
                                  std::to_string(bytes) + " < " + std::to_string(need));
@@ -182,7 +183,8 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
   rc = with_types(h, [&](auto lat, auto s) -> int {
     using Lt = decltype(lat);
     using S = decltype(s);
-    StepParams<S> p = make_params<S>(h, 0);
+    // buf = 1 makes fB/gB/relB the buffers that the first step (parity 0) reads
+    StepParams<S> p = make_params<S>(h, 1);
     return dispatch_init<Lt, S>(h, p, rho, u, T, alpha, solid_bit, st);
   });
   if (rc) return rc;
@@ -215,8 +217,7 @@ int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream) {
     });
     if (rc) return rc;
     if (fl) {
-      finalize_diag<<<1, 1024, 0, st>>>(scratch_partials(h), h->L.bulk_blocks + h->L.bc_blocks,
-                                       scratch_final(h));
+      launch_reduce(h, st);
       h->diag_valid = true;
     }
     h->step += 1;
@@ -247,7 +248,7 @@ int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream) {
     return dispatch_step<Lt, S>(h, p, st);
   });
   if (rc) return rc;
-  finalize_diag<<<1, 1024, 0, st>>>(scratch_partials(h), h->L.bulk_blocks + h->L.bc_blocks, scratch_final(h));
+  launch_reduce(h, st);
   h->diag_valid = true;
   LBM_CUDA_TRY(cudaGetLastError());
   return LBM_OK;

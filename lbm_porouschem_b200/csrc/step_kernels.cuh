@@ -16,8 +16,8 @@
 //   f[buf][k][c]   storage type S (float / __half shifted / double), buf = A|B
 //   g[buf][k][c]   temperature populations
 //   mask[c]        uint8: bit0/bit1 solid at even/odd parity, bit2 reactive
-//   alpha[c]       float32 reactive fraction (solid cells only, updated in place)
-//   rel[buf][c]    float32 gas release per unit lattice weight (reacting solids)
+//   alpha[c]       reactive fraction (compute precision; solid cells only, in place)
+//   rel[buf][c]    gas release per unit lattice weight (reacting solids)
 // Solid cells carry no flow populations: a fluid cell pulling from a solid
 // neighbour bounces its own opposite population instead, so the f planes of
 // solid cells are neither read nor written (except when a cell flips).
@@ -69,9 +69,9 @@ struct StepParams {
   const S* gA;
   S* gB;
   uint8_t* mask;
-  float* alpha;
-  const float* relA;
-  float* relB;
+  C* alpha;        // reactive fraction (compute precision), updated in place
+  const C* relA;   // gas release per unit lattice weight, read plane
+  C* relB;         //   and write plane
   int par;  // step parity: mask bit read this pass
   int eos;
   int half_force;
@@ -84,7 +84,8 @@ struct StepParams {
   int active;  // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;   // LBM_STEP_*
-  double* partials;
+  double* partials;    // SoA: partials[i * partial_rows + block]
+  int partial_rows;
   int block_offset;
   C* rho_out;
   C* u_out;
@@ -312,7 +313,7 @@ struct DiagAcc {
 };
 
 // Block reduction with warp shuffles (FP64), one partial row per block.
-__device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row) {
+__device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row, size_t stride) {
   __shared__ double sh[32][kNumDiag];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
@@ -336,7 +337,7 @@ __device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row) 
         const double w = __shfl_xor_sync(0xffffffffu, v, o);
         v = (i == 3 || i == 5) ? fmax(v, w) : (i == 4 ? fmin(v, w) : v + w);
       }
-      if (lane == 0) out_row[i] = v;
+      if (lane == 0) out_row[(size_t)i * stride] = v;
     }
   }
 }
@@ -346,7 +347,7 @@ __device__ __forceinline__ void diag_cell(const StepParams<S>& p, DiagAcc& a, in
                                           bool reactive_solid, typename Store<S>::C rho,
                                           typename Store<S>::C ux, typename Store<S>::C uy,
                                           typename Store<S>::C uz, typename Store<S>::C T, bool thermal,
-                                          float alpha) {
+                                          typename Store<S>::C alpha) {
   using C = typename Store<S>::C;
   if (thermal) {
     a.v[1] += (double)T;
@@ -446,7 +447,7 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
       C rho, ux, uy, uz;
       K::template pull_flow<PYRO>(p, nb, c, F);
       K::moments(p, F, rho, ux, uy, uz);
-      if (diag) diag_cell<L, S>(p, acc, c, true, false, rho, ux, uy, uz, T, THERMAL, 0.f);
+      if (diag) diag_cell<L, S>(p, acc, c, true, false, rho, ux, uy, uz, T, THERMAL, (C)0);
       if (!peek) {
         K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
         K::store_flow(p, c, F);
@@ -457,7 +458,7 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
       }
     } else {
       C ux = 0, uy = 0, uz = 0;
-      float an = 0.f;
+      C an = 0;
       const bool reactive = PYRO && (mk & LBM_MASK_REACTIVE);
       if constexpr (PYRO) {
         if (reactive && peek) {
@@ -468,7 +469,7 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
             solid_next = false;
             C rb;
             neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
-            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, 0.f);
+            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, (C)0);
           }
         } else if (reactive) {
           // Arrhenius rate at the solid temperature, src/LBM/LBM2D/_chemical.py:198-212
@@ -482,7 +483,7 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
           }
           const C da = kr * a * p.dtp;
           const C anC = a - da;
-          an = (float)anC;
+          an = anC;
           p.alpha[c] = an;
           dS = -p.heat_norm * da;
           const C mg = p.gas_coef * da;
@@ -504,12 +505,12 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
               constexpr int k = decltype(kk)::value;
               F[k] = K::template feq<k>(p, rb, ux, uy, uz, usq);
             });
-            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, 0.f);
+            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, (C)0);
             K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
             K::store_flow(p, c, F);
-            p.relB[c] = 0.f;
+            p.relB[c] = (C)0;
           } else {
-            p.relB[c] = W > (C)0 ? (float)(mg / W) : 0.f;
+            p.relB[c] = W > (C)0 ? mg / W : (C)0;
           }
         }
       }
@@ -530,7 +531,7 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
   }
   if (diag) {
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
-    block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk) * kNumDiag);
+    block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk), (size_t)p.partial_rows);
   }
 }
 
@@ -644,7 +645,7 @@ __global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4
     const int c = x + p.nx * (y + p.ny * z);
     MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z);
     if (diag) {
-      diag_cell<L, S>(p, acc, c, true, false, s.rho, s.ux, s.uy, s.uz, s.T, THERMAL, 0.f);
+      diag_cell<L, S>(p, acc, c, true, false, s.rho, s.ux, s.uy, s.uz, s.T, THERMAL, (C)0);
     }
     if (!(p.flags & kStepPeek)) {
       K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4
   }
   if (diag) {
     const int blk = blockIdx.x + gridDim.x * blockIdx.y;
-    block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk) * kNumDiag);
+    block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk), (size_t)p.partial_rows);
   }
 }
 
@@ -707,34 +708,59 @@ __global__ void init_equilibrium_kernel(StepParams<S> p, const float* rho_in, co
     K::store_thermal(p, (int)c, G);
   }
   if constexpr (PYRO) {
-    p.alpha[c] = alpha_in ? alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? 1.f : 0.f);
-    p.relB[c] = 0.f;
-    const_cast<float*>(p.relA)[c] = 0.f;
+    p.alpha[c] = alpha_in ? (C)alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? (C)1 : (C)0);
+    p.relB[c] = (C)0;
+    const_cast<C*>(p.relA)[c] = (C)0;
   }
 }
 
-// Deterministic final reduction of the block partials (fixed order).
-static __global__ void __launch_bounds__(1024) finalize_diag(const double* partials, int nrows, double* out) {
-  __shared__ double sh[1024];
+constexpr int kStage1Blocks = 256;  // first-level partial sums of the diagnostics
+
+__device__ __forceinline__ double diag_identity(int i) {
+  return i == 4 ? 1e300 : ((i == 3 || i == 5) ? -1e300 : 0.0);
+}
+__device__ __forceinline__ double diag_combine(int i, double a, double b) {
+  return (i == 3 || i == 5) ? fmax(a, b) : (i == 4 ? fmin(a, b) : a + b);
+}
+
+// Fixed-shape shared-memory tree over 256 threads; returns the total in thread 0.
+__device__ __forceinline__ double block_tree_256(int i, double v, double* sh) {
+  sh[threadIdx.x] = v;
+  __syncthreads();
+  for (int s = 128; s > 0; s >>= 1) {
+    if ((int)threadIdx.x < s) sh[threadIdx.x] = diag_combine(i, sh[threadIdx.x], sh[threadIdx.x + s]);
+    __syncthreads();
+  }
+  const double r = sh[0];
+  __syncthreads();
+  return r;
+}
+
+// Stage 1: block b reduces a contiguous chunk of the per-block partial rows
+// (SoA layout partials[i * nrows + row]).  Fixed partition and tree: the
+// result does not depend on scheduling.  Launch: kStage1Blocks x 256.
+static __global__ void __launch_bounds__(256) reduce_diag_stage1(const double* partials, int nrows,
+                                                                 double* stage1) {
+  __shared__ double sh[256];
+  const int chunk = (nrows + gridDim.x - 1) / gridDim.x;
+  const int r0 = blockIdx.x * chunk, r1 = min(nrows, r0 + chunk);
   for (int i = 0; i < kNumDiag; ++i) {
-    const bool isMax = (i == 3 || i == 5), isMin = (i == 4);
-    double v = isMin ? 1e300 : (isMax ? -1e300 : 0.0);
-    for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
-      const double w = partials[(size_t)r * kNumDiag + i];
-      v = isMax ? fmax(v, w) : (isMin ? fmin(v, w) : v + w);
-    }
-    sh[threadIdx.x] = v;
-    __syncthreads();
-    for (int s = blockDim.x / 2; s > 0; s >>= 1) {
-      if ((int)threadIdx.x < s) {
-        const double w = sh[threadIdx.x + s];
-        double& a = sh[threadIdx.x];
-        a = isMax ? fmax(a, w) : (isMin ? fmin(a, w) : a + w);
-      }
-      __syncthreads();
-    }
-    if (threadIdx.x == 0) out[i] = (i == 3) ? sqrt(sh[0]) : sh[0];
-    __syncthreads();
+    double v = diag_identity(i);
+    for (int r = r0 + threadIdx.x; r < r1; r += blockDim.x)
+      v = diag_combine(i, v, partials[(size_t)i * nrows + r]);
+    v = block_tree_256(i, v, sh);
+    if (threadIdx.x == 0) stage1[i * gridDim.x + blockIdx.x] = v;
+  }
+}
+
+// Stage 2: one block of 256 threads reduces the stage-1 sums into out[kNumDiag].
+static __global__ void __launch_bounds__(256) reduce_diag_stage2(const double* stage1, int n, double* out) {
+  __shared__ double sh[256];
+  for (int i = 0; i < kNumDiag; ++i) {
+    double v = diag_identity(i);
+    for (int r = threadIdx.x; r < n; r += blockDim.x) v = diag_combine(i, v, stage1[i * n + r]);
+    v = block_tree_256(i, v, sh);
+    if (threadIdx.x == 0) out[i] = (i == 3) ? sqrt(v) : v;
   }
 }
 

@@ -190,7 +190,7 @@ class Lattice:
         if cfg.thermal != "none":
             out["T"] = from_flat(self._view(N.LBM_FIELD_T, cd).cpu().numpy(), cfg.shape)
         if cfg.pyro:
-            out["alpha"] = from_flat(self._view(N.LBM_FIELD_ALPHA, torch.float32).cpu().numpy(), cfg.shape)
+            out["alpha"] = from_flat(self._view(N.LBM_FIELD_ALPHA, cd).cpu().numpy(), cfg.shape)
         par = self.nsteps & 1
         m = self.mask.cpu().numpy()
         out["solid"] = from_flat(((m >> par) & 1).astype(bool), cfg.shape)

@@ -97,5 +97,6 @@ def algorithmic_bytes_per_step(cfg: LatticeConfig, solid: np.ndarray) -> int:
     if cfg.thermal != "none":
         b += n * 2 * cfg.QT * s
     if cfg.pyro:
-        b += nsolid * (4 + 4 + 4 + 4)
+        cb = 8 if cfg.precision == "fp64" else 4
+        b += nsolid * 4 * cb   # alpha read + write, release write, release read by neighbours
     return b
