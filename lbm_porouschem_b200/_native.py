@@ -92,7 +92,7 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     global _lib
     if _lib is not None:
         return _lib
-    p = Path(path) if path else LIB_PATH
+    p = Path(path or os.environ.get("LBM_LIBRARY") or LIB_PATH)
     if not p.exists():
         raise RuntimeError(
             f"{p} not found: build it with `python -m lbm_porouschem_b200._build` "

@@ -38,6 +38,7 @@ struct Launch {
   int bc_threads;
   dim3 bc_grid;
   int bulk_blocks, bc_blocks;
+  int flip_blocks;    // grid of flip_cells (pyrolysis only), 256 threads each
 };
 
 inline Launch plan(const lbm_desc& d, int tx) {
@@ -58,6 +59,7 @@ inline Launch plan(const lbm_desc& d, int tx) {
   L.bc_threads = 128;
   L.bc_grid = dim3((maxcells + L.bc_threads - 1) / L.bc_threads, L.nfaces > 0 ? L.nfaces : 1, 1);
   L.bc_blocks = L.nfaces > 0 ? (int)(L.bc_grid.x * L.bc_grid.y) : 0;
+  L.flip_blocks = d.pyro ? 2 * 148 : 0;
   return L;
 }
 
@@ -90,7 +92,7 @@ namespace capi {
 
 // Scratch layout: partials [kNumDiag][rows] | stage-1 sums [kNumDiag][kStage1Blocks] |
 // final [kNumDiag] | (256-byte aligned) device copy of the 6 side records.
-inline int partial_rows(const Launch& L) { return L.bulk_blocks + L.bc_blocks; }
+inline int partial_rows(const Launch& L) { return L.bulk_blocks + L.bc_blocks + L.flip_blocks; }
 inline size_t scratch_diag_doubles(const Launch& L) {
   return (size_t)kNumDiag * (partial_rows(L) + kStage1Blocks + 1);
 }
@@ -146,7 +148,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.itauT_f = d.thermal ? (C)1 / (C)d.tauT_fluid : (C)0;
   p.itauT_s = d.thermal ? (C)1 / (C)d.tauT_solid : (C)0;
   p.rho0 = (C)d.rho0; p.T0 = (C)d.T0;
-  p.pyA = (C)d.pyro_A; p.pyb = (C)d.pyro_b; p.pyEa = (C)d.pyro_Ea; p.pyTmin = (C)d.pyro_Tmin;
+  p.pyA = (C)d.pyro_A; p.pyb = (C)d.pyro_b; p.pyEaR = (C)(d.pyro_Ea / kGasConstant); p.pyTmin = (C)d.pyro_Tmin;
   p.Tref = (C)d.T_ref; p.Tscale = (C)d.T_scale; p.dtp = (C)d.dt_phys;
   p.heat_norm = (C)d.heat_norm; p.gas_coef = (C)d.gas_coef; p.alpha_flip = (C)d.alpha_flip;
   p.active = 0;

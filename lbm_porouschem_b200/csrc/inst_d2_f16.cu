@@ -15,6 +15,11 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
     const int2 f2 = make_int2(L.faces[4], L.faces[5]);
     step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, st>>>(p, f01, f2);
   }
+  if constexpr (THERM == 2) {
+    // after the boundary kernel: it moves mirrored populations of boundary cells too
+    p.block_offset = L.bulk_blocks + L.bc_blocks;
+    flip_cells<Lt, S, COLL, THERM><<<L.flip_blocks, 256, 0, st>>>(p);
+  }
 }
 
 template <class Lt, class S>

@@ -3,24 +3,28 @@
 // One pass of step_bulk<> does, per cell, what the reference does in three
 // separate Taichi loops (src/LBM/LBM2D/_evolution.py:16-25):
 //   stream (pull form of the push at :67-95, halfway bounce-back at :78-86)
-//   -> macro (:118-202: rho, u, T, sources, pyrolysis, flip)
-//   -> collision of the NEXT step (:26-66: BGK toward feq, Guo force, thermal
-//      BGK with the geq(dS) source).
+//   -> macro (:118-202: rho, u, T, sources, pyrolysis)
+//   -> collision of the NEXT step (:26-66: BGK/MRT toward feq, Guo force,
+//      thermal BGK with the geq(dS) source).
 // Reading post-collision populations of step n and writing those of step n+1
-// keeps one read and one write per population per step, the minimum for an
-// A/B double buffer.  Cells on active (non-periodic) domain sides are skipped
-// here and finished by step_boundary<>, which re-derives the non-equilibrium
-// extrapolation (src/LBM/LBM2D/_boundary.py:17-101) from the same input buffer.
+// keeps one read and one write per population per step.  Cells on active
+// (non-periodic) domain sides are finished by step_boundary<>, which re-derives
+// the non-equilibrium extrapolation (src/LBM/LBM2D/_boundary.py:17-101) from
+// the same input buffer; cells that turn fluid are finished by flip_cells<>.
 //
 // Layout in HBM (structure of arrays, x fastest, c = x + nx*(y + ny*z)):
 //   f[buf][k][c]   storage type S (float / __half shifted / double), buf = A|B
 //   g[buf][k][c]   temperature populations
 //   mask[c]        uint8: bit0/bit1 solid at even/odd parity, bit2 reactive
-//   alpha[c]       reactive fraction (compute precision; solid cells only, in place)
-//   rel[buf][c]    gas release per unit lattice weight (reacting solids)
-// Solid cells carry no flow populations: a fluid cell pulling from a solid
-// neighbour bounces its own opposite population instead, so the f planes of
-// solid cells are neither read nor written (except when a cell flips).
+//   alpha[c]       reactive fraction (compute precision; solid cells, in place)
+//   rel[buf][c]    gas release per unit lattice weight (reacting solid cells)
+//
+// Bounce-back by mirror stores.  Solid cells carry no flow populations.  When
+// fluid cell c collides and its neighbour c+e_k is solid, the outgoing
+// population f*_k(c) is stored in the solid neighbour's slot f[opp k][c+e_k]:
+// that is exactly the slot cell c pulls direction opp(k) from on the next
+// step, so every pull is an unconditional load f[k][c-e_k] and the halfway
+// bounce-back needs no mask test before the loads are issued.
 #pragma once
 #include <cuda_fp16.h>
 #include <math.h>
@@ -55,9 +59,9 @@ template <> struct Store<__half> {
   }
 };
 
-constexpr int kNumDiag = 10;  // partial slots per block (order of lbm_diag fields)
-constexpr int kStepPeek = 1 << 8;  // internal flag: recompute outputs, leave the state untouched
-constexpr double kGasConstant = 8.314441;  // src/LBM/util/constant.py:17
+constexpr int kNumDiag = 10;              // partial slots per block (order of lbm_diag fields)
+constexpr int kStepPeek = 1 << 8;         // internal flag: recompute outputs, leave the state untouched
+constexpr double kGasConstant = 8.314441; // src/LBM/util/constant.py:17
 
 template <class S>
 struct StepParams {
@@ -72,18 +76,18 @@ struct StepParams {
   C* alpha;        // reactive fraction (compute precision), updated in place
   const C* relA;   // gas release per unit lattice weight, read plane
   C* relB;         //   and write plane
-  int par;  // step parity: mask bit read this pass
+  int par;         // step parity: mask bit read this pass
   int eos;
   int half_force;
   int has_force;
   C nu, Fx, Fy, Fz;
-  C mrt_sn[19];  // s_r / |M_r|^2 for non-viscous, non-conserved rows
+  C mrt_sn[19];    // s_r / |M_r|^2 for non-viscous, non-conserved rows
   C itauT_f, itauT_s;
   C rho0, T0;
-  C pyA, pyb, pyEa, pyTmin, Tref, Tscale, dtp, heat_norm, gas_coef, alpha_flip;
-  int active;  // bit s: side s uses NEE
+  C pyA, pyb, pyEaR, pyTmin, Tref, Tscale, dtp, heat_norm, gas_coef, alpha_flip;  // pyEaR = Ea/R
+  int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
-  int flags;   // LBM_STEP_*
+  int flags;       // LBM_STEP_* | kStepPeek
   double* partials;    // SoA: partials[i * partial_rows + block]
   int partial_rows;
   int block_offset;
@@ -108,7 +112,7 @@ __device__ __forceinline__ typename Store<S>::C gshift(const StepParams<S>& p) {
 __device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? n - 1 : (v > n - 1 ? 0 : v); }
 
 // Indices of the 3x3x3 neighbourhood of (x,y,z) with the reference's periodic
-// wrap (src/LBM/LBM2D/_evolution.py:205-212): xs[d+1], ys[d+1]*nx, zs[d+1]*nx*ny.
+// wrap (src/LBM/LBM2D/_evolution.py:205-212).
 struct Nbhd {
   int xs[3], ro[3], po[3];
   __device__ __forceinline__ Nbhd(int x, int y, int z, int nx, int ny, int nz) {
@@ -117,7 +121,6 @@ struct Nbhd {
     const int pl = nx * ny;
     po[0] = wrapi(z - 1, nz) * pl; po[1] = z * pl; po[2] = wrapi(z + 1, nz) * pl;
   }
-  // cell at offset (dx,dy,dz) in {-1,0,1}^3
   __device__ __forceinline__ int at(int dx, int dy, int dz) const {
     return xs[dx + 1] + ro[dy + 1] + po[dz + 1];
   }
@@ -128,30 +131,39 @@ template <class C> __device__ __forceinline__ bool finite_(C v) { return isfinit
 template <class L, class S>
 struct Kern {
   using C = typename Store<S>::C;
-  static constexpr int Q = L::Q, QT = L::QT;
   using P = StepParams<S>;
+  static constexpr int Q = L::Q, QT = L::QT, NP = num_pairs<L>();
 
-  __device__ __forceinline__ static bool solid_at(const P& p, int c) {
-    return (p.mask[c] >> p.par) & 1;
+  __device__ __forceinline__ static bool solid_bit(const P& p, int c, int bit) {
+    return (p.mask[c] >> bit) & 1;
   }
 
-  // Post-stream flow populations of fluid cell c (pull form of the reference push).
+  // bit k (1..Q-1) set if the neighbour c + e_k is solid at mask parity `bit`.
+  __device__ __forceinline__ static uint32_t neighbour_bits(const P& p, const Nbhd& nb, int bit) {
+    uint32_t b = 0;
+    static_for<Q>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if constexpr (k > 0) b |= (uint32_t)((p.mask[nb.at(L::ex(k), L::ey(k), L::ez(k))] >> bit) & 1) << k;
+    });
+    return b;
+  }
+
+  // Post-stream flow populations of fluid cell c: unconditional pulls (mirror
+  // slots hold the bounced populations) plus the gas released by reacting
+  // solid neighbours (pull direction k comes from c - e_k = c + e_opp(k)).
   template <bool PYRO>
-  __device__ __forceinline__ static void pull_flow(const P& p, const Nbhd& nb, int c, C F[Q]) {
+  __device__ __forceinline__ static void pull_flow(const P& p, const Nbhd& nb, int c, uint32_t nbits, C F[Q]) {
     static_for<Q>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       if constexpr (k == 0) {
         F[0] = Store<S>::ld(p.fA, c, fshift<L, S, 0>(p));
       } else {
         const int src = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-        if (solid_at(p, src)) {
-          constexpr int o = L::opp(k);
-          C v = Store<S>::ld(p.fA, (size_t)o * p.N + c, fshift<L, S, o>(p));
-          if constexpr (PYRO) v += (C)p.relA[src] * (C)L::w(k);
-          F[k] = v;
-        } else {
-          F[k] = Store<S>::ld(p.fA, (size_t)k * p.N + src, fshift<L, S, k>(p));
+        C v = Store<S>::ld(p.fA, (size_t)k * p.N + src, fshift<L, S, k>(p));
+        if constexpr (PYRO) {
+          if ((nbits >> L::opp(k)) & 1) v += p.relA[src] * (C)L::w(k);
         }
+        F[k] = v;
       }
     });
   }
@@ -179,17 +191,45 @@ struct Kern {
       const C s = p.eos == 0 ? r : (C)1;
       jx += (C)0.5 * p.Fx * s; jy += (C)0.5 * p.Fy * s; jz += (C)0.5 * p.Fz * s;
     }
-    if (p.eos == 0) { jx /= r; jy /= r; jz /= r; }
+    if (p.eos == 0) {
+      const C ir = (C)1 / r;
+      jx *= ir; jy *= ir; jz *= ir;
+    }
     rho = r; ux = jx; uy = jy; uz = jz;
   }
 
-  // feq9/feq19 with eps = 1 (src/LBM/LBM2D/_evolution.py:213-225)
+  // feq9/feq19 (src/LBM/LBM2D/_evolution.py:213-225, eps = 1) split into the
+  // part even under e -> -e (ev) and the odd part (od): feq_k = ev + od,
+  // feq_opp(k) = ev - od.
   template <int k>
-  __device__ __forceinline__ static C feq(const P& p, C rho, C ux, C uy, C uz, C usq) {
+  __device__ __forceinline__ static void feq_pair(const P& p, C rho, C ux, C uy, C uz, C usq, C& ev, C& od) {
     constexpr C ie = (C)1 / ((C)1 + (C)1e-12);
     const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
-    if (p.eos == 1) return (C)L::w(k) * (rho + (C)3.0 * eu + (C)4.5 * eu * eu * ie - (C)1.5 * usq * ie);
-    return (C)L::w(k) * rho * ((C)1.0 + (C)3.0 * eu + (C)4.5 * eu * eu * ie - (C)1.5 * usq * ie);
+    const C w = (C)L::w(k);
+    if (p.eos == 1) {
+      ev = w * (rho + (C)4.5 * eu * eu * ie - (C)1.5 * usq * ie);
+      od = w * ((C)3.0 * eu);
+    } else {
+      ev = w * rho * ((C)1.0 + (C)4.5 * eu * eu * ie - (C)1.5 * usq * ie);
+      od = w * rho * ((C)3.0 * eu);
+    }
+  }
+  __device__ __forceinline__ static C feq_rest(const P& p, C rho, C usq) {
+    constexpr C ie = (C)1 / ((C)1 + (C)1e-12);
+    const C w = (C)L::w(0);
+    return p.eos == 1 ? w * (rho - (C)1.5 * usq * ie) : w * rho * ((C)1.0 - (C)1.5 * usq * ie);
+  }
+  // Full equilibrium set of (rho, u) in F.
+  __device__ __forceinline__ static void feq_all(const P& p, C rho, C ux, C uy, C uz, C F[Q]) {
+    const C usq = ux * ux + uy * uy + uz * uz;
+    F[0] = feq_rest(p, rho, usq);
+    static_for<NP>([&](auto pp) {
+      constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+      C ev, od;
+      feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+      F[k] = ev + od;
+      F[o] = ev - od;
+    });
   }
 
   // forceTermGuo, src/LBM/LBM2D/_evolution.py:284-298 (eps = 1)
@@ -204,86 +244,143 @@ struct Kern {
     return p.eos == 1 ? t : rho * t;
   }
 
-  // Flow collision: BGK (_evolution.py:33) or MRT (new), plus Guo forcing.
-  // Writes the post-collision populations over F.
+  // Flow collision (BGK: _evolution.py:33; MRT: new) plus Guo forcing; writes
+  // the post-collision populations over F.  Works on opposite-direction pairs.
   template <int COLL>
   __device__ __forceinline__ static void collide_flow(const P& p, C F[Q], C rho, C ux, C uy, C uz) {
     const C tau = (C)3 * (p.eos == 0 ? p.nu / rho : p.nu) + (C)0.5;
     const C itau = (C)1 / tau;
     const C usq = ux * ux + uy * uy + uz * uz;
-    const C pre = (C)1.0 - (C)1.0 / (C)2.0 / tau;
+    const C fe0 = feq_rest(p, rho, usq);
     if constexpr (COLL == LBM_COLL_BGK) {
-      static_for<Q>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        C v = F[k] - itau * (F[k] - feq<k>(p, rho, ux, uy, uz, usq));
-        if (p.has_force) v += guo<k>(p, rho, ux, uy, uz, pre);
-        F[k] = v;
+      F[0] = F[0] - itau * (F[0] - fe0);
+      static_for<NP>([&](auto pp) {
+        constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+        C ev, od;
+        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+        F[k] = F[k] - itau * (F[k] - (ev + od));
+        F[o] = F[o] - itau * (F[o] - (ev - od));
       });
     } else {
-      C fn[Q];
-      static_for<Q>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        fn[k] = F[k] - feq<k>(p, rho, ux, uy, uz, usq);
+      // non-equilibrium parts in pair form: Sn = fneq_k + fneq_o, Dn = fneq_k - fneq_o
+      const C n0 = F[0] - fe0;
+      C Sn[NP], Dn[NP];
+      static_for<NP>([&](auto pp) {
+        constexpr int q = decltype(pp)::value;
+        constexpr int k = pk<L>(q), o = L::opp(k);
+        C ev, od;
+        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+        const C a = F[k] - (ev + od), b = F[o] - (ev - od);
+        Sn[q] = a + b;
+        Dn[q] = a - b;
       });
-      C m[Q];
+      // forward transform of the non-conserved moments, scaled by s_r/|M_r|^2
+      C mt[Q];
       static_for<Q>([&](auto rr) {
         constexpr int r = decltype(rr)::value;
         if constexpr (!L::mrt_conserved(r)) {
+          constexpr bool even = mrt_even<L>(r);
           C acc = 0;
-          static_for<Q>([&](auto kk) {
-            constexpr int k = decltype(kk)::value;
-            constexpr double mv = L::mrt(r, k);
-            if constexpr (mv == 1.0) acc += fn[k];
-            else if constexpr (mv == -1.0) acc -= fn[k];
-            else if constexpr (mv != 0.0) acc += (C)mv * fn[k];
+          if constexpr (even && L::mrt(r, 0) != 0.0) acc = (C)L::mrt(r, 0) * n0;
+          static_for<NP>([&](auto pp) {
+            constexpr int q = decltype(pp)::value;
+            constexpr double mv = L::mrt(r, pk<L>(q));
+            const C v = even ? Sn[q] : Dn[q];
+            if constexpr (mv == 1.0) acc += v;
+            else if constexpr (mv == -1.0) acc -= v;
+            else if constexpr (mv != 0.0) acc += (C)mv * v;
           });
           constexpr double inv_norm = 1.0 / mrt_norm<L>(r);
-          if constexpr (L::mrt_viscous(r)) m[r] = acc * itau * (C)inv_norm;
-          else m[r] = acc * p.mrt_sn[r];
+          if constexpr (L::mrt_viscous(r)) mt[r] = acc * itau * (C)inv_norm;
+          else mt[r] = acc * p.mrt_sn[r];
         }
       });
-      static_for<Q>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        C acc = 0;
+      // back transform: even part E (same for k and opp), odd part O (opposite sign)
+      {
+        C e0 = 0;
+        static_for<Q>([&](auto rr) {
+          constexpr int r = decltype(rr)::value;
+          if constexpr (!L::mrt_conserved(r) && mrt_even<L>(r) && L::mrt(r, 0) != 0.0)
+            e0 += (C)L::mrt(r, 0) * mt[r];
+        });
+        F[0] -= e0;
+      }
+      static_for<NP>([&](auto pp) {
+        constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+        C E = 0, O = 0;
         static_for<Q>([&](auto rr) {
           constexpr int r = decltype(rr)::value;
           if constexpr (!L::mrt_conserved(r)) {
             constexpr double mv = L::mrt(r, k);
-            if constexpr (mv == 1.0) acc += m[r];
-            else if constexpr (mv == -1.0) acc -= m[r];
-            else if constexpr (mv != 0.0) acc += (C)mv * m[r];
+            C& a = mrt_even<L>(r) ? E : O;
+            if constexpr (mv == 1.0) a += mt[r];
+            else if constexpr (mv == -1.0) a -= mt[r];
+            else if constexpr (mv != 0.0) a += (C)mv * mt[r];
           }
         });
-        C v = F[k] - acc;
-        if (p.has_force) v += guo<k>(p, rho, ux, uy, uz, pre);
-        F[k] = v;
+        F[k] -= E + O;
+        F[o] -= E - O;
+      });
+    }
+    if (p.has_force) {
+      const C pre = (C)1.0 - (C)1.0 / (C)2.0 / tau;
+      static_for<Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        F[k] += guo<k>(p, rho, ux, uy, uz, pre);
       });
     }
   }
 
-  // Thermal collision with source (conjugate): fluid geq = TF.geq (advected),
-  // solid geq = w T (TS.geq, LBM2D/_thermal.py:162-166); source wt*dS (:54-58).
-  __device__ __forceinline__ static void collide_thermal(const P& p, C G[QT], C T, bool solid, C ux, C uy,
-                                                         C uz, C dS) {
-    const C itau = solid ? p.itauT_s : p.itauT_f;
+  // Thermal collision with source, one code path for fluid and solid cells:
+  // fluid geq = TF.geq (advected), solid geq = w T (TS.geq, LBM2D/_thermal.py:162-166),
+  // i.e. the fluid form with u = 0; source wt*dS (_evolution.py:54-58).
+  __device__ __forceinline__ static void collide_thermal(const P& p, C G[QT], C T, C itau, C ux, C uy, C uz,
+                                                         C dS) {
     const C usq = ux * ux + uy * uy + uz * uz;
-    static_for<QT>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      C ge;
-      if (solid) {
-        ge = (C)L::wt(k) * T;
-      } else {
-        const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
-        ge = (C)L::wt(k) * T * ((C)1.0 + (C)L::ta * eu + (C)L::tb * eu * eu - (C)L::tc * usq);
-      }
-      G[k] = G[k] - itau * (G[k] - ge) + (C)L::wt(k) * dS;
+    {
+      const C ge = (C)L::wt(0) * T * ((C)1.0 - (C)L::tc * usq);
+      G[0] = G[0] - itau * (G[0] - ge) + (C)L::wt(0) * dS;
+    }
+    static_for<(QT - 1) / 2>([&](auto pp) {
+      constexpr int k = pkt<L, QT>(decltype(pp)::value), o = L::opp(k);
+      const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
+      const C wT = (C)L::wt(k) * T;
+      const C ev = wT * ((C)1.0 + (C)L::tb * eu * eu - (C)L::tc * usq);
+      const C od = wT * ((C)L::ta * eu);
+      const C src = (C)L::wt(k) * dS;
+      G[k] = G[k] - itau * (G[k] - (ev + od)) + src;
+      G[o] = G[o] - itau * (G[o] - (ev - od)) + src;
+    });
+  }
+  // geq of (T, u) itself (initialisation).
+  __device__ __forceinline__ static void geq_all(C T, C ux, C uy, C uz, C G[QT]) {
+    const C usq = ux * ux + uy * uy + uz * uz;
+    G[0] = (C)L::wt(0) * T * ((C)1.0 - (C)L::tc * usq);
+    static_for<(QT - 1) / 2>([&](auto pp) {
+      constexpr int k = pkt<L, QT>(decltype(pp)::value), o = L::opp(k);
+      const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
+      const C wT = (C)L::wt(k) * T;
+      const C ev = wT * ((C)1.0 + (C)L::tb * eu * eu - (C)L::tc * usq);
+      const C od = wT * ((C)L::ta * eu);
+      G[k] = ev + od;
+      G[o] = ev - od;
     });
   }
 
-  __device__ __forceinline__ static void store_flow(const P& p, int c, const C F[Q]) {
+  // Store post-collision flow populations; a population headed for a solid
+  // neighbour (bit k of sbits) goes to the neighbour's mirror slot opp(k).
+  __device__ __forceinline__ static void store_flow(const P& p, const Nbhd& nb, int c, uint32_t sbits,
+                                                    const C F[Q]) {
     static_for<Q>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      Store<S>::st(p.fB, (size_t)k * p.N + c, F[k], fshift<L, S, k>(p));
+      if constexpr (k == 0) {
+        Store<S>::st(p.fB, c, F[0], fshift<L, S, 0>(p));
+      } else {
+        const size_t idx = ((sbits >> k) & 1)
+                               ? (size_t)L::opp(k) * p.N + nb.at(L::ex(k), L::ey(k), L::ez(k))
+                               : (size_t)k * p.N + c;
+        Store<S>::st(p.fB, idx, F[k], fshift<L, S, k>(p));
+      }
     });
   }
   __device__ __forceinline__ static void store_thermal(const P& p, int c, const C G[QT]) {
@@ -306,7 +403,6 @@ struct DiagAcc {
   double v[kNumDiag];
   __device__ __forceinline__ void clear() {
     for (int i = 0; i < kNumDiag; ++i) v[i] = 0;
-    v[3] = 0;       // umax^2
     v[4] = 1e300;   // Tmin
     v[5] = -1e300;  // Tmax
   }
@@ -342,49 +438,45 @@ __device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row, 
   }
 }
 
-template <class L, class S>
-__device__ __forceinline__ void diag_cell(const StepParams<S>& p, DiagAcc& a, int c, bool fluid,
-                                          bool reactive_solid, typename Store<S>::C rho,
+// Flow part of one cell's diagnostics (and macro/residual outputs).
+template <class S>
+__device__ __forceinline__ void diag_flow(const StepParams<S>& p, DiagAcc& a, int c, typename Store<S>::C rho,
                                           typename Store<S>::C ux, typename Store<S>::C uy,
-                                          typename Store<S>::C uz, typename Store<S>::C T, bool thermal,
-                                          typename Store<S>::C alpha) {
-  using C = typename Store<S>::C;
-  if (thermal) {
-    a.v[1] += (double)T;
-    a.v[4] = fmin(a.v[4], (double)T);
-    a.v[5] = fmax(a.v[5], (double)T);
-    if (!finite_(T)) a.v[6] += 1;
+                                          typename Store<S>::C uz) {
+  a.v[0] += (double)rho;
+  const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
+  a.v[3] = fmax(a.v[3], u2);
+  if (!finite_(rho)) a.v[6] += 1;
+  a.v[7] += 1;
+  if (p.flags & LBM_STEP_RESIDUAL) {
+    const double dx = (double)ux - p.uprev[c], dy = (double)uy - p.uprev[p.N + c],
+                 dz = (double)uz - p.uprev[2 * p.N + c];
+    a.v[8] += dx * dx + dy * dy + dz * dz;
+    a.v[9] += u2;
+    p.uprev[c] = (float)ux;
+    p.uprev[p.N + c] = (float)uy;
+    p.uprev[2 * p.N + c] = (float)uz;
   }
-  if (fluid) {
-    a.v[0] += (double)rho;
-    const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
-    a.v[3] = fmax(a.v[3], u2);
-    if (!finite_(rho)) a.v[6] += 1;
-    a.v[7] += 1;
-    if (p.flags & LBM_STEP_RESIDUAL) {
-      const double dx = (double)ux - p.uprev[c], dy = (double)uy - p.uprev[p.N + c],
-                   dz = (double)uz - p.uprev[2 * p.N + c];
-      a.v[8] += dx * dx + dy * dy + dz * dz;
-      a.v[9] += u2;
-      p.uprev[c] = (float)ux;
-      p.uprev[p.N + c] = (float)uy;
-      p.uprev[2 * p.N + c] = (float)uz;
-    }
-    if (p.flags & LBM_STEP_MACRO) {
-      p.rho_out[c] = rho;
-      p.u_out[c] = ux;
-      p.u_out[p.N + c] = uy;
-      p.u_out[2 * p.N + c] = uz;
-    }
-  } else if (reactive_solid) {
-    a.v[2] += (double)alpha;
+  if (p.flags & LBM_STEP_MACRO) {
+    p.rho_out[c] = rho;
+    p.u_out[c] = ux;
+    p.u_out[p.N + c] = uy;
+    p.u_out[2 * p.N + c] = uz;
   }
-  if (thermal && (p.flags & LBM_STEP_MACRO)) p.T_out[c] = T;
-  (void)sizeof(C);
+}
+// Temperature part (every cell).
+template <class S>
+__device__ __forceinline__ void diag_thermal(const StepParams<S>& p, DiagAcc& a, int c, typename Store<S>::C T) {
+  a.v[1] += (double)T;
+  a.v[4] = fmin(a.v[4], (double)T);
+  a.v[5] = fmax(a.v[5], (double)T);
+  if (!finite_(T)) a.v[6] += 1;
+  if (p.flags & LBM_STEP_MACRO) p.T_out[c] = T;
 }
 
-// Mean post-stream (rho, u) over the fluid neighbours of (x,y,z), in direction
-// order 1..Q-1; (1, 0) if there are none.  Used when a spent solid cell turns fluid.
+// Mean post-stream (rho, u) over the fluid neighbours of (x,y,z) at the pass
+// parity, in direction order 1..Q-1; (1, 0) if there are none.  Used when a
+// spent solid cell turns fluid.
 template <class L, class S>
 __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y, int z,
                                             typename Store<S>::C& rb, typename Store<S>::C& ux,
@@ -394,21 +486,23 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
   constexpr int Q = L::Q;
   C rs = 0, us0 = 0, us1 = 0, us2 = 0;
   int n = 0;
-  static_for<Q>([&](auto kk) {
-    constexpr int q = decltype(kk)::value;
-    if constexpr (q > 0) {
-      const int xq = wrapi(x + L::ex(q), p.nx), yq = wrapi(y + L::ey(q), p.ny), zq = wrapi(z + L::ez(q), p.nz);
-      const int cq = xq + p.nx * (yq + p.ny * zq);
-      if (!K::solid_at(p, cq)) {
-        const Nbhd nq(xq, yq, zq, p.nx, p.ny, p.nz);
-        C Fq[Q], rq, uxq, uyq, uzq;
-        K::template pull_flow<true>(p, nq, cq, Fq);
-        K::moments(p, Fq, rq, uxq, uyq, uzq);
-        rs += rq; us0 += uxq; us1 += uyq; us2 += uzq;
-        ++n;
-      }
-    }
-  });
+  for (int q = 1; q < Q; ++q) {
+    int dx = 0, dy = 0, dz = 0;
+    static_for<Q>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if (k == q) { dx = L::ex(k); dy = L::ey(k); dz = L::ez(k); }
+    });
+    const int xq = wrapi(x + dx, p.nx), yq = wrapi(y + dy, p.ny), zq = wrapi(z + dz, p.nz);
+    const int cq = xq + p.nx * (yq + p.ny * zq);
+    if (K::solid_bit(p, cq, p.par)) continue;
+    const Nbhd nq(xq, yq, zq, p.nx, p.ny, p.nz);
+    const uint32_t nbq = K::neighbour_bits(p, nq, p.par);
+    C Fq[Q], rq, uxq, uyq, uzq;
+    K::template pull_flow<true>(p, nq, cq, nbq, Fq);
+    K::moments(p, Fq, rq, uxq, uyq, uzq);
+    rs += rq; us0 += uxq; us1 += uyq; us2 += uzq;
+    ++n;
+  }
   rb = n ? rs / (C)n : (C)1;
   ux = n ? us0 / (C)n : (C)0;
   uy = n ? us1 / (C)n : (C)0;
@@ -418,111 +512,128 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
 // ------------------------------------------------------------------ kernels
 // THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis.
 template <class L, class S, int COLL, int THERM>
-__global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
+// FP32/FP16 arithmetic: at most 128 registers per thread, 4 blocks of 128
+// threads (16 warps) per SM; FP64 keeps the full register budget.  blockDim.x
+// is a multiple of 32 and at most 256 (a tile of consecutive x cells).
+__global__ void __launch_bounds__(256, (std::is_same<S, double>::value ? 1 : 2))
+    step_bulk(const __grid_constant__ StepParams<S> p) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr int Q = L::Q, QT = L::QT;
   constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
-  const int x = blockIdx.x * blockDim.x + threadIdx.x;
   const int y = blockIdx.y, z = blockIdx.z;
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
   const bool peek = (p.flags & kStepPeek) != 0;
   DiagAcc acc;
   if (diag) acc.clear();
 
-  if (x < p.nx && !K::on_active_side(p, x, y, z)) {
+  // Rank the tile's cells fluid first, then solid, then cells this kernel skips
+  // (past nx or on an active side), so that warps run one branch instead of both.
+  __shared__ uint8_t s_rank_cell[256];
+  __shared__ uint8_t s_mask[256];
+  __shared__ int s_count[2][8];
+  int x, cell_kind;  // 0 fluid, 1 solid, 2 skipped
+  uint8_t mk;
+  {
+    const int xt = blockIdx.x * blockDim.x + threadIdx.x;
+    const bool ok = xt < p.nx && !K::on_active_side(p, xt, y, z);
+    const uint8_t mt = ok ? p.mask[xt + p.nx * (y + p.ny * z)] : (uint8_t)0;
+    const int kind = !ok ? 2 : (((mt >> p.par) & 1) ? 1 : 0);
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+    const unsigned bf = __ballot_sync(0xffffffffu, kind == 0), bs = __ballot_sync(0xffffffffu, kind == 1);
+    if (lane == 0) { s_count[0][warp] = __popc(bf); s_count[1][warp] = __popc(bs); }
+    s_mask[threadIdx.x] = mt;
+    __syncthreads();
+    int nf = 0, ns = 0, pf = 0, ps = 0, pk_ = 0;
+    for (int w = 0; w < nw; ++w) {
+      if (w < warp) { pf += s_count[0][w]; ps += s_count[1][w]; pk_ += 32 - s_count[0][w] - s_count[1][w]; }
+      nf += s_count[0][w]; ns += s_count[1][w];
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    int rank;
+    if (kind == 0) rank = pf + __popc(bf & lt);
+    else if (kind == 1) rank = nf + ps + __popc(bs & lt);
+    else rank = nf + ns + pk_ + __popc(~(bf | bs) & lt);
+    s_rank_cell[rank] = (uint8_t)threadIdx.x;
+    __syncthreads();
+    const int t = s_rank_cell[threadIdx.x];
+    x = blockIdx.x * blockDim.x + t;
+    mk = s_mask[t];
+    cell_kind = (int)threadIdx.x < nf ? 0 : ((int)threadIdx.x < nf + ns ? 1 : 2);
+  }
+
+  if (cell_kind != 2) {
     const int c = x + p.nx * (y + p.ny * z);
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-    const uint8_t mk = p.mask[c];
-    const bool solid = (mk >> p.par) & 1;
-    bool solid_next = solid;
+    const bool solid = cell_kind == 1;
+    const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
     C G[QT > 0 ? QT : 1];
-    C T = 0, dS = 0;
+    C T = 0, dS = 0, rho = 0, ux = 0, uy = 0, uz = 0;
     if constexpr (THERMAL) {
       K::pull_thermal(p, nb, c, G);
       static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
     }
+    bool solid_next = solid;
+    bool flipping = false;
     if (!solid) {
       C F[Q];
-      C rho, ux, uy, uz;
-      K::template pull_flow<PYRO>(p, nb, c, F);
+      K::template pull_flow<PYRO>(p, nb, c, nbits, F);
       K::moments(p, F, rho, ux, uy, uz);
-      if (diag) diag_cell<L, S>(p, acc, c, true, false, rho, ux, uy, uz, T, THERMAL, (C)0);
+      if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
       if (!peek) {
         K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
-        K::store_flow(p, c, F);
-        if constexpr (THERMAL) {
-          K::collide_thermal(p, G, T, false, ux, uy, uz, (C)0);
-          K::store_thermal(p, c, G);
-        }
+        K::store_flow(p, nb, c, nbits, F);
       }
-    } else {
-      C ux = 0, uy = 0, uz = 0;
-      C an = 0;
-      const bool reactive = PYRO && (mk & LBM_MASK_REACTIVE);
-      if constexpr (PYRO) {
-        if (reactive && peek) {
-          // Current state: alpha already updated; a cell flipped in the last pass
-          // reports the neighbour-mean state it was given.
-          an = p.alpha[c];
-          if (!((mk >> (p.par ^ 1)) & 1)) {
-            solid_next = false;
-            C rb;
-            neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
-            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, (C)0);
-          }
-        } else if (reactive) {
+    } else if constexpr (PYRO) {
+      if (mk & LBM_MASK_REACTIVE) {
+        if (peek) {
+          // current state: a cell that turned fluid on the last pass is fluid now;
+          // flip_cells<> reports its flow state
+          if (!((mk >> (p.par ^ 1)) & 1)) solid_next = false;
+        } else {
           // Arrhenius rate at the solid temperature, src/LBM/LBM2D/_chemical.py:198-212
-          const C a = (C)p.alpha[c];
+          const C a = p.alpha[c];
           const C TK = T * p.Tscale + p.Tref;
           C kr = 0;
           if (TK > p.pyTmin) {
             const C Te = TK + (C)1e-6;
-            kr = p.pyA * exp(-(p.pyEa / Te / (C)kGasConstant));
+            kr = p.pyA * exp(-(p.pyEaR / Te));
             if (p.pyb != (C)0) kr *= pow(Te, p.pyb);
           }
           const C da = kr * a * p.dtp;
-          const C anC = a - da;
-          an = anC;
+          const C an = a - da;
           p.alpha[c] = an;
           dS = -p.heat_norm * da;
-          const C mg = p.gas_coef * da;
-          C W = 0;
-          static_for<Q>([&](auto kk) {
-            constexpr int k = decltype(kk)::value;
-            if constexpr (k > 0) {
-              if (!K::solid_at(p, nb.at(L::ex(k), L::ey(k), L::ez(k)))) W += (C)L::w(k);
-            }
-          });
-          if (anC < p.alpha_flip) {
-            // Spent cell turns fluid at the mean (rho, u) of its fluid neighbours.
+          if (an < p.alpha_flip) {
+            // turns fluid: flip_cells<> finishes it after this pass and finds the
+            // heat source here
             solid_next = false;
-            C rb;
-            neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
-            C F[Q];
-            const C usq = ux * ux + uy * uy + uz * uz;
+            flipping = true;
+            p.relB[c] = dS;
+          } else {
+            C W = 0;
             static_for<Q>([&](auto kk) {
               constexpr int k = decltype(kk)::value;
-              F[k] = K::template feq<k>(p, rb, ux, uy, uz, usq);
+              if constexpr (k > 0) {
+                if (!((nbits >> k) & 1)) W += (C)L::w(k);
+              }
             });
-            if (diag) diag_cell<L, S>(p, acc, c, true, false, rb, ux, uy, uz, (C)0, false, (C)0);
-            K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
-            K::store_flow(p, c, F);
-            p.relB[c] = (C)0;
-          } else {
-            p.relB[c] = W > (C)0 ? mg / W : (C)0;
+            p.relB[c] = W > (C)0 ? p.gas_coef * da / W : (C)0;
           }
         }
       }
-      if constexpr (THERMAL) {
-        if (!peek) {
-          K::collide_thermal(p, G, T, solid_next, ux, uy, uz, dS);
-          K::store_thermal(p, c, G);
-        }
-      }
-      if (diag) diag_cell<L, S>(p, acc, c, false, solid_next && reactive, 0, 0, 0, 0, T, THERMAL, an);
     }
-    // Mask bit for the next parity: written only when it changes.
+    if constexpr (THERMAL) {
+      if (!peek && !flipping) {
+        const bool fl = !solid;
+        K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
+                           fl ? uz : (C)0, dS);
+        K::store_thermal(p, c, G);
+      }
+      if (diag) diag_thermal(p, acc, c, T);
+    }
+    if (PYRO && diag && solid_next && (mk & LBM_MASK_REACTIVE)) acc.v[2] += (double)p.alpha[c];
+    // mask bit for the next parity: written only when it changes
     if (!peek) {
       const int np = p.par ^ 1;
       const uint8_t want = (uint8_t)((mk & ~(1u << np)) | ((solid_next ? 1u : 0u) << np));
@@ -533,6 +644,76 @@ __global__ void __launch_bounds__(256) step_bulk(const StepParams<S> p) {
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk), (size_t)p.partial_rows);
   }
+}
+
+// Cells that turned fluid on this pass (mask bit par solid, bit par^1 fluid).
+// Runs after step_bulk and step_boundary, over the whole mask (in a peek pass it
+// only reports the flow state of cells that turned fluid on the last pass):
+//  1. fluid neighbours z = X - e_k stored their population towards X in X's
+//     mirror slot f[opp k][X]; it moves to f[k][z], where X now pulls it from;
+//  2. X takes the mean post-stream (rho, u) of its fluid neighbours, collides
+//     from that equilibrium and stores with the mirror rule of the next parity;
+//  3. its temperature populations collide as fluid with the heat source that
+//     step_bulk left in rel[B][X].
+template <class L, class S, int COLL, int THERM>
+__global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepParams<S> p) {
+  using K = Kern<L, S>;
+  using C = typename Store<S>::C;
+  constexpr int Q = L::Q, QT = L::QT;
+  constexpr bool THERMAL = THERM >= 1;
+  const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
+  DiagAcc acc;
+  if (diag) acc.clear();
+  const int np = p.par ^ 1;
+  const bool peek = (p.flags & kStepPeek) != 0;
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t c0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < p.N; c0 += stride) {
+    const uint8_t mk = p.mask[c0];
+    if (!(((mk >> p.par) & 1) && !((mk >> np) & 1))) continue;
+    const int c = (int)c0;
+    const int x = c % p.nx, y = (c / p.nx) % p.ny, z = c / (p.nx * p.ny);
+    const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
+    C rb, ux, uy, uz;
+    neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
+    if (peek) {
+      // recomputing the current state: report the state the cell was given
+      if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
+      continue;
+    }
+    {
+      C mir[Q];
+      static_for<Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        if constexpr (k > 0)
+          mir[k] = Store<S>::ld(p.fB, (size_t)L::opp(k) * p.N + c, fshift<L, S, L::opp(k)>(p));
+      });
+      static_for<Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        if constexpr (k > 0) {
+          const int zc = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
+          if (!K::solid_bit(p, zc, p.par)) Store<S>::st(p.fB, (size_t)k * p.N + zc, mir[k], fshift<L, S, k>(p));
+        }
+      });
+    }
+    {
+      C F[Q];
+      K::feq_all(p, rb, ux, uy, uz, F);
+      K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
+      K::store_flow(p, nb, c, K::neighbour_bits(p, nb, np), F);
+    }
+    if constexpr (THERMAL) {
+      C G[QT];
+      K::pull_thermal(p, nb, c, G);
+      C T = 0;
+      static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
+      const C dS = p.relB[c];
+      p.relB[c] = (C)0;
+      K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
+      K::store_thermal(p, c, G);
+    }
+    if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
+  }
+  if (diag) block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blockIdx.x), (size_t)p.partial_rows);
 }
 
 // --------------------------------------------------------- boundary kernel
@@ -548,14 +729,15 @@ struct MState {
 // 1: y sides, 2: z sides), in the reference's loop order
 // (src/LBM/LBM3D/_boundary.py:15-68).  PASS = -1 is the post-stream macro state.
 template <class L, class S, bool THERMAL, bool PYRO, int PASS>
-__device__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z) {
+__device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   MState<L, S> s;
   if constexpr (PASS < 0) {
     const int c = x + p.nx * (y + p.ny * z);
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-    K::template pull_flow<PYRO>(p, nb, c, s.F);
+    const uint32_t nbits = PYRO ? K::neighbour_bits(p, nb, p.par) : 0u;
+    K::template pull_flow<PYRO>(p, nb, c, nbits, s.F);
     K::moments(p, s.F, s.rho, s.ux, s.uy, s.uz);
     s.T = 0;
     if constexpr (THERMAL) {
@@ -586,10 +768,14 @@ __device__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z) {
     else if (sd.rho_type == LBM_BC_ZEROGRADIENT) s.rho = in.rho;
     const C usb = s.ux * s.ux + s.uy * s.uy + s.uz * s.uz;
     const C usi = in.ux * in.ux + in.uy * in.uy + in.uz * in.uz;
-    static_for<L::Q>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      s.F[k] = K::template feq<k>(p, s.rho, s.ux, s.uy, s.uz, usb) +
-               (in.F[k] - K::template feq<k>(p, in.rho, in.ux, in.uy, in.uz, usi));
+    s.F[0] = K::feq_rest(p, s.rho, usb) + (in.F[0] - K::feq_rest(p, in.rho, usi));
+    static_for<num_pairs<L>()>([&](auto pp) {
+      constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+      C evb, odb, evi, odi;
+      K::template feq_pair<k>(p, s.rho, s.ux, s.uy, s.uz, usb, evb, odb);
+      K::template feq_pair<k>(p, in.rho, in.ux, in.uy, in.uz, usi, evi, odi);
+      s.F[k] = (evb + odb) + (in.F[k] - (evi + odi));
+      s.F[o] = (evb - odb) + (in.F[o] - (evi - odi));
     });
     if constexpr (THERMAL) {
       if (sd.T_type == LBM_BC_FIXEDVALUE) s.T = (C)sd.T;
@@ -610,7 +796,8 @@ __device__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z) {
 // One thread per boundary cell.  blockIdx.y selects an active face; a cell on
 // several active faces is owned by the lowest-numbered one.
 template <class L, class S, int COLL, int THERM>
-__global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4 faces01, int2 faces2) {
+__global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ StepParams<S> p, int4 faces01,
+                                                      int2 faces2) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
@@ -633,7 +820,6 @@ __global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4
     z = face == 4 ? 0 : p.nz - 1; x = i % p.nx; y = i / p.nx;
   }
   if (valid) {
-    // ownership: skip if a lower-numbered active face also contains the cell
     for (int f = 0; f < face; ++f) {
       if (!(p.active & (1 << f))) continue;
       const bool on = (f == 0 && x == 0) || (f == 1 && x == p.nx - 1) || (f == 2 && y == 0) ||
@@ -645,13 +831,15 @@ __global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4
     const int c = x + p.nx * (y + p.ny * z);
     MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z);
     if (diag) {
-      diag_cell<L, S>(p, acc, c, true, false, s.rho, s.ux, s.uy, s.uz, s.T, THERMAL, (C)0);
+      diag_flow(p, acc, c, s.rho, s.ux, s.uy, s.uz);
+      if (THERMAL) diag_thermal(p, acc, c, s.T);
     }
     if (!(p.flags & kStepPeek)) {
+      const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
       K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
-      K::store_flow(p, c, s.F);
+      K::store_flow(p, nb, c, K::neighbour_bits(p, nb, p.par), s.F);
       if constexpr (THERMAL) {
-        K::collide_thermal(p, s.G, s.T, false, s.ux, s.uy, s.uz, (C)0);
+        K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
         K::store_thermal(p, c, s.G);
       }
     }
@@ -665,9 +853,11 @@ __global__ void __launch_bounds__(128) step_boundary(const StepParams<S> p, int4
 // ------------------------------------------------------- init / finalize
 // Equilibrium initialisation: post-collision state of f = feq(rho,u), g = geq(T,u),
 // i.e. what the reference's first collision produces after init_kernel
-// (src/LBM/LBM2D/_initialize.py:37-65).
+// (src/LBM/LBM2D/_initialize.py:37-65).  Writes the B side of `p` (the buffer the
+// first pass reads) with the mirror rule; `solid_bit` selects the input mask bit.
 template <class L, class S, int COLL, int THERM>
-__global__ void init_equilibrium_kernel(StepParams<S> p, const float* rho_in, const float* u_in,
+__global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p, const float* rho_in,
+                                        const float* u_in,
                                         const float* T_in, const float* alpha_in, int solid_bit) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
@@ -677,34 +867,22 @@ __global__ void init_equilibrium_kernel(StepParams<S> p, const float* rho_in, co
   if (c >= p.N) return;
   const uint8_t m0 = p.mask[c];
   const bool solid = (m0 >> solid_bit) & 1;
-  p.mask[c] = (uint8_t)((m0 & LBM_MASK_REACTIVE) | (solid ? LBM_MASK_SOLID : 0u));
+  const int x = (int)(c % p.nx), y = (int)((c / p.nx) % p.ny), z = (int)(c / ((size_t)p.nx * p.ny));
+  const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
+  // neighbours' bit `solid_bit` keeps its value while the bytes are normalised
+  const uint32_t nbits = K::neighbour_bits(p, nb, solid_bit);
   const C rho = (C)rho_in[c];
   const C ux = (C)u_in[c], uy = (C)u_in[p.N + c], uz = (C)u_in[2 * p.N + c];
   if (!solid) {
     C F[Q];
-    const C usq = ux * ux + uy * uy + uz * uz;
-    static_for<Q>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      F[k] = K::template feq<k>(p, rho, ux, uy, uz, usq);
-    });
+    K::feq_all(p, rho, ux, uy, uz, F);
     K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
-    K::store_flow(p, (int)c, F);
+    K::store_flow(p, nb, (int)c, nbits, F);
   }
   if constexpr (THERMAL) {
-    const C T = (C)T_in[c];
     C G[QT];
-    const C z0 = 0;
-    static_for<QT>([&](auto kk) { G[decltype(kk)::value] = z0; });
-    // geq itself: collide_thermal with itau toward geq from G = geq gives geq.
-    const C usq = solid ? (C)0 : ux * ux + uy * uy + uz * uz;
-    static_for<QT>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      if (solid) G[k] = (C)L::wt(k) * T;
-      else {
-        const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
-        G[k] = (C)L::wt(k) * T * ((C)1.0 + (C)L::ta * eu + (C)L::tb * eu * eu - (C)L::tc * usq);
-      }
-    });
+    if (solid) K::geq_all((C)T_in[c], (C)0, (C)0, (C)0, G);
+    else K::geq_all((C)T_in[c], ux, uy, uz, G);
     K::store_thermal(p, (int)c, G);
   }
   if constexpr (PYRO) {
@@ -712,6 +890,7 @@ __global__ void init_equilibrium_kernel(StepParams<S> p, const float* rho_in, co
     p.relB[c] = (C)0;
     const_cast<C*>(p.relA)[c] = (C)0;
   }
+  p.mask[c] = (uint8_t)((m0 & LBM_MASK_REACTIVE) | (solid ? LBM_MASK_SOLID : 0u));
 }
 
 constexpr int kStage1Blocks = 256;  // first-level partial sums of the diagnostics
@@ -723,7 +902,7 @@ __device__ __forceinline__ double diag_combine(int i, double a, double b) {
   return (i == 3 || i == 5) ? fmax(a, b) : (i == 4 ? fmin(a, b) : a + b);
 }
 
-// Fixed-shape shared-memory tree over 256 threads; returns the total in thread 0.
+// Fixed-shape shared-memory tree over 256 threads; returns the total in every thread.
 __device__ __forceinline__ double block_tree_256(int i, double v, double* sh) {
   sh[threadIdx.x] = v;
   __syncthreads();
