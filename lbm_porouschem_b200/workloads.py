@@ -56,9 +56,10 @@ def _pyro_cfg(dim, nx, ny, nz, precision, collision, rho_in, walls: bool) -> Lat
     if walls:
         sides[2] = SideBC.wall(T_type=ZERO_GRADIENT)
         sides[3] = SideBC.wall(T_type=ZERO_GRADIENT)
+    # T0: FP16 storage shift of the temperature populations, mid-range of T in [0, 1]
     return LatticeConfig(dim=dim, nx=nx, ny=ny, nz=nz, collision=collision, precision=precision,
                          nu=(tau - 0.5) / 3.0, thermal="conjugate", tauT_fluid=0.6, tauT_solid=0.9,
-                         pyro=True, sides=sides)
+                         pyro=True, sides=sides, T0=0.5)
 
 
 def pyro2d(nx: int = 512, ny: int = 256, seed: int = 0, precision: str = "fp32",

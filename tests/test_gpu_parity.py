@@ -143,6 +143,7 @@ def test_flow2d_fp16_vs_fp64_oracle(oracle_mod):
 
 def test_pyro3d_fp16_runs_close_to_fp64(oracle_mod):
     w = _fast_pyro(workloads.pyro3d(20, seed=3, ny=16, nz=12), A=1.2e11)
+    w.cfg.T0 = 1.0   # FP16 stores g - wt*T0: the shift sits at the working temperature
     lat, o = _run_pair(oracle_mod, w, 120, "f64", "fp16")
     g, r = lat.fields(), o.fields()
     assert np.array_equal(g["solid"], r["solid"])
