@@ -189,6 +189,24 @@ LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
  * src/LBM/LBM2D/_evolution.py:15). */
 LBM_API int64_t lbm_step_count(const lbm_handle* h);
 
+/* No counterpart in the reference.  The diagnostics of the current state (the
+ * values lbm_compute_macro(h, LBM_STEP_DIAG, ...) + lbm_read_diag return),
+ * computed without any device allocation, for callers that cannot allocate
+ * device memory: e.g. a plug-in whose host application owns every device
+ * allocation through its own pool, or a hook inside a latency-critical time
+ * loop where a cudaMalloc, which may synchronise the device, is not allowed.
+ * The lattice state must be bound; LBM_FIELD_SCRATCH need not be.  The
+ * reduction's scratch is a static device array held by every GPU that loads
+ * the library until exit (about 2.6 MB): lattices whose launch plan needs more
+ * than LBM_NOALLOC_MAX_ROWS partial rows (one per thread block, e.g. up to
+ * about 128^3 cells in 3D) are rejected with LBM_ERR_SIZE.  The first call on
+ * a device looks up the array's device address (make it before any stream
+ * capture).  All calls share the array and each call rewrites every value it
+ * reads, so calls that overlap on the GPU (different streams or handles at
+ * the same time) race.  Synchronises `stream`. */
+#define LBM_NOALLOC_MAX_ROWS 32768
+LBM_API int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

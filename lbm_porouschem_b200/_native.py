@@ -41,8 +41,9 @@ EXPORTED = (
     "lbm_abi_version", "lbm_last_error", "lbm_required_bytes", "lbm_create", "lbm_destroy",
     "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_step", "lbm_compute_macro",
     "lbm_read_diag",
-    "lbm_step_count",
+    "lbm_step_count", "lbm_diag_noalloc",
 )
+LBM_NOALLOC_MAX_ROWS = 32768
 
 
 class lbm_side_desc(C.Structure):
@@ -121,6 +122,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_read_diag.restype = i32
     lib.lbm_step_count.argtypes = [vp]
     lib.lbm_step_count.restype = i64
+    lib.lbm_diag_noalloc.argtypes = [vp, C.POINTER(lbm_diag), vp]
+    lib.lbm_diag_noalloc.restype = i32
     if lib.lbm_abi_version() != 1:
         raise RuntimeError("liblbm_b200.so ABI version mismatch")
     _lib = lib

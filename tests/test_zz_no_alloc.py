@@ -1,0 +1,71 @@
+"""lbm_diag_noalloc: diagnostics for callers that cannot allocate device memory.
+
+Some callers of this library cannot call cudaMalloc: a plug-in whose host
+application owns every device allocation through its own memory pool, or a
+monitoring hook inside a latency-critical time loop where an allocation (which
+may synchronise the whole device) is not allowed.  lbm_diag_noalloc gives them
+the diagnostics of the current lattice state using a static device array as
+scratch.  These tests call it through the C ABI and check it against the
+allocating path (lbm_compute_macro + lbm_read_diag) on two calls in a row, and
+check that a lattice too large for the static array is refused.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from lbm_porouschem_b200 import _native as N
+from lbm_porouschem_b200 import workloads
+
+pytestmark = pytest.mark.gpu
+
+KEYS = ("mass", "energy", "solid_alpha", "umax", "Tmin", "Tmax", "nfluid", "nonfinite")
+
+
+def _noalloc(lat):
+    d = N.lbm_diag()
+    N.check(lat.lib.lbm_diag_noalloc(lat._h, ctypes.byref(d), lat._s()))
+    return {k: getattr(d, k) for k, _ in N.lbm_diag._fields_}
+
+
+def _allocating(lat):
+    return lat.diagnostics()
+
+
+@pytest.mark.parametrize("precision", ["fp64", "fp32"])
+def test_noalloc_matches_allocating_path_twice(precision):
+    from lbm_porouschem_b200.lattice import Lattice
+    w = workloads.pyro2d(64, 40, seed=11, precision=precision)
+    w.cfg.pyro_A = 4.5e10
+    w.cfg.heat_norm = 0.02
+    w.cfg.gas_coef = 0.05
+    w.init["T"] = 1.0
+    lat = Lattice(w.cfg)
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    rtol = 1e-12 if precision == "fp64" else 1e-6
+    for nsteps in (37, 180):            # the second call follows further steps (cells convert)
+        lat.step(nsteps)
+        a = _noalloc(lat)
+        b = _allocating(lat)
+        assert a["step"] == b["step"] == lat.nsteps
+        for k in KEYS:
+            assert a[k] == pytest.approx(b[k], rel=rtol, abs=1e-12), k
+    assert a["nfluid"] > 0 and np.isfinite(a["mass"])
+    lat.close()
+
+
+def test_noalloc_rejects_lattice_beyond_static_scratch():
+    from lbm_porouschem_b200.config import LatticeConfig
+    from lbm_porouschem_b200.lattice import Lattice
+    # 32 x 200 x 200: one 32-wide block per (y, z) row -> 40000 partial rows > 32768
+    cfg = LatticeConfig(dim=3, nx=32, ny=200, nz=200, nu=0.1)
+    lat = Lattice(cfg)
+    lat.set_geometry(np.zeros(cfg.shape, dtype=bool))
+    lat.init()
+    lat.step(1)
+    d = N.lbm_diag()
+    rc = lat.lib.lbm_diag_noalloc(lat._h, ctypes.byref(d), lat._s())
+    assert rc == N.LBM_ERR_SIZE
+    assert b"LBM_NOALLOC_MAX_ROWS" in lat.lib.lbm_last_error()
+    lat.close()
