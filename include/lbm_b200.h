@@ -44,6 +44,7 @@ extern "C" {
 #define LBM_ERR_CUDA 3       /* a CUDA call failed */
 #define LBM_ERR_NONFINITE 4  /* diagnostics saw NaN/Inf */
 #define LBM_ERR_SIZE 5       /* a size exceeds a fixed limit */
+#define LBM_ERR_TIMEOUT 6    /* a bounded wait inside a kernel gave up (state invalid) */
 
 /* descriptor enums */
 #define LBM_COLL_BGK 0

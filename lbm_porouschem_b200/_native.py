@@ -20,6 +20,7 @@ LBM_ERR_UNBOUND = 2
 LBM_ERR_CUDA = 3
 LBM_ERR_NONFINITE = 4
 LBM_ERR_SIZE = 5
+LBM_ERR_TIMEOUT = 6
 
 LBM_COLL_BGK, LBM_COLL_MRT = 0, 1
 LBM_PREC_FP32, LBM_PREC_FP16, LBM_PREC_FP64 = 0, 1, 2

@@ -3,12 +3,14 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 
+#include "staged_kernel.cuh"
 #include "step_kernels.cuh"
 
 namespace lbm {
@@ -39,7 +41,20 @@ struct Launch {
   dim3 bc_grid;
   int bulk_blocks, bc_blocks;
   int flip_blocks;    // grid of flip_cells (pyrolysis only), 256 threads each
+  bool staged;        // bulk update by step_bulk_staged (persistent grid of bulk_blocks)
 };
+
+// Streaming multiprocessors of the current device (148 on B200; also the value
+// used when no device is visible, e.g. when only sizes are being computed).
+inline int sm_count() {
+  int dev = 0, n = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+    cudaGetLastError();
+    return 148;
+  }
+  return n;
+}
 
 inline Launch plan(const lbm_desc& d, int tx) {
   Launch L{};
@@ -60,6 +75,15 @@ inline Launch plan(const lbm_desc& d, int tx) {
   L.bc_grid = dim3((maxcells + L.bc_threads - 1) / L.bc_threads, L.nfaces > 0 ? L.nfaces : 1, 1);
   L.bc_blocks = L.nfaces > 0 ? (int)(L.bc_grid.x * L.bc_grid.y) : 0;
   L.flip_blocks = d.pyro ? 2 * 148 : 0;
+  // staged bulk kernel (rows split into kStagedTile tiles, persistent grid): opt-in
+  // with LBM_STAGED=1; on B200 it measured slower than step_bulk (barrier-bound)
+  const char* e = getenv("LBM_STAGED");
+  L.staged = d.nx % kStagedTile == 0 && e && e[0] == '1';
+  if (L.staged) {
+    const long ntiles = (long)(d.nx / kStagedTile) * d.ny * d.nz;
+    const int per_sm = d.precision == LBM_PREC_FP64 ? 1 : 4;
+    L.bulk_blocks = (int)std::min<long>(ntiles, (long)sm_count() * per_sm);
+  }
   return L;
 }
 
@@ -97,7 +121,7 @@ inline size_t scratch_diag_doubles(const Launch& L) {
   return (size_t)kNumDiag * (partial_rows(L) + kStage1Blocks + 1);
 }
 inline size_t scratch_bytes(const Launch& L) {
-  return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes;
+  return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16;
 }
 inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
 inline double* scratch_stage1(lbm_handle* h) {
@@ -108,6 +132,8 @@ inline lbm_side_desc* scratch_sides(lbm_handle* h) {
   const size_t off = (scratch_diag_doubles(h->L) * sizeof(double) + 255) / 256 * 256;
   return (lbm_side_desc*)((char*)h->ptr[LBM_FIELD_SCRATCH] + off);
 }
+// Kernel error flag (bounded waits that timed out), after the side records.
+inline int* scratch_err(lbm_handle* h) { return (int*)(scratch_sides(h) + 6); }
 // Two-stage deterministic reduction of the block partials into scratch_final().
 inline void launch_reduce(lbm_handle* h, cudaStream_t st) {
   reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), partial_rows(h->L), scratch_stage1(h));
@@ -154,6 +180,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;
+  p.err = h->ptr[LBM_FIELD_SCRATCH] ? scratch_err(h) : nullptr;
   p.flags = 0;
   p.partials = h->ptr[LBM_FIELD_SCRATCH] ? scratch_partials(h) : nullptr;
   p.partial_rows = partial_rows(h->L);

@@ -8,7 +8,19 @@ namespace capi {
 template <class Lt, class S, int COLL, int THERM>
 static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const Launch& L = h->L;
-  step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
+  if (L.staged) {
+    using LY = StagedLayout<Lt, S, kStagedTile>;
+    constexpr size_t smem = (size_t)kStagedStages * LY::STAGE_BYTES;
+    static bool attr_set = false;  // one attribute call per process and instantiation
+    if (!attr_set) {
+      cudaFuncSetAttribute(step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages>,
+                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      attr_set = true;
+    }
+    step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages><<<L.bulk_blocks, kStagedTile, smem, st>>>(p);
+  } else {
+    step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
+  }
   if (L.nfaces > 0) {
     p.block_offset = L.bulk_blocks;
     const int4 f01 = make_int4(L.faces[0], L.faces[1], L.faces[2], L.faces[3]);

@@ -258,9 +258,12 @@ int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
   if (!h || !out) return fail(LBM_ERR_ARG, "NULL argument");
   if (!h->diag_valid) return fail(LBM_ERR_ARG, "no diagnostics: call lbm_step with LBM_STEP_DIAG");
   double v[kNumDiag];
+  int err = 0;
   cudaStream_t st = (cudaStream_t)stream;
   LBM_CUDA_TRY(cudaMemcpyAsync(v, scratch_final(h), sizeof(v), cudaMemcpyDeviceToHost, st));
+  LBM_CUDA_TRY(cudaMemcpyAsync(&err, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
   LBM_CUDA_TRY(cudaStreamSynchronize(st));
+  if (err) return fail(LBM_ERR_TIMEOUT, "a staged-load wait in the step kernel timed out; the state is invalid");
   out->mass = v[0]; out->energy = v[1]; out->solid_alpha = v[2]; out->umax = v[3];
   out->Tmin = v[4]; out->Tmax = v[5]; out->nonfinite = v[6]; out->nfluid = v[7];
   out->res_num = v[8]; out->res_den = v[9];

@@ -95,6 +95,7 @@ struct StepParams {
   C* u_out;
   C* T_out;
   float* uprev;
+  int* err;        // set to 1 when a bounded wait gives up
 };
 
 // Per-population storage shifts (FP16 deviation storage); zero otherwise.

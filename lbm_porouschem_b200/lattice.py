@@ -39,6 +39,8 @@ class Lattice:
         self.device = torch.device(device)
         self.stream = stream
         self._desc = cfg.to_desc()
+        import os
+        self._staged_env = os.environ.get("LBM_STAGED", "0")[:1] == "1"
         h = ctypes.c_void_p()
         N.check(self.lib.lbm_create(ctypes.byref(self._desc), ctypes.byref(h)))
         self._h = h
@@ -71,6 +73,11 @@ class Lattice:
     @property
     def mask(self) -> torch.Tensor:
         return self.buf[N.LBM_FIELD_MASK]
+
+    def _staged(self) -> bool:
+        """True if the bulk update uses the shared-memory staged kernel (LBM_STAGED=1, rows a
+        multiple of 128)."""
+        return self.cfg.nx % 128 == 0 and self._staged_env
 
     @property
     def nsteps(self) -> int:
