@@ -30,7 +30,7 @@ sys.path.insert(0, str(ROOT))
 import numpy as np  # noqa: E402
 
 
-def parse():
+def parse(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=600)
@@ -43,7 +43,41 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps for the e2e leg (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
-    return ap.parse_args()
+    return ap.parse_args(argv)
+
+
+# ---------------------------------------------------------------- ranks (replicas, no data-path collective)
+def rank_barrier(world: int) -> None:
+    import torch.distributed as dist
+    if world > 1:
+        dist.barrier()
+
+
+def max_over_ranks(v: float, world: int, device: str) -> float:
+    """Largest per-rank value (the job's time is its slowest replica's)."""
+    if world == 1:
+        return v
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([v], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_mlups(cells_per_rank: int, steps: int, world: int, ms_max: float) -> float:
+    """Whole-job throughput: every rank updates its own lattice ``steps`` times."""
+    return cells_per_rank * steps * world / (ms_max * 1e-3) / 1e6
+
+
+def rank_seed(base: int, rank: int) -> int:
+    """Each replica packs its own geometry."""
+    return base + rank
+
+
+def launches_per_step(cfg) -> int:
+    """Kernels one lbm_step launches: bulk, boundary sides (if any), flip (pyrolysis)."""
+    nbc = sum(1 for s in cfg.sides if s.active)
+    return 1 + (1 if nbc else 0) + (1 if (cfg.thermal != "none" and cfg.pyro) else 0)
 
 
 def make_workload(args, seed):
@@ -151,8 +185,8 @@ def read_traffic(w):
 
 
 # ---------------------------------------------------------------- main
-def main():
-    args = parse()
+def main(argv=None):
+    args = parse(argv)
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -188,25 +222,18 @@ def main():
         dist.init_process_group("nccl", init_method="env://", device_id=torch.device("cuda", local),
                                 timeout=__import__("datetime").timedelta(seconds=300))
 
+    dev = f"cuda:{local}"
+
     def barrier():
-        if world > 1:
-            dist.barrier()
+        rank_barrier(world)
 
-    def max_over_ranks(v: float) -> float:
-        if world == 1:
-            return v
-        t = torch.tensor([v], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    w = make_workload(args, args.seed + rank)
+    w = make_workload(args, rank_seed(args.seed, rank))
     cfg = w.cfg
     stream = torch.cuda.Stream()
     lat = Lattice(cfg, device=f"cuda:{local}", stream=stream)
     lat.set_geometry(w.solid, w.reactive)
     lat.init(**w.init)
     alg_bytes = W.algorithmic_bytes_per_step(cfg, w.solid)
-    nbc = sum(1 for s in cfg.sides if s.active)
 
     # ---- device-resident throughput (value)
     with torch.cuda.stream(stream):
@@ -226,9 +253,9 @@ def main():
     clk = clocks.stop()
     barrier()
     torch.cuda.synchronize()
-    ms_max = max_over_ranks(ms)
-    value = cfg.ncells * args.steps * world / (ms_max * 1e-3) / 1e6
-    launches = args.steps * (2 if nbc else 1)
+    ms_max = max_over_ranks(ms, world, dev)
+    value = job_mlups(cfg.ncells, args.steps, world, ms_max)
+    launches = args.steps * launches_per_step(cfg)
 
     # ---- end to end through the public API (host copies inside the timed region)
     k2 = args.e2e_steps or args.steps
@@ -248,8 +275,8 @@ def main():
     e1.synchronize()
     wall = time.perf_counter() - t0
     ms_e2e = max(e0.elapsed_time(e1), wall * 1e3)
-    ms_e2e = max_over_ranks(ms_e2e)
-    e2e_value = cfg.ncells * k2 * world / (ms_e2e * 1e-3) / 1e6
+    ms_e2e = max_over_ranks(ms_e2e, world, dev)
+    e2e_value = job_mlups(cfg.ncells, k2, world, ms_e2e)
     import ctypes
     from lbm_porouschem_b200 import _native as N
     h2d = 6 * ctypes.sizeof(N.lbm_side_desc)

@@ -1,0 +1,473 @@
+"""Reference-shaped solver classes on the CUDA lattice update.
+
+``LBM2DSolver`` / ``LBM3DSolver`` keep the constructor, the setters that the
+reference's YAML driver calls (src/LBM/app.py:101-602), ``init_simulation``,
+``step``, ``log_info`` and field access (``rho``, ``v``, ``solid``, ``TF.S``,
+``TS.S`` with ``to_numpy``/``from_numpy``) of src/LBM/LBM2D/__init__.py:29-70 and
+src/LBM/LBM3D/__init__.py:11-62, and run every step through the C ABI.
+
+Supported on the CUDA path: constant viscosity (IDEAL_GAS or INCOMPRESSIBLE),
+binary solid masks with halfway bounce-back, body force (Guo), BGK or MRT,
+the conjugate temperature field (one distribution over fluid and solid), the
+single-step pyrolysis model with solid->fluid flip, and NEE boundaries
+(inlet / outlet / wall / symmetric, temperature fixedValue / zeroGradient).
+Features of the reference outside that set raise NotImplementedError with the
+reason instead of silently running something else.
+"""
+from __future__ import annotations
+
+import logging
+from typing import Callable, Optional
+
+import numpy as np
+
+from .config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
+from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, SOURCE_TERM, VISCOSITY_MODEL
+
+_BC_CODE = {BC.periodic: PERIODIC, BC.zeroGradient: ZERO_GRADIENT, BC.fixedValue: FIXED_VALUE}
+_log = logging.getLogger("LBM 2D logger")
+
+
+def _as_array(param, shape, ncomp: int = 0):
+    """init_field semantics (src/LBM/LBM2D/_io.py:37-57): a number fills the field, a str
+    is a text file in Fortran order, an ndarray is used as is."""
+    if isinstance(param, (int, float, np.floating, np.integer)):
+        return np.full(shape, float(param))
+    if isinstance(param, str):
+        return np.reshape(np.loadtxt(param), shape, order="F")
+    a = np.asarray(param, dtype=np.float64)
+    if a.shape != shape:
+        a = a.reshape(shape)
+    return a
+
+
+class Field:
+    """Host-side stand-in for a Taichi field of the reference solver.
+
+    Before ``init_simulation`` it holds the initial values; afterwards
+    ``to_numpy`` returns the current state read back from the GPU."""
+
+    def __init__(self, solver: "_SolverBase", name: str, ncomp: int = 0, init=0.0):
+        self._s = solver
+        self.name = name
+        self.ncomp = ncomp
+        shp = solver._shape + ((ncomp,) if ncomp else ())
+        self._host = np.full(shp, float(init))
+
+    @property
+    def shape(self):
+        return self._s._shape
+
+    def from_numpy(self, a) -> None:
+        if self._s._lat is not None:
+            raise RuntimeError(f"{self.name}: set initial fields before init_simulation()")
+        self._host = np.asarray(a, dtype=np.float64).reshape(self._host.shape).copy()
+
+    def to_numpy(self) -> np.ndarray:
+        return self._s._read_field(self.name, self._host)
+
+    def fill(self, v) -> None:
+        self.from_numpy(np.full(self._host.shape, float(v)))
+
+
+class ScalarFieldView:
+    """TF / TS of the reference (src/LBM/LBM2D/_scalarField.py:5-58): normalisation and
+    per-side boundary settings of one temperature field."""
+
+    def __init__(self, solver: "_SolverBase", name: str):
+        self.LBM = solver
+        self.name = name
+        self.S = Field(solver, name)
+        self.v_ref = 0.0
+        self.v_scale = 1.0
+        self.BC = [BC.periodic] * solver._nsides
+        self.s_BC = [0.0] * solver._nsides
+        self.thermal_diff = 3e-5
+
+    def get_physical_value(self, v):
+        return v * self.v_scale + self.v_ref
+
+    def get_normalized_value(self, v_phys):
+        return (v_phys - self.v_ref) / self.v_scale
+
+    def set_BC(self, i, bc):
+        self.BC[i] = bc
+
+    def set_BCs(self, bcs):
+        for i, b in enumerate(bcs):
+            self.set_BC(i, b)
+
+    def set_s_BC_value(self, i, s):
+        self.s_BC[i] = self.get_normalized_value(s)
+
+
+class _SolverBase:
+    DIM = 2
+
+    def __init__(self, X, Y, Z, dx=1, dt=1, name="default_LBM", isThermal=False, isChemical=False,
+                 isPoro=False, isRadiation=False):
+        self.name = name
+        self.X, self.Y, self.Z = X, Y, Z
+        self.dx, self.dt = dx, dt
+        self.nx = int(X / dx)
+        self.ny = int(Y / dx)
+        self.nz = int(Z / dx) if self.DIM == 3 else 1
+        self._shape = (self.nx, self.ny, self.nz)
+        self._nsides = 4 if self.DIM == 2 else 6
+        self.t = 0.0
+        self.tLattice: int = 0
+        self.tol = 1e-6
+        self.TEMPERATURE = bool(isThermal)
+        self.CHEMISTRY = bool(isChemical)
+        self.PORO = bool(isPoro)
+        self.RADIATION = bool(isRadiation and isThermal)
+        self.viscosity_model = VISCOSITY_MODEL.NONE
+        self.visco = 2e-5
+        self.source_term_model = SOURCE_TERM.NONE
+        self.force_term_model = FORCE_TERM.NONE
+        self.boundary_condition_model = BC_MODEL.NEE
+        self.EOS = FLUID_STATE_EQUATION.IDEAL_GAS
+        self.collision = "bgk"
+        self.precision = "fp32"
+        self.body_force = (0.0, 0.0, 0.0)
+        self.half_force_velocity = False
+        # reference behaviour switches (default: the fixed behaviour)
+        self.ref_quirk_nee_on_periodic = False
+        self.bc = [BC_FLOW.periodic] * self._nsides
+        self.bc_v = [BC.periodic] * self._nsides
+        self.bc_rho = [BC.periodic] * self._nsides
+        self.v_BC = [(0.0, 0.0, 0.0)] * self._nsides
+        self.rho_BC = [1.0] * self._nsides
+        self.flow_BC = [0.0] * self._nsides
+        self.UpdateBCfunc: list[Callable] = []
+        self.GetVariableFunc: list[Callable] = []
+        self.exportPath = "vtk"
+        self.snapshotPath = "snapshot.yaml"
+        self.rho = Field(self, "rho", 0, 1.0)
+        self.v = Field(self, "v", 3, 0.0)
+        self.solid = Field(self, "solid", 0, 0.0)
+        self.rhos = Field(self, "rhos", 0, 0.0)
+        self.TF = ScalarFieldView(self, "TF")
+        self.TS = ScalarFieldView(self, "TS")
+        self._pyro: Optional[dict] = None
+        self._reactive: Optional[np.ndarray] = None
+        self._lat = None
+
+    # ------------------------------------------------------------ reference dunders
+    def __repr__(self):
+        return self.__str__()
+
+    def __str__(self):
+        return self.description()
+
+    def __call__(self):
+        print(self)
+
+    def description(self) -> str:
+        d = f"{self.name}: {self.nx} x {self.ny} x {self.nz} lattice, dx={self.dx}, dt={self.dt}\n"
+        d += f"  collision {self.collision.upper()}, storage {self.precision}, viscosity (LU) {self._nu_lu():.6g}\n"
+        d += f"  thermal {'conjugate' if self.TEMPERATURE else 'off'}, pyrolysis {'on' if self._pyro else 'off'}\n"
+        return d
+
+    # ------------------------------------------------------------ setters (src/LBM/LBM2D/_io.py)
+    def set_vtk_path(self, path):
+        self.exportPath = path
+
+    def init_field(self, field: Field, param):
+        field.from_numpy(_as_array(param, self._shape))
+
+    def init_field3(self, field: Field, p1, p2, p3):
+        comps = [_as_array(p, self._shape) for p in (p1, p2, p3)]
+        field.from_numpy(np.stack(comps, axis=-1))
+
+    def add_solid(self, solid):
+        s = self.solid._host + np.asarray(solid, dtype=np.float64).reshape(self._shape)
+        self.solid.from_numpy(s)
+
+    def add_rho_solid(self, rhos):
+        self.rhos.from_numpy(self.rhos._host + np.asarray(rhos, dtype=np.float64).reshape(self._shape))
+
+    def set_viscosity(self, mu):
+        self.visco = mu
+        self.viscosity_model = VISCOSITY_MODEL.CONSTANT
+
+    def set_viscosity_sutherland(self, As, Ts):
+        raise NotImplementedError("Sutherland viscosity is not on the CUDA path (constant viscosity only)")
+
+    def set_viscosity_mixture(self):
+        raise NotImplementedError("mixture viscosity needs species transport, which is not on the CUDA path")
+
+    def set_fluid_Trange(self, Trange):
+        self.TF.v_ref, self.TF.v_scale = Trange[0], Trange[1] - Trange[0]
+
+    def set_solid_Trange(self, Trange):
+        self.TS.v_ref, self.TS.v_scale = Trange[0], Trange[1] - Trange[0]
+
+    def set_fluid_thermal_diff(self, diff):
+        self.TF.thermal_diff = diff
+
+    def set_solid_thermal_diff(self, diff):
+        self.TS.thermal_diff = diff
+
+    def set_fluid_Prandtl(self, Pr):
+        self.TF.thermal_diff = self.visco / Pr
+
+    def set_BC(self, i, bc):
+        """Flow side type (src/LBM/LBM2D/_io.py:385-402)."""
+        self.bc[i] = bc
+        if bc == BC_FLOW.inlet or bc == BC_FLOW.inlet_flow or bc == BC_FLOW.wall:
+            self.bc_v[i], self.bc_rho[i] = BC.fixedValue, BC.zeroGradient
+        elif bc == BC_FLOW.outlet:
+            self.bc_v[i], self.bc_rho[i] = BC.zeroGradient, BC.fixedValue
+        elif bc == BC_FLOW.symmetric:
+            self.bc_v[i], self.bc_rho[i] = BC.zeroGradient, BC.zeroGradient
+        if bc == BC_FLOW.wall:
+            self.v_BC[i] = (0.0, 0.0, 0.0)
+        if bc == BC_FLOW.inlet_flow:
+            raise NotImplementedError("flow-rate inlets (updateBC_kernel) are not on the CUDA path")
+
+    def set_BCs(self, bcs):
+        for i, b in enumerate(bcs):
+            self.set_BC(i, b)
+
+    def set_v_BC(self, i, bc):
+        self.bc_v[i] = bc
+
+    def set_rho_BC(self, i, bc):
+        self.bc_rho[i] = bc
+
+    def set_v_BC_value(self, i, v):
+        v = tuple(float(x) for x in (v if np.ndim(v) else (v, 0.0, 0.0)))
+        self.v_BC[i] = (v + (0.0, 0.0, 0.0))[:3]
+        self._push_sides()
+
+    def set_rho_BC_value(self, i, r):
+        self.rho_BC[i] = float(r)
+        self._push_sides()
+
+    def set_flow_BC_value(self, i, f):
+        self.flow_BC[i] = float(f)
+
+    def set_TF_BC(self, i, bc):
+        self.TF.set_BC(i, bc)
+
+    def set_TF_BC_value(self, i, T):
+        self.TF.set_s_BC_value(i, T)
+        self._push_sides()
+
+    def set_TS_BC(self, i, bc):
+        self.TS.set_BC(i, bc)
+
+    def set_TS_BC_value(self, i, T):
+        self.TS.set_s_BC_value(i, T)
+
+    def set_heat_exchange_surface(self, surface):
+        pass  # the conjugate field exchanges heat through the interface itself
+
+    def set_heat_exchange_coef(self, coef):
+        pass
+
+    def set_poro_Darcy(self, s, coefDarcy):
+        raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
+
+    def set_poro_Darcy_Forchheimer(self, s, coefDarcy, coefForchheimer):
+        raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
+
+    def set_specie(self, *a, **k):
+        raise NotImplementedError("species transport is not on the CUDA path; use set_pyrolysis()")
+
+    def add_reaction(self, *a, **k):
+        raise NotImplementedError("general reaction networks are not on the CUDA path; use set_pyrolysis()")
+
+    def load_cantera(self, file):
+        raise NotImplementedError("Cantera mechanisms are not on the CUDA path; use set_pyrolysis()")
+
+    def load_stl(self, *a, **k):
+        raise NotImplementedError("STL voxelisation is not on the CUDA path; pass a solid mask to add_solid()")
+
+    # ------------------------------------------------------------ new settings of the CUDA path
+    def set_body_force(self, g, half_force_velocity: bool = True):
+        """Constant body acceleration (lattice units); u includes F/2 by default."""
+        self.body_force = tuple(float(x) for x in g) + (0.0,) * (3 - len(g))
+        self.half_force_velocity = half_force_velocity
+        self.force_term_model = FORCE_TERM.GUO
+
+    def set_collision(self, model: str):
+        self.collision = model.lower()
+
+    def set_precision(self, precision: str):
+        self.precision = precision.lower()
+
+    def set_pyrolysis(self, A=1e8, Ea=1.25e5, b=0.0, dH=4e5, capacity=1000.0, rho_solid=1.0,
+                      char_yield=0.25, alpha_flip=0.01, Tmin=0.0, reactive=None):
+        """Single-step pyrolysis of reactive solid cells: rate A (T+1e-6)^b exp(-Ea/(R T)) at the
+        cell temperature (K), endothermic dH (J/kg), gas fraction 1 - char_yield released to
+        the fluid, the cell turns fluid below reactive fraction ``alpha_flip``.  ``reactive``:
+        mask of reactive cells (default: every solid cell)."""
+        if not self.TEMPERATURE:
+            raise ValueError("pyrolysis needs the temperature field (isThermal=True)")
+        self._pyro = dict(A=A, Ea=Ea, b=b, dH=dH, capacity=capacity, rho_solid=rho_solid,
+                          char_yield=char_yield, alpha_flip=alpha_flip, Tmin=Tmin)
+        if reactive is not None:
+            self._reactive = np.asarray(reactive, dtype=bool).reshape(self._shape)
+
+    # ------------------------------------------------------------ configuration
+    def _nu_lu(self) -> float:
+        return self.visco * self.dt / self.dx ** 2
+
+    def _tau_T(self, diff) -> float:
+        D = diff * self.dt / self.dx ** 2
+        return (3.0 if self.DIM == 2 else 4.0) * D + 0.5   # _scalarField.py:56-58 (2D/3D)
+
+    def _sides(self) -> list:
+        sides = [SideBC() for _ in range(6)]
+        for i in range(self._nsides):
+            vt, rt, Tt = _BC_CODE[self.bc_v[i]], _BC_CODE[self.bc_rho[i]], _BC_CODE[self.TF.BC[i]]
+            if not self.TEMPERATURE:
+                Tt = PERIODIC
+            if self.boundary_condition_model == BC_MODEL.NONE:
+                active = False
+            elif self.boundary_condition_model == BC_MODEL.NEE:
+                active = self.ref_quirk_nee_on_periodic or (vt, rt, Tt) != (PERIODIC, PERIODIC, PERIODIC)
+            else:
+                raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path (NEE only)")
+            sides[i] = SideBC(active, vt, rt, Tt, self.v_BC[i], self.rho_BC[i], self.TF.s_BC[i])
+        return sides
+
+    def _config(self) -> LatticeConfig:
+        if self.viscosity_model not in (VISCOSITY_MODEL.CONSTANT, VISCOSITY_MODEL.NONE):
+            raise NotImplementedError(f"{self.viscosity_model} is not on the CUDA path")
+        cfg = LatticeConfig(
+            dim=self.DIM, nx=self.nx, ny=self.ny, nz=self.nz, collision=self.collision, precision=self.precision,
+            eos="ideal_gas" if self.EOS == FLUID_STATE_EQUATION.IDEAL_GAS else "incompressible",
+            nu=self._nu_lu(), force=self.body_force, half_force_velocity=self.half_force_velocity,
+            thermal="conjugate" if self.TEMPERATURE else "none", sides=self._sides())
+        if self.TEMPERATURE:
+            cfg.tauT_fluid = self._tau_T(self.TF.thermal_diff)
+            cfg.tauT_solid = self._tau_T(self.TS.thermal_diff)
+            cfg.T_ref, cfg.T_scale = self.TF.v_ref, self.TF.v_scale
+        if self._pyro:
+            pz = self._pyro
+            cfg.pyro = True
+            cfg.pyro_A, cfg.pyro_Ea, cfg.pyro_b, cfg.pyro_Tmin = pz["A"], pz["Ea"], pz["b"], pz["Tmin"]
+            cfg.dt_phys = self.dt
+            cfg.heat_norm = pz["dH"] / (pz["capacity"] * cfg.T_scale)
+            cfg.gas_coef = (1.0 - pz["char_yield"]) * pz["rho_solid"]
+            cfg.alpha_flip = pz["alpha_flip"]
+        return cfg
+
+    # ------------------------------------------------------------ run
+    def init_simulation(self, device: str = "cuda"):
+        """Equilibrium initialisation (src/LBM/LBM2D/_initialize.py:16-65) on the GPU."""
+        from .lattice import Lattice
+        s = self.solid._host
+        if np.any((s > 0) & (s < 1)):
+            raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
+        solid = s >= 1
+        cfg = self._config()
+        reactive = None
+        if cfg.pyro:
+            reactive = solid if self._reactive is None else (self._reactive & solid)
+        self._cfg = cfg
+        self._lat = Lattice(cfg, device=device)
+        self._lat.set_geometry(solid, reactive)
+        u = np.moveaxis(self.v._host, -1, 0)
+        self._lat.init(rho=self.rho._host, u=u, T=self.TF.S._host if self.TEMPERATURE else 0.0)
+        self._cache = None
+        self._cache_step = -1
+
+    def updateBC(self, t):
+        for func in self.UpdateBCfunc:
+            func(self, t)
+
+    def step(self):
+        """One lattice step (src/LBM/LBM2D/_evolution.py:12-15)."""
+        if self._lat is None:
+            raise RuntimeError("call init_simulation() first")
+        self.updateBC(self.t)
+        self._lat.step(1)
+        self.tLattice += 1
+        self.t = self.tLattice * self.dt
+
+    def _push_sides(self):
+        if getattr(self, "_lat", None) is not None:
+            self._lat.set_sides(self._sides())
+
+    def _state(self) -> dict:
+        if self._cache_step != self._lat.nsteps:
+            self._cache = self._lat.fields()
+            self._cache_step = self._lat.nsteps
+        return self._cache
+
+    def _read_field(self, name: str, host: np.ndarray) -> np.ndarray:
+        if self._lat is None:
+            return host.copy()
+        st = self._state()
+        if name == "rho":
+            out = host.copy()
+            fl = ~st["solid"]
+            out[fl] = st["rho"][fl]
+            return out
+        if name == "v":
+            out = host.copy()
+            fl = ~st["solid"]
+            out[fl] = np.moveaxis(st["u"], 0, -1)[fl]
+            out[~fl] = 0.0
+            return out
+        if name == "solid":
+            return st["solid"].astype(np.float64)
+        if name in ("TF", "TS"):
+            return st["T"].copy()
+        return host.copy()
+
+    # ------------------------------------------------------------ output (src/LBM/LBM2D/_io.py:538-598)
+    def _diag(self) -> dict:
+        if self._lat is None or self._lat.nsteps == 0:
+            fl = self.solid._host < 1
+            u = np.linalg.norm(self.v._host, axis=-1)
+            T = self.TF.S._host
+            return {"umax": float(u[fl].max(initial=0.0)), "Tmin": float(T.min()), "Tmax": float(T.max())}
+        return self._lat.diagnostics()
+
+    def get_max_v(self):
+        return self._diag()["umax"]
+
+    def get_max_T(self):
+        return self.TF.get_physical_value(self._diag()["Tmax"]) if self.TEMPERATURE else -1
+
+    def get_min_T(self):
+        return self.TF.get_physical_value(self._diag()["Tmin"]) if self.TEMPERATURE else -1
+
+    def log_info(self) -> str:
+        d = self._diag()
+        p = f"    t(LU)={self.tLattice} : Max velocity magnitude (LU) : {d['umax']:.7f}, "
+        if self.TEMPERATURE:
+            p += (f"Min temperature: {self.TF.get_physical_value(d['Tmin']):.7f} K, "
+                  f"Max temperature : {self.TF.get_physical_value(d['Tmax']):.7f}")
+        return p
+
+    def export_snapshot(self, config=None):
+        pass  # the reference's snapshot export is a no-op too (src/LBM/LBM2D/_io.py:589-598)
+
+    def check_python(self):
+        pass
+
+    def export_VTK_pyvista(self):
+        raise NotImplementedError("VTK export (pyvista) is not on the CUDA path; read fields with to_numpy()")
+
+    def close(self):
+        if self._lat is not None:
+            self._lat.close()
+            self._lat = None
+
+
+class LBM2DSolver(_SolverBase):
+    """2D solver (D2Q9 flow + D2Q5 temperature) with the reference constructor
+    (src/LBM/LBM2D/__init__.py:65-70)."""
+    DIM = 2
+
+
+class LBM3DSolver(_SolverBase):
+    """3D solver (D3Q19 flow + D3Q7 temperature) with the reference constructor
+    (src/LBM/LBM3D/__init__.py:11-62)."""
+    DIM = 3

@@ -1,0 +1,128 @@
+"""YAML case driver: geometry voxelisation and case building (CPU), a short run (GPU)."""
+import logging
+
+import numpy as np
+import pytest
+import yaml
+
+from lbm_porouschem_b200.app import _centres, build_case, voxelise
+from lbm_porouschem_b200.config import FIXED_VALUE, ZERO_GRADIENT
+
+CASE2D = """
+basic:
+  name: channel_pyro
+  dimension: 2
+  arch: gpu
+  collision: mrt
+module:
+  temperature: true
+  chemistry: true
+spaceControl:
+  geometry: [0.096, 0.032]
+  DX: 1.0e-3
+timeControl:
+  startTime: 0
+  endTime: 0.002
+  DT: 1.0e-4
+flowProperties:
+  viscosity: {type: constant, value: 2.0e-5}
+thermalPropertiesFluid:
+  normalize: {Trange: [300, 800]}
+  thermalDiff: {type: constant, value: 3.0e-5}
+thermalPropertiesSolid:
+  normalize: {Trange: [300, 800]}
+  thermalDiff: {type: constant, value: 1.0e-5}
+chemicalProperties:
+  type: pyrolysis
+  zone: [grain]
+  A: 1.0e8
+  Ea: 1.25e5
+geometry:
+  grain: {type: sphere, center: [0.03, 0.016, 0], radius: 0.006}
+  post: {type: box, center: [0.06, 0.016, 0], size: [0.008, 0.01, 0.01]}
+initialCondition:
+  flow: {rho: 1, velocity: [0, 0, 0]}
+  thermal: {T: 300}
+  solid:
+    s1: {zone: ALL, type: concrete}
+boundaryCondition:
+  left:
+    flow: {type: inlet, velocity: [0.01, 0, 0]}
+    thermalFluid: {type: fixedValue, value: 800}
+  right:
+    flow: {type: outlet, rho: 1}
+    thermalFluid: {type: zeroGradient}
+  down:
+    flow: {type: wall}
+  up:
+    flow: {type: wall}
+outputControl:
+  log: {interval: 5.0e-4}
+"""
+
+
+def _log():
+    lg = logging.getLogger("test_app")
+    lg.setLevel(logging.WARNING)
+    return lg
+
+
+def test_voxelise_shapes_3d():
+    dx = 1.0
+    g = _centres(40, 40, 40, dx, 3)
+    sph = voxelise({"type": "sphere", "center": [20, 20, 20], "radius": 10}, g, dx)
+    assert abs(sph.sum() - 4 / 3 * np.pi * 1000) / (4 / 3 * np.pi * 1000) < 0.03
+    cyl = voxelise({"type": "cylinder", "center": [20, 20, 20], "radius": 8, "height": 20, "axis": [1, 0, 0]}, g, dx)
+    assert abs(cyl.sum() - np.pi * 64 * 20) / (np.pi * 64 * 20) < 0.05
+    assert cyl[20, 20, 27] == 1 and cyl[20, 20, 29] == 0 and cyl[31, 20, 20] == 0
+    cone = voxelise({"type": "cone", "center": [20, 20, 20], "radius": 10, "height": 20}, g, dx)
+    assert abs(cone.sum() - np.pi * 100 * 20 / 3) / (np.pi * 100 * 20 / 3) < 0.08
+    assert cone[20, 20, 11] == 1 and cone[28, 20, 11] == 1 and cone[28, 20, 28] == 0
+    box = voxelise({"type": "box", "center": [20, 20, 20], "size": [10, 6, 4]}, g, dx)
+    assert box.sum() == 10 * 6 * 4
+    with pytest.raises(NotImplementedError):
+        voxelise({"type": "stl", "path": "x.stl"}, g, dx)
+
+
+def test_build_case_from_yaml():
+    cfg = yaml.safe_load(CASE2D)
+    lb = build_case(cfg, _log())
+    assert (lb.nx, lb.ny, lb.nz) == (96, 32, 1)
+    c = lb._config()
+    assert c.collision == "mrt" and c.thermal == "conjugate" and c.pyro
+    s = lb.solid.to_numpy()
+    assert s.max() == 1.0 and abs(s.sum() - (np.pi * 36 + 8 * 10)) < 12
+    # reactive cells: only the sphere zone
+    assert lb._reactive.sum() == pytest.approx(np.pi * 36, abs=8)
+    assert not lb._reactive[60, 16, 0] and s[60, 16, 0] == 1
+    sd = c.sides
+    assert sd[0].v_type == FIXED_VALUE and sd[0].v == (0.01, 0.0, 0.0) and sd[0].T == pytest.approx(1.0)
+    assert sd[1].rho_type == FIXED_VALUE and sd[1].T_type == ZERO_GRADIENT
+    assert sd[2].active and sd[3].active
+    assert np.all(lb.TF.S.to_numpy() == 0.0)                         # 300 K normalised
+
+
+def test_unsupported_options_stop_the_run():
+    cfg = yaml.safe_load(CASE2D)
+    cfg["chemicalProperties"] = {"type": "cantera", "canteraFile": "mech.yaml"}
+    with pytest.raises(NotImplementedError):
+        build_case(cfg, _log())
+    cfg = yaml.safe_load(CASE2D)
+    cfg["initialCondition"]["solid"]["s1"]["type"] = "poro"
+    with pytest.raises(NotImplementedError):
+        build_case(cfg, _log())
+
+
+@pytest.mark.gpu
+def test_cli_runs_case(tmp_path, monkeypatch):
+    from lbm_porouschem_b200.cli import run
+    cfg = yaml.safe_load(CASE2D)
+    cfg["outputControl"]["vtk"] = {"interval": 1.0e-3, "path": str(tmp_path / "out")}
+    p = tmp_path / "case.yaml"
+    p.write_text(yaml.safe_dump(cfg))
+    monkeypatch.chdir(tmp_path)
+    assert run(["-c", str(p), "-v", "0"]) == 0
+    files = sorted((tmp_path / "out").glob("*.npz"))
+    assert len(files) == 3                                           # t = 0, 10, 20
+    d = np.load(files[-1])
+    assert np.isfinite(d["rho"]).all() and d["T"].max() > 300.0     # the hot inlet has warmed the fluid

@@ -1,0 +1,158 @@
+"""Reference-shaped solver surface: setter -> lattice configuration mapping (CPU) and
+stepping through the CUDA path (GPU)."""
+import numpy as np
+import pytest
+
+from lbm_porouschem_b200 import LatticeConfig, SideBC
+from lbm_porouschem_b200.config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT
+from lbm_porouschem_b200.flag import BC, BC_FLOW, BC_MODEL
+from lbm_porouschem_b200.solver import LBM2DSolver, LBM3DSolver
+
+
+def _channel2d():
+    s = LBM2DSolver(X=0.064, Y=0.032, Z=0.0, dx=1e-3, dt=1e-4, name="channel", isThermal=True)
+    s.set_viscosity(2e-5)
+    s.set_fluid_Trange([300.0, 800.0])
+    s.set_solid_Trange([300.0, 800.0])
+    s.set_fluid_thermal_diff(3e-5)
+    s.set_solid_thermal_diff(1e-5)
+    s.set_BC(0, BC_FLOW.inlet)
+    s.set_BC(1, BC_FLOW.outlet)
+    s.set_BC(2, BC_FLOW.wall)
+    s.set_BC(3, BC_FLOW.wall)
+    s.set_v_BC_value(0, [0.01, 0.0])
+    s.set_rho_BC_value(1, 1.0)
+    s.set_TF_BC(0, BC.fixedValue)
+    s.set_TF_BC_value(0, 800.0)
+    s.set_TF_BC(1, BC.zeroGradient)
+    return s
+
+
+def test_grid_from_physical_size():
+    s = LBM3DSolver(X=0.02, Y=0.01, Z=0.005, dx=1e-3)
+    assert (s.nx, s.ny, s.nz) == (20, 10, 5)
+    s2 = LBM2DSolver(X=64, Y=32, Z=0)
+    assert (s2.nx, s2.ny, s2.nz) == (64, 32, 1)
+
+
+def test_setters_map_to_lattice_config():
+    s = _channel2d()
+    cfg = s._config()
+    assert isinstance(cfg, LatticeConfig)
+    assert (cfg.dim, cfg.nx, cfg.ny, cfg.nz) == (2, 64, 32, 1)
+    assert cfg.nu == pytest.approx(2e-5 * 1e-4 / 1e-6)             # visco dt / dx^2
+    assert cfg.tau() == pytest.approx(3 * cfg.nu + 0.5)
+    # D2Q5: tau = 3 D + 1/2 with D = diff dt / dx^2 (src/LBM/LBM2D/_scalarField.py tau)
+    assert cfg.tauT_fluid == pytest.approx(3 * 3e-5 * 1e-4 / 1e-6 + 0.5)
+    assert cfg.tauT_solid == pytest.approx(3 * 1e-5 * 1e-4 / 1e-6 + 0.5)
+    assert (cfg.T_ref, cfg.T_scale) == (300.0, 500.0)
+    sd = cfg.sides
+    assert sd[0].active and sd[0].v_type == FIXED_VALUE and sd[0].rho_type == ZERO_GRADIENT
+    assert sd[0].v == (0.01, 0.0, 0.0)
+    assert sd[0].T_type == FIXED_VALUE and sd[0].T == pytest.approx(1.0)   # (800 - 300) / 500
+    assert sd[1].active and sd[1].v_type == ZERO_GRADIENT and sd[1].rho_type == FIXED_VALUE
+    assert sd[1].T_type == ZERO_GRADIENT
+    assert sd[2].active and sd[2].v == (0.0, 0.0, 0.0) and sd[2].v_type == FIXED_VALUE
+    assert not sd[4].active and not sd[5].active                       # 2D: no z sides
+
+
+def test_3d_thermal_tau_and_periodic_sides():
+    s = LBM3DSolver(X=16, Y=8, Z=8, dx=1, dt=1, isThermal=True)
+    s.set_viscosity(0.1)
+    s.set_fluid_thermal_diff(0.05)
+    s.set_solid_thermal_diff(0.1)
+    s.set_BC(0, BC_FLOW.inlet)
+    s.set_v_BC_value(0, [0.02, 0.0, 0.0])
+    cfg = s._config()
+    assert cfg.tauT_fluid == pytest.approx(4 * 0.05 + 0.5)              # D3Q7: 4 D + 1/2
+    assert cfg.tauT_solid == pytest.approx(4 * 0.1 + 0.5)
+    assert [x.active for x in cfg.sides] == [True, False, False, False, False, False]
+    s.ref_quirk_nee_on_periodic = True                                 # reference applies NEE on all sides
+    assert all(x.active for x in s._config().sides)
+    s.boundary_condition_model = BC_MODEL.NONE
+    assert not any(x.active for x in s._config().sides)
+
+
+def test_prandtl_and_pyrolysis_mapping():
+    s = LBM3DSolver(X=0.008, Y=0.008, Z=0.008, dx=1e-3, dt=1e-4, isThermal=True)
+    s.set_viscosity(2e-5)
+    s.set_fluid_Prandtl(0.7)
+    assert s._config().tauT_fluid == pytest.approx(4 * (2e-5 * 1e-4 / 1e-6) / 0.7 + 0.5)
+    s.set_fluid_Trange([300.0, 800.0])
+    s.set_pyrolysis(A=1e8, Ea=1.25e5, dH=4e5, capacity=1000.0, char_yield=0.25, alpha_flip=0.02)
+    cfg = s._config()
+    assert cfg.pyro and cfg.pyro_A == 1e8 and cfg.pyro_Ea == 1.25e5 and cfg.dt_phys == 1e-4
+    assert cfg.heat_norm == pytest.approx(4e5 / (1000.0 * 500.0))
+    assert cfg.gas_coef == pytest.approx(0.75) and cfg.alpha_flip == 0.02
+    with pytest.raises(ValueError):
+        LBM2DSolver(X=8, Y=8, Z=0).set_pyrolysis()                    # needs the temperature field
+
+
+def test_unsupported_features_raise():
+    s = LBM2DSolver(X=8, Y=8, Z=0)
+    with pytest.raises(NotImplementedError):
+        s.set_viscosity_sutherland(1.0, 1.0)
+    with pytest.raises(NotImplementedError):
+        s.load_cantera("gri30.yaml")
+    with pytest.raises(NotImplementedError):
+        s.set_BC(0, BC_FLOW.inlet_flow)
+    s.boundary_condition_model = BC_MODEL.NEBB
+    s.set_BC(0, BC_FLOW.outlet)
+    with pytest.raises(NotImplementedError):
+        s._config()
+
+
+def test_init_field_forms(tmp_path):
+    s = LBM2DSolver(X=6, Y=4, Z=0)
+    s.init_field(s.rho, 1.02)
+    assert np.all(s.rho.to_numpy() == 1.02)
+    a = np.arange(24, dtype=np.float64).reshape(6, 4, 1)
+    p = tmp_path / "rho.txt"
+    np.savetxt(p, a.flatten(order="F"))
+    s.init_field(s.rho, str(p))
+    assert np.array_equal(s.rho.to_numpy(), a)
+    s.init_field3(s.v, 0.01, a, 0.0)
+    v = s.v.to_numpy()
+    assert v.shape == (6, 4, 1, 3) and np.all(v[..., 0] == 0.01) and np.array_equal(v[..., 1], a)
+    s.add_solid(np.ones((6, 4, 1)) * (a > 20))
+    assert s.solid.to_numpy().sum() == 3
+    assert "6 x 4 x 1" in s.description()
+    assert "t(LU)=0" in s.log_info()
+
+
+@pytest.mark.gpu
+def test_solver_steps_like_lattice():
+    """The solver is a thin front: stepping it equals stepping a Lattice configured directly."""
+    from lbm_porouschem_b200 import Lattice
+    s = _channel2d()
+    rng = np.random.default_rng(3)
+    solid = np.zeros((64, 32, 1))
+    solid[20:28, 10:18] = 1.0
+    s.add_solid(solid)
+    T0 = 300.0 + 100.0 * rng.random((64, 32, 1))
+    s.init_field(s.TF.S, (T0 - 300.0) / 500.0)
+    s.init_field(s.rho, 1.0)
+    s.init_simulation()
+    for _ in range(50):
+        s.step()
+    got = {"rho": s.rho.to_numpy(), "v": s.v.to_numpy(), "T": s.TF.S.to_numpy()}
+
+    cfg = LatticeConfig(dim=2, nx=64, ny=32, nz=1, nu=2e-5 * 1e-4 / 1e-6, thermal="conjugate",
+                        tauT_fluid=3 * 3e-5 * 1e-4 / 1e-6 + 0.5, tauT_solid=3 * 1e-5 * 1e-4 / 1e-6 + 0.5,
+                        T_ref=300.0, T_scale=500.0,
+                        sides=[SideBC.inlet((0.01, 0.0, 0.0), FIXED_VALUE, 1.0),
+                               SideBC.outlet(1.0, ZERO_GRADIENT, 0.0),
+                               SideBC.wall(PERIODIC), SideBC.wall(PERIODIC), SideBC(), SideBC()])
+    lat = Lattice(cfg)
+    lat.set_geometry(solid >= 1)
+    lat.init(rho=1.0, u=(0.0, 0.0, 0.0), T=(T0 - 300.0) / 500.0)
+    lat.step(50)
+    ref = lat.fields()
+    fl = ~ref["solid"]
+    np.testing.assert_array_equal(got["rho"][fl], ref["rho"][fl])
+    np.testing.assert_array_equal(got["v"][fl], np.moveaxis(ref["u"], 0, -1)[fl])
+    np.testing.assert_array_equal(got["T"], ref["T"])
+    assert s.tLattice == 50 and s.t == pytest.approx(50 * 1e-4)
+    assert "Max velocity magnitude" in s.log_info()
+    s.close()
+    lat.close()
