@@ -233,7 +233,9 @@ def main(argv=None):
     lat = Lattice(cfg, device=f"cuda:{local}", stream=stream)
     lat.set_geometry(w.solid, w.reactive)
     lat.init(**w.init)
-    alg_bytes = W.algorithmic_bytes_per_step(cfg, w.solid)
+    bpl = W.bytes_per_lattice_update(cfg)
+    alg_bytes = bpl * cfg.ncells                       # per step, every cell updated once
+    sparse_bytes = W.algorithmic_bytes_per_step(cfg, w.solid)
 
     # ---- device-resident throughput (value)
     with torch.cuda.stream(stream):
@@ -303,9 +305,12 @@ def main(argv=None):
             "config": {**describe(w, args), "parallelism": f"replicas x{world}"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": traffic,
-                         "algorithmic_bytes_per_step": alg_bytes,
-                         "bytes_per_lu": round(alg_bytes / cfg.ncells, 2),
-                         "note": f"step kernels (bulk + boundary) per step; peak {peak_src}"},
+                         "algorithmic_bytes_per_step": alg_bytes, "bytes_per_lu": bpl,
+                         "sparse_bytes_per_lu": round(sparse_bytes / cfg.ncells, 2),
+                         "note": f"{bpl} B per lattice update (dense A/B pull count) x cells / device time of "
+                                 f"the whole step (bulk + boundary + flip kernels); peak {peak_src}; "
+                                 f"sparse_bytes_per_lu: lower bound when solid cells carry no flow "
+                                 f"populations; traffic: DRAM bytes per step from ncu"},
             "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS", "h2d_bytes_per_step": h2d,
                     "d2h_bytes_per_step": d2h, "steps": k2},
             "gpu_launches": launches,

@@ -129,7 +129,7 @@ typedef struct lbm_diag {
 #define LBM_FIELD_U 6       /* 3 planes */
 #define LBM_FIELD_T 7
 #define LBM_FIELD_UPREV 8   /* 3 float32 planes, residual reference */
-#define LBM_FIELD_SCRATCH 9 /* reduction partials + control block */
+#define LBM_FIELD_SCRATCH 9 /* reduction partials, control block, cell lists of the bulk update */
 #define LBM_NUM_FIELDS 10
 
 /* lbm_step flags */
@@ -165,7 +165,10 @@ LBM_API int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, vo
  * NULL without thermal), alpha[N] (NULL: 1 on reactive cells), all float32.
  * Compute precision is float32 for FP32/FP16 storage and float64 for FP64.  The solid mask must be bound first.  Replaces init_simulation /
  * init_kernel (src/LBM/LBM2D/_initialize.py:16-65, LBM3D/_initialize.py:17-77).
- * Resets the step counter. */
+ * Resets the step counter and builds the cell lists of the bulk update (in
+ * SCRATCH).  Synchronises `stream` once when a side is active: a solid cell on
+ * an active side or next to one fails with LBM_ERR_ARG (NEE extrapolates from
+ * the inner neighbour, so the two outer layers of an active side must be fluid). */
 LBM_API int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,
                              const float* alpha, void* stream);
 

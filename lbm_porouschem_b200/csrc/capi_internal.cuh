@@ -10,6 +10,7 @@
 #include <cstring>
 #include <string>
 
+#include "list_kernel.cuh"
 #include "staged_kernel.cuh"
 #include "step_kernels.cuh"
 
@@ -42,6 +43,12 @@ struct Launch {
   int bulk_blocks, bc_blocks;
   int flip_blocks;    // grid of flip_cells (pyrolysis only), 256 threads each
   bool staged;        // bulk update by step_bulk_staged (persistent grid of bulk_blocks)
+  bool list;          // bulk update by step_list (persistent grid of bulk_blocks x 128)
+  bool list_stage;    // step_list stages pulled populations in shared memory (FP32/FP64; LBM_LIST_STAGE)
+  size_t N;
+  int list_base;      // first entry of the solid list (capacity of the fluid list)
+  size_t list_cap;    // entries in both lists
+  int list_nbb;       // blocks of the list build
 };
 
 // Streaming multiprocessors of the current device (148 on B200; also the value
@@ -84,6 +91,24 @@ inline Launch plan(const lbm_desc& d, int tx) {
     const int per_sm = d.precision == LBM_PREC_FP64 ? 1 : 4;
     L.bulk_blocks = (int)std::min<long>(ntiles, (long)sm_count() * per_sm);
   }
+  // cell-list bulk kernel from 65536 cells up (below, its start-up round trips
+  // outweigh what it saves); LBM_BULK=tile / list forces either form
+  const char* b = getenv("LBM_BULK");
+  L.N = (size_t)d.nx * d.ny * d.nz;
+  const bool force_tile = b && std::strcmp(b, "tile") == 0, force_list = b && std::strcmp(b, "list") == 0;
+  L.list = !L.staged && !force_tile && (force_list || L.N >= 65536);
+  // staging the pulls in shared memory pays in 2D; in 3D direct loads measured
+  // faster (D3Q19 + D3Q7 + pyrolysis, 256^3: 11.2 against 9.6 GLUPS in FP32)
+  const char* ls = getenv("LBM_LIST_STAGE");
+  L.list_stage = ls ? ls[0] == '1' : d.dim == 2;
+  L.list_base = (int)((L.N + 64 + 31) / 32 * 32);
+  L.list_cap = 2 * (size_t)L.list_base;
+  L.list_nbb = (int)((L.N + kListChunk - 1) / kListChunk);
+  if (L.list) {
+    const int per_sm = d.precision == LBM_PREC_FP64 ? 2 : 4;  // 128-thread blocks at the register cap
+    const long chunks = (long)(L.N / 32) + 8;
+    L.bulk_blocks = (int)std::max<long>(1, std::min<long>((chunks + 3) / 4, (long)sm_count() * per_sm));
+  }
   return L;
 }
 
@@ -120,7 +145,17 @@ inline int partial_rows(const Launch& L) { return L.bulk_blocks + L.bc_blocks + 
 inline size_t scratch_diag_doubles(const Launch& L) {
   return (size_t)kNumDiag * (partial_rows(L) + kStage1Blocks + 1);
 }
+// Cell lists (step_list): header | build blocks [4][nbb] | ent_c | ent_b | pos | flips[2][N],
+// 256-byte aligned after the error flag.
+inline size_t list_offset(const Launch& L) {
+  return ((scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16 + 255) / 256 * 256;
+}
+inline size_t list_bytes(const Launch& L) {
+  if (!L.list) return 0;
+  return (size_t)kLhSlots * 4 + (size_t)4 * L.list_nbb * 4 + 2 * L.list_cap * 4 + L.N * 4 + 2 * L.N * 4;
+}
 inline size_t scratch_bytes(const Launch& L) {
+  if (L.list) return list_offset(L) + list_bytes(L);
   return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16;
 }
 inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
@@ -132,8 +167,15 @@ inline lbm_side_desc* scratch_sides(lbm_handle* h) {
   const size_t off = (scratch_diag_doubles(h->L) * sizeof(double) + 255) / 256 * 256;
   return (lbm_side_desc*)((char*)h->ptr[LBM_FIELD_SCRATCH] + off);
 }
-// Kernel error flag (bounded waits that timed out), after the side records.
+// Kernel error flags after the side records: bit 0 a bounded wait timed out,
+// bit 1 the fluid list overflowed.
 inline int* scratch_err(lbm_handle* h) { return (int*)(scratch_sides(h) + 6); }
+inline int* scratch_lhdr(lbm_handle* h) { return (int*)((char*)h->ptr[LBM_FIELD_SCRATCH] + list_offset(h->L)); }
+inline int* scratch_lblk(lbm_handle* h) { return scratch_lhdr(h) + kLhSlots; }
+inline uint32_t* scratch_ent_c(lbm_handle* h) { return (uint32_t*)(scratch_lblk(h) + 4 * (size_t)h->L.list_nbb); }
+inline uint32_t* scratch_ent_b(lbm_handle* h) { return scratch_ent_c(h) + h->L.list_cap; }
+inline int* scratch_pos(lbm_handle* h) { return (int*)(scratch_ent_b(h) + h->L.list_cap); }
+inline int* scratch_flips(lbm_handle* h) { return scratch_pos(h) + h->N; }
 // Two-stage deterministic reduction of the block partials into scratch_final().
 inline void launch_reduce(lbm_handle* h, cudaStream_t st) {
   reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), partial_rows(h->L), scratch_stage1(h));
@@ -189,6 +231,13 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.u_out = (C*)h->ptr[LBM_FIELD_U];
   p.T_out = (C*)h->ptr[LBM_FIELD_T];
   p.uprev = (float*)h->ptr[LBM_FIELD_UPREV];
+  if (h->L.list && h->ptr[LBM_FIELD_SCRATCH]) {
+    p.lhdr = scratch_lhdr(h);
+    p.ent_c = scratch_ent_c(h);
+    p.ent_b = scratch_ent_b(h);
+    p.pos = scratch_pos(h);
+    p.flips = scratch_flips(h);
+  }
   return p;
 }
 

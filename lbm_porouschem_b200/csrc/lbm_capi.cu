@@ -58,6 +58,56 @@ static int validate(const lbm_desc* d) {
   return LBM_OK;
 }
 
+// Sets bit 2 of *flag if a cell on an active (NEE) side, or its inner neighbour,
+// is solid: NEE replaces every population of a side cell from the post-stream
+// state of the inner neighbour (src/LBM/LBM2D/_boundary.py:54-101), which
+// presumes two fluid cells, and solid cells here carry no flow populations.
+static __global__ void __launch_bounds__(256) check_sides_kernel(const uint8_t* mask, int nx, int ny, int nz,
+                                                                 int active, size_t N, int* flag) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += stride) {
+    if (!(mask[c] & LBM_MASK_SOLID)) continue;
+    const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
+    const bool near = ((active & 1) && x <= 1) || ((active & 2) && x >= nx - 2) || ((active & 4) && y <= 1) ||
+                      ((active & 8) && y >= ny - 2) || ((active & 16) && z <= 1) || ((active & 32) && z >= nz - 2);
+    if (near) atomicOr(flag, 4);
+  }
+}
+
+// Cell lists of the step_list kernel from the (normalised) mask; runs after the
+// equilibrium initialisation, on the caller's stream.
+template <class Lt>
+static int build_lists_t(lbm_handle* h, cudaStream_t st) {
+  ListBuild a{};
+  a.mask = (const uint8_t*)h->ptr[LBM_FIELD_MASK];
+  a.nx = h->d.nx; a.ny = h->d.ny; a.nz = h->d.nz;
+  a.active = 0;
+  for (int s = 0; s < 6; ++s) if (h->d.side[s].active) a.active |= 1 << s;
+  a.par = 0;
+  a.thermal = h->d.thermal;
+  a.N = h->N;
+  a.nbb = h->L.list_nbb;
+  a.blk = scratch_lblk(h);
+  a.hdr = scratch_lhdr(h);
+  a.ent_c = scratch_ent_c(h);
+  a.ent_b = scratch_ent_b(h);
+  a.pos = scratch_pos(h);
+  a.solid_base = h->L.list_base;
+  // padding entries everywhere (cell index 0xffffffff), no entry for any cell (-1)
+  LBM_CUDA_TRY(cudaMemsetAsync(a.ent_c, 0xff, h->L.list_cap * 4, st));
+  LBM_CUDA_TRY(cudaMemsetAsync(a.ent_b, 0xff, h->L.list_cap * 4, st));
+  LBM_CUDA_TRY(cudaMemsetAsync(a.pos, 0xff, h->N * 4, st));
+  list_count<Lt><<<a.nbb, 256, 0, st>>>(a);
+  list_scan<Lt><<<1, 1024, 0, st>>>(a);
+  list_scatter<Lt><<<a.nbb, 256, 0, st>>>(a);
+  LBM_CUDA_TRY(cudaGetLastError());
+  return LBM_OK;
+}
+static int build_lists(lbm_handle* h, cudaStream_t st) {
+  if (!h->L.list) return LBM_OK;
+  return h->d.dim == 2 ? build_lists_t<Lattice<2>>(h, st) : build_lists_t<Lattice<3>>(h, st);
+}
+
 extern "C" {
 
 int32_t lbm_abi_version(void) { return LBM_ABI_VERSION; }
@@ -189,6 +239,27 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
   });
   if (rc) return rc;
   LBM_CUDA_TRY(cudaGetLastError());
+  {
+    int active = 0;
+    for (int s = 0; s < 6; ++s) if (h->d.side[s].active) active |= 1 << s;
+    int flag = 0;
+    LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
+    if (active) {
+      check_sides_kernel<<<2 * sm_count(), 256, 0, st>>>((const uint8_t*)h->ptr[LBM_FIELD_MASK], h->d.nx, h->d.ny,
+                                                        h->d.nz, active, h->N, scratch_err(h));
+      LBM_CUDA_TRY(cudaGetLastError());
+      LBM_CUDA_TRY(cudaMemcpyAsync(&flag, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
+      LBM_CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    if (flag & 4) {
+      LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
+      return fail(LBM_ERR_ARG,
+                  "a solid cell lies on an active (NEE) side or next to one; the two outer layers of an active "
+                  "side must be fluid");
+    }
+  }
+  rc = build_lists(h, st);
+  if (rc) return rc;
   h->step = 0;
   h->diag_valid = false;
   return LBM_OK;
@@ -263,7 +334,8 @@ int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
   LBM_CUDA_TRY(cudaMemcpyAsync(v, scratch_final(h), sizeof(v), cudaMemcpyDeviceToHost, st));
   LBM_CUDA_TRY(cudaMemcpyAsync(&err, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
   LBM_CUDA_TRY(cudaStreamSynchronize(st));
-  if (err) return fail(LBM_ERR_TIMEOUT, "a staged-load wait in the step kernel timed out; the state is invalid");
+  if (err & 1) return fail(LBM_ERR_TIMEOUT, "a staged-load wait in the step kernel timed out; the state is invalid");
+  if (err & 2) return fail(LBM_ERR_CUDA, "the fluid cell list overflowed; the state is invalid");
   out->mass = v[0]; out->energy = v[1]; out->solid_alpha = v[2]; out->umax = v[3];
   out->Tmin = v[4]; out->Tmax = v[5]; out->nonfinite = v[6]; out->nfluid = v[7];
   out->res_num = v[8]; out->res_den = v[9];

@@ -81,6 +81,8 @@ extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) 
   if (!h->ptr[LBM_FIELD_F] || !h->ptr[LBM_FIELD_MASK] || (h->d.thermal && !h->ptr[LBM_FIELD_G]) ||
       (h->d.pyro && (!h->ptr[LBM_FIELD_ALPHA] || !h->ptr[LBM_FIELD_REL])))
     return fail(LBM_ERR_UNBOUND, "lbm_diag_noalloc needs the lattice state (F, MASK, G, ALPHA, REL) bound");
+  if (h->L.list && !h->ptr[LBM_FIELD_SCRATCH])
+    return fail(LBM_ERR_UNBOUND, "lbm_diag_noalloc needs SCRATCH bound: it holds the cell lists of the lattice");
   double* diag = nullptr;
   lbm_side_desc* sides = nullptr;
   int rc = device_arrays(&diag, &sides);

@@ -63,6 +63,15 @@ constexpr int kNumDiag = 10;              // partial slots per block (order of l
 constexpr int kStepPeek = 1 << 8;         // internal flag: recompute outputs, leave the state untouched
 constexpr double kGasConstant = 8.314441; // src/LBM/util/constant.py:17
 
+// Register cap of the FP32/FP16 bulk kernels (FP64 keeps the full budget):
+// 128 registers = 4 blocks of 128 threads (16 warps) per SM.  On B200 at 256^3
+// (D3Q19-MRT + D3Q7 + pyrolysis) 96 and 80 measured no faster.
+#ifndef LBM_BULK_MAXNREG
+#define LBM_BULK_MAXNREG 128
+#endif
+template <class S> struct BulkRegs { static constexpr int v = LBM_BULK_MAXNREG; };
+template <> struct BulkRegs<double> { static constexpr int v = 255; };
+
 template <class S>
 struct StepParams {
   using C = typename Store<S>::C;
@@ -96,6 +105,34 @@ struct StepParams {
   C* T_out;
   float* uprev;
   int* err;        // set to 1 when a bounded wait gives up
+  // cell lists (step_list<>): entry cell index / neighbour-solid bits, the entry
+  // of each cell (-1: none) and the list header (kLh* slots)
+  uint32_t* ent_c;
+  uint32_t* ent_b;
+  int* pos;
+  int* lhdr;
+  int* flips;      // [2][N]: cells that turned fluid on a pass of parity 0 / 1
+};
+
+// Cell-list entries (step_list<>): bit k (1..Q-1) of the bit word is set if
+// c + e_k is solid; kEntReactive marks a reactive cell, kEntDead an entry whose
+// cell has left the list.
+constexpr uint32_t kEntReactive = 1u << 24;
+constexpr uint32_t kEntDead = 1u << 31;
+constexpr uint32_t kEntPad = 0xffffffffu;  // cell index of a padding entry
+
+// List header slots (int32).
+enum : int {
+  kLhFi = 0,      // end of the fluid interior segment
+  kLhFg = 1,      // begin of the fluid general segment (multiple of 32)
+  kLhFe = 2,      // end of the fluid list (grows when cells turn fluid)
+  kLhSb = 3,      // begin of the solid list = capacity of the fluid list
+  kLhSi = 4,      // end of the solid interior segment
+  kLhSg = 5,      // begin of the solid general segment
+  kLhSe = 6,      // end of the solid list
+  kLhFlip0 = 8,   // cells that turned fluid on a pass of parity 0 / 1 (flip lists)
+  kLhFlip1 = 9,
+  kLhSlots = 16
 };
 
 // Per-population storage shifts (FP16 deviation storage); zero otherwise.
@@ -116,11 +153,20 @@ __device__ __forceinline__ int wrapi(int v, int n) { return v < 0 ? n - 1 : (v >
 // wrap (src/LBM/LBM2D/_evolution.py:205-212).
 struct Nbhd {
   int xs[3], ro[3], po[3];
+  Nbhd() = default;
   __device__ __forceinline__ Nbhd(int x, int y, int z, int nx, int ny, int nz) {
     xs[0] = wrapi(x - 1, nx); xs[1] = x; xs[2] = wrapi(x + 1, nx);
     ro[0] = wrapi(y - 1, ny) * nx; ro[1] = y * nx; ro[2] = wrapi(y + 1, ny) * nx;
     const int pl = nx * ny;
     po[0] = wrapi(z - 1, nz) * pl; po[1] = z * pl; po[2] = wrapi(z + 1, nz) * pl;
+  }
+  // Cell c away from every periodic edge: neighbours are plain offsets.
+  __device__ __forceinline__ static Nbhd interior(int c, int nx, int pl) {
+    Nbhd n;
+    n.xs[0] = c - 1; n.xs[1] = c; n.xs[2] = c + 1;
+    n.ro[0] = -nx; n.ro[1] = 0; n.ro[2] = nx;
+    n.po[0] = -pl; n.po[1] = 0; n.po[2] = pl;
+    return n;
   }
   __device__ __forceinline__ int at(int dx, int dy, int dz) const {
     return xs[dx + 1] + ro[dy + 1] + po[dz + 1];
@@ -512,16 +558,112 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
 
 // ------------------------------------------------------------------ kernels
 // THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis.
-template <class L, class S, int COLL, int THERM>
-// FP32/FP16 arithmetic: at most 128 registers per thread, 4 blocks of 128
-// threads (16 warps) per SM; FP64 keeps the full register budget.  blockDim.x
-// is a multiple of 32 and at most 256 (a tile of consecutive x cells).
-__global__ void __launch_bounds__(256, (std::is_same<S, double>::value ? 1 : 2))
-    step_bulk(const __grid_constant__ StepParams<S> p) {
+
+// Where cell_update<> takes its post-stream populations from: straight from the
+// input buffers in HBM (this source), or from copies staged in shared memory
+// (StagedPull in list_kernel.cuh).
+template <class L, class S>
+struct GlobalPull {
+  using C = typename Store<S>::C;
+  template <bool PYRO>
+  __device__ __forceinline__ void flow(const StepParams<S>& p, const Nbhd& nb, int c, uint32_t nbits,
+                                       C F[L::Q]) const {
+    Kern<L, S>::template pull_flow<PYRO>(p, nb, c, nbits, F);
+  }
+  __device__ __forceinline__ void thermal(const StepParams<S>& p, const Nbhd& nb, int c, C G[L::QT]) const {
+    Kern<L, S>::pull_thermal(p, nb, c, G);
+  }
+  __device__ __forceinline__ C alpha(const StepParams<S>& p, int c) const { return p.alpha[c]; }
+};
+//
+// One cell of the fused update (shared by the tile and the cell-list bulk
+// kernels): temperature pull, flow pull/moments/collision/store for fluid cells,
+// Arrhenius pyrolysis for reactive solid cells, temperature collision/store and
+// the diagnostics.  nbits: bit k set if c + e_k is solid at this parity.  mk is
+// the mask byte (read only by a peek pass over a reactive cell).  Returns whether
+// the cell is solid at the next parity.
+template <class L, class S, int COLL, int THERM, class Src = GlobalPull<L, S>>
+__device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc& acc, bool diag, bool peek, int c,
+                                            const Nbhd& nb, uint32_t nbits, bool solid, bool reactive,
+                                            uint8_t mk, const Src& src = Src()) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr int Q = L::Q, QT = L::QT;
   constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
+  C G[QT > 0 ? QT : 1];
+  C T = 0, dS = 0, rho = 0, ux = 0, uy = 0, uz = 0;
+  if constexpr (THERMAL) {
+    src.thermal(p, nb, c, G);
+    static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
+  }
+  bool solid_next = solid;
+  bool flipping = false;
+  if (!solid) {
+    C F[Q];
+    src.template flow<PYRO>(p, nb, c, nbits, F);
+    K::moments(p, F, rho, ux, uy, uz);
+    if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
+    if (!peek) {
+      K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
+      K::store_flow(p, nb, c, nbits, F);
+    }
+  } else if constexpr (PYRO) {
+    if (reactive) {
+      if (peek) {
+        // current state: a cell that turned fluid on the last pass is fluid now;
+        // flip_cells<> reports its flow state
+        if (!((mk >> (p.par ^ 1)) & 1)) solid_next = false;
+      } else {
+        // Arrhenius rate at the solid temperature, src/LBM/LBM2D/_chemical.py:198-212
+        const C a = src.alpha(p, c);
+        const C TK = T * p.Tscale + p.Tref;
+        C kr = 0;
+        if (TK > p.pyTmin) {
+          const C Te = TK + (C)1e-6;
+          kr = p.pyA * exp(-(p.pyEaR / Te));
+          if (p.pyb != (C)0) kr *= pow(Te, p.pyb);
+        }
+        const C da = kr * a * p.dtp;
+        const C an = a - da;
+        p.alpha[c] = an;
+        dS = -p.heat_norm * da;
+        if (an < p.alpha_flip) {
+          // turns fluid: flip_cells<> finishes it after this pass and finds the
+          // heat source here
+          solid_next = false;
+          flipping = true;
+          p.relB[c] = dS;
+        } else {
+          C W = 0;
+          static_for<Q>([&](auto kk) {
+            constexpr int k = decltype(kk)::value;
+            if constexpr (k > 0) {
+              if (!((nbits >> k) & 1)) W += (C)L::w(k);
+            }
+          });
+          p.relB[c] = W > (C)0 ? p.gas_coef * da / W : (C)0;
+        }
+      }
+    }
+  }
+  if constexpr (THERMAL) {
+    if (!peek && !flipping) {
+      const bool fl = !solid;
+      K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
+                         fl ? uz : (C)0, dS);
+      K::store_thermal(p, c, G);
+    }
+    if (diag) diag_thermal(p, acc, c, T);
+  }
+  if (PYRO && diag && solid_next && reactive) acc.v[2] += (double)p.alpha[c];
+  return solid_next;
+}
+
+// Tile form of the bulk update: one block per run of blockDim.x cells of an x row
+// (blockDim.x a multiple of 32, at most 256); register cap BulkRegs<S>.
+template <class L, class S, int COLL, int THERM>
+__global__ void __maxnreg__(BulkRegs<S>::v) step_bulk(const __grid_constant__ StepParams<S> p) {
+  using K = Kern<L, S>;
   const int y = blockIdx.y, z = blockIdx.z;
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
   const bool peek = (p.flags & kStepPeek) != 0;
@@ -568,72 +710,8 @@ __global__ void __launch_bounds__(256, (std::is_same<S, double>::value ? 1 : 2))
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
     const bool solid = cell_kind == 1;
     const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
-    C G[QT > 0 ? QT : 1];
-    C T = 0, dS = 0, rho = 0, ux = 0, uy = 0, uz = 0;
-    if constexpr (THERMAL) {
-      K::pull_thermal(p, nb, c, G);
-      static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
-    }
-    bool solid_next = solid;
-    bool flipping = false;
-    if (!solid) {
-      C F[Q];
-      K::template pull_flow<PYRO>(p, nb, c, nbits, F);
-      K::moments(p, F, rho, ux, uy, uz);
-      if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
-      if (!peek) {
-        K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
-        K::store_flow(p, nb, c, nbits, F);
-      }
-    } else if constexpr (PYRO) {
-      if (mk & LBM_MASK_REACTIVE) {
-        if (peek) {
-          // current state: a cell that turned fluid on the last pass is fluid now;
-          // flip_cells<> reports its flow state
-          if (!((mk >> (p.par ^ 1)) & 1)) solid_next = false;
-        } else {
-          // Arrhenius rate at the solid temperature, src/LBM/LBM2D/_chemical.py:198-212
-          const C a = p.alpha[c];
-          const C TK = T * p.Tscale + p.Tref;
-          C kr = 0;
-          if (TK > p.pyTmin) {
-            const C Te = TK + (C)1e-6;
-            kr = p.pyA * exp(-(p.pyEaR / Te));
-            if (p.pyb != (C)0) kr *= pow(Te, p.pyb);
-          }
-          const C da = kr * a * p.dtp;
-          const C an = a - da;
-          p.alpha[c] = an;
-          dS = -p.heat_norm * da;
-          if (an < p.alpha_flip) {
-            // turns fluid: flip_cells<> finishes it after this pass and finds the
-            // heat source here
-            solid_next = false;
-            flipping = true;
-            p.relB[c] = dS;
-          } else {
-            C W = 0;
-            static_for<Q>([&](auto kk) {
-              constexpr int k = decltype(kk)::value;
-              if constexpr (k > 0) {
-                if (!((nbits >> k) & 1)) W += (C)L::w(k);
-              }
-            });
-            p.relB[c] = W > (C)0 ? p.gas_coef * da / W : (C)0;
-          }
-        }
-      }
-    }
-    if constexpr (THERMAL) {
-      if (!peek && !flipping) {
-        const bool fl = !solid;
-        K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
-                           fl ? uz : (C)0, dS);
-        K::store_thermal(p, c, G);
-      }
-      if (diag) diag_thermal(p, acc, c, T);
-    }
-    if (PYRO && diag && solid_next && (mk & LBM_MASK_REACTIVE)) acc.v[2] += (double)p.alpha[c];
+    const bool solid_next = cell_update<L, S, COLL, THERM>(p, acc, diag, peek, c, nb, nbits, solid,
+                                                          (mk & LBM_MASK_REACTIVE) != 0, mk);
     // mask bit for the next parity: written only when it changes
     if (!peek) {
       const int np = p.par ^ 1;
@@ -645,6 +723,33 @@ __global__ void __launch_bounds__(256, (std::is_same<S, double>::value ? 1 : 2))
     const int blk = blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z);
     block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk), (size_t)p.partial_rows);
   }
+}
+
+// Cell-list upkeep for cell c turning fluid (nbn: its neighbour bits at the
+// next parity): its solid entry dies, a fluid entry is appended, and the bit
+// that points at c is cleared in the entries of its neighbours.  Neighbours that
+// turn fluid on the same pass build their entries from the next-parity mask, so
+// the order of these updates does not matter.
+template <class L, class S>
+__device__ __forceinline__ void list_turn_fluid(const StepParams<S>& p, int c, const Nbhd& nb, uint32_t nbn) {
+  const int old = p.pos[c];
+  if (old >= 0) atomicOr(&p.ent_b[old], kEntDead);
+  const int idx = atomicAdd(&p.lhdr[kLhFe], 1);
+  if (idx >= p.lhdr[kLhSb]) {  // cannot happen: the fluid list has room for every listed cell
+    if (p.err) atomicOr(p.err, 2);
+    return;
+  }
+  p.ent_c[idx] = (uint32_t)c;
+  p.ent_b[idx] = nbn;
+  p.pos[c] = idx;
+  static_for<L::Q>([&](auto kk) {
+    constexpr int k = decltype(kk)::value;
+    if constexpr (k > 0) {
+      const int n = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));  // n + e_k = c
+      const int pn = p.pos[n];
+      if (pn >= 0) atomicAnd(&p.ent_b[pn], ~(1u << k));
+    }
+  });
 }
 
 // Cells that turned fluid on this pass (mask bit par solid, bit par^1 fluid).
@@ -668,7 +773,13 @@ __global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepPa
   const int np = p.par ^ 1;
   const bool peek = (p.flags & kStepPeek) != 0;
   const size_t stride = (size_t)gridDim.x * blockDim.x;
-  for (size_t c0 = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c0 < p.N; c0 += stride) {
+  // with cell lists the bulk pass listed the cells that turned fluid; otherwise
+  // the whole mask is scanned
+  const bool listed = p.lhdr != nullptr;
+  const size_t n = listed ? (size_t)p.lhdr[kLhFlip0 + p.par] : p.N;
+  if (listed && !peek && blockIdx.x == 0 && threadIdx.x == 0) p.lhdr[kLhFlip0 + np] = 0;  // for the next pass
+  for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    const size_t c0 = listed ? (size_t)p.flips[(size_t)p.par * p.N + i] : i;
     const uint8_t mk = p.mask[c0];
     if (!(((mk >> p.par) & 1) && !((mk >> np) & 1))) continue;
     const int c = (int)c0;
@@ -700,7 +811,9 @@ __global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepPa
       C F[Q];
       K::feq_all(p, rb, ux, uy, uz, F);
       K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
-      K::store_flow(p, nb, c, K::neighbour_bits(p, nb, np), F);
+      const uint32_t nbn = K::neighbour_bits(p, nb, np);
+      K::store_flow(p, nb, c, nbn, F);
+      if (p.lhdr) list_turn_fluid<L>(p, c, nb, nbn);
     }
     if constexpr (THERMAL) {
       C G[QT];

@@ -41,6 +41,8 @@ class Lattice:
         self._desc = cfg.to_desc()
         import os
         self._staged_env = os.environ.get("LBM_STAGED", "0")[:1] == "1"
+        bulk = os.environ.get("LBM_BULK", "")
+        self._tile_env = bulk == "tile" or (bulk != "list" and cfg.ncells < 65536)
         h = ctypes.c_void_p()
         N.check(self.lib.lbm_create(ctypes.byref(self._desc), ctypes.byref(h)))
         self._h = h
@@ -78,6 +80,15 @@ class Lattice:
         """True if the bulk update uses the shared-memory staged kernel (LBM_STAGED=1, rows a
         multiple of 128)."""
         return self.cfg.nx % 128 == 0 and self._staged_env
+
+    @property
+    def bulk_kernel(self) -> str:
+        """Form of the bulk update this lattice runs: "list" (cell lists; the default from
+        65536 cells, or LBM_BULK=list), "tile" (smaller lattices, or LBM_BULK=tile) or
+        "staged" (LBM_STAGED=1); fixed when the lattice is created."""
+        if self._staged():
+            return "staged"
+        return "tile" if self._tile_env else "list"
 
     @property
     def nsteps(self) -> int:

@@ -82,8 +82,24 @@ def pyro3d(n: int = 256, seed: int = 0, precision: str = "fp32", collision: str 
                     {"rho": 1.0, "u": (0.0, 0.0, 0.0), "T": 0.0})
 
 
+def bytes_per_lattice_update(cfg: LatticeConfig) -> int:
+    """Bytes one lattice update moves by the dense A/B pull count: read and write every
+    flow and temperature population, read the mask byte, read and write the per-cell
+    reaction state (B = 2 Q s + 2 QT s + 1 + 2 s_state [pyrolysis]).  D3Q19 + D3Q7 +
+    pyrolysis: 217 B in FP32, 113 B with FP16 storage, 433 B in FP64; D2Q9 alone: 73 B.
+    This is the per-update figure the roofline fraction is quoted on."""
+    s = {"fp32": 4, "fp16": 2, "fp64": 8}[cfg.precision]
+    b = 2 * cfg.Q * s + 1
+    if cfg.thermal != "none":
+        b += 2 * cfg.QT * s
+    if cfg.pyro:
+        b += 2 * (8 if cfg.precision == "fp64" else 4)
+    return b
+
+
 def algorithmic_bytes_per_step(cfg: LatticeConfig, solid: np.ndarray) -> int:
-    """Minimum DRAM bytes one step must move in this design (the roofline numerator).
+    """Minimum DRAM bytes one step must move in this design, where solid cells carry no
+    flow populations (a lower bound below the dense per-update count).
 
     Fluid cells read and write Q flow populations; every cell reads and writes QT
     temperature populations (conjugate mode); every cell reads its mask byte;

@@ -55,12 +55,15 @@ def test_noalloc_matches_allocating_path_twice(precision):
     lat.close()
 
 
-def test_noalloc_rejects_lattice_beyond_static_scratch():
+def test_noalloc_rejects_lattice_beyond_static_scratch(monkeypatch):
     from lbm_porouschem_b200.config import LatticeConfig
     from lbm_porouschem_b200.lattice import Lattice
-    # 32 x 200 x 200: one 32-wide block per (y, z) row -> 40000 partial rows > 32768
+    # 32 x 200 x 200 with the tile form of the bulk update: one 32-wide block per
+    # (y, z) row -> 40000 partial rows > 32768 (the cell-list form needs a few hundred)
+    monkeypatch.setenv("LBM_BULK", "tile")
     cfg = LatticeConfig(dim=3, nx=32, ny=200, nz=200, nu=0.1)
     lat = Lattice(cfg)
+    assert lat.bulk_kernel == "tile"
     lat.set_geometry(np.zeros(cfg.shape, dtype=bool))
     lat.init()
     lat.step(1)
