@@ -44,7 +44,6 @@ struct Launch {
   int flip_blocks;    // grid of flip_cells (pyrolysis only), 256 threads each
   bool staged;        // bulk update by step_bulk_staged (persistent grid of bulk_blocks)
   bool list;          // bulk update by step_list (persistent grid of bulk_blocks x 128)
-  bool list_stage;    // step_list stages pulled populations in shared memory (FP32/FP64; LBM_LIST_STAGE)
   size_t N;
   int list_base;      // first entry of the solid list (capacity of the fluid list)
   size_t list_cap;    // entries in both lists
@@ -97,10 +96,6 @@ inline Launch plan(const lbm_desc& d, int tx) {
   L.N = (size_t)d.nx * d.ny * d.nz;
   const bool force_tile = b && std::strcmp(b, "tile") == 0, force_list = b && std::strcmp(b, "list") == 0;
   L.list = !L.staged && !force_tile && (force_list || L.N >= 65536);
-  // staging the pulls in shared memory pays in 2D; in 3D direct loads measured
-  // faster (D3Q19 + D3Q7 + pyrolysis, 256^3: 11.2 against 9.6 GLUPS in FP32)
-  const char* ls = getenv("LBM_LIST_STAGE");
-  L.list_stage = ls ? ls[0] == '1' : d.dim == 2;
   L.list_base = (int)((L.N + 64 + 31) / 32 * 32);
   L.list_cap = 2 * (size_t)L.list_base;
   L.list_nbb = (int)((L.N + kListChunk - 1) / kListChunk);

@@ -5,26 +5,25 @@
 namespace lbm {
 namespace capi {
 
-template <class Lt, class S, int COLL, int THERM, bool OUT, bool STAGE>
+template <class Lt, class S, int COLL, int THERM, int MODE>
 static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st) {
-  constexpr size_t smem = list_smem_bytes<Lt, S>(128, STAGE);
+  constexpr size_t smem = list_smem_bytes<Lt, S>(128);
   if (smem > 0) {
     // opt in above the 48 KB default: with the static reduction buffer the total can
     // pass it even when the stages alone do not
     static bool attr_set = false;  // one attribute call per process and instantiation
     if (!attr_set) {
-      cudaFuncSetAttribute(step_list<Lt, S, COLL, THERM, OUT, STAGE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+      cudaFuncSetAttribute(step_list<Lt, S, COLL, THERM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                            (int)smem);
       attr_set = true;
     }
   }
-  step_list<Lt, S, COLL, THERM, OUT, STAGE><<<L.bulk_blocks, 128, smem, st>>>(p);
+  step_list<Lt, S, COLL, THERM, MODE><<<L.bulk_blocks, 128, smem, st>>>(p);
 }
 
 template <class Lt, class S, int COLL, int THERM>
 static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const Launch& L = h->L;
-  bool list_done = false;  // the staged list form ran
   if (L.staged) {
     using LY = StagedLayout<Lt, S, kStagedTile>;
     constexpr size_t smem = (size_t)kStagedStages * LY::STAGE_BYTES;
@@ -36,17 +35,9 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
     }
     step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages><<<L.bulk_blocks, kStagedTile, smem, st>>>(p);
   } else if (L.list) {
-    if constexpr (Staged<S>::value) {
-      if (L.list_stage) {
-        if (p.flags) launch_list<Lt, S, COLL, THERM, true, true>(L, p, st);
-        else launch_list<Lt, S, COLL, THERM, false, true>(L, p, st);
-        list_done = true;
-      }
-    }
-    if (!list_done) {
-      if (p.flags) launch_list<Lt, S, COLL, THERM, true, false>(L, p, st);
-      else launch_list<Lt, S, COLL, THERM, false, false>(L, p, st);
-    }
+    if (p.flags & kStepPeek) launch_list<Lt, S, COLL, THERM, 2>(L, p, st);
+    else if (p.flags) launch_list<Lt, S, COLL, THERM, 1>(L, p, st);
+    else launch_list<Lt, S, COLL, THERM, 0>(L, p, st);
   } else {
     step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
   }

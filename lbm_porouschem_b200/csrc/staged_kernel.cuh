@@ -181,7 +181,7 @@ __global__ void __launch_bounds__(TILE, (std::is_same<S, double>::value ? 1 : 4)
 
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
   const bool peek = (p.flags & kStepPeek) != 0;
-  DiagAcc acc;
+  DiagAcc<typename Store<S>::C> acc;
   if (diag) acc.clear();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int ntiles = (p.nx / TILE) * p.ny * p.nz;
@@ -332,7 +332,7 @@ __global__ void __launch_bounds__(TILE, (std::is_same<S, double>::value ? 1 : 4)
         }
         if (diag) diag_thermal(p, acc, c, T);
       }
-      if (PYRO && diag && solid_next && (mk & LBM_MASK_REACTIVE)) acc.v[2] += (double)p.alpha[c];
+      if (PYRO && diag && solid_next && (mk & LBM_MASK_REACTIVE)) acc.alpha += (double)p.alpha[c];
       if (!peek) {
         const int np = p.par ^ 1;
         const uint8_t want = (uint8_t)((mk & ~(1u << np)) | ((solid_next ? 1u : 0u) << np));

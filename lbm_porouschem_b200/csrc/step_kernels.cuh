@@ -446,23 +446,77 @@ struct Kern {
 };
 
 // --------------------------------------------------------------- diagnostics
+// Per-thread diagnostics: FP64 sums (mass, energy, solid reactive fraction,
+// residual numerator and denominator), max |u|^2 / min T / max T in the compute
+// type C, integer counts.  The block partial rows are FP64 in lbm_diag order.
+template <class C>
 struct DiagAcc {
-  double v[kNumDiag];
+  double mass, energy, alpha, res_num, res_den;
+  C u2max, Tmin, Tmax;
+  unsigned nonfinite, nfluid;
   __device__ __forceinline__ void clear() {
-    for (int i = 0; i < kNumDiag; ++i) v[i] = 0;
-    v[4] = 1e300;   // Tmin
-    v[5] = -1e300;  // Tmax
+    mass = energy = alpha = res_num = res_den = 0;
+    u2max = 0;
+    Tmin = (C)3.0e38;
+    Tmax = (C)-3.0e38;
+    nonfinite = nfluid = 0;
+  }
+  // add another accumulator (a cell's contribution) into this one
+  __device__ __forceinline__ void merge(const DiagAcc& b) {
+    mass += b.mass; energy += b.energy; alpha += b.alpha; res_num += b.res_num; res_den += b.res_den;
+    u2max = fmax(u2max, b.u2max); Tmin = fmin(Tmin, b.Tmin); Tmax = fmax(Tmax, b.Tmax);
+    nonfinite += b.nonfinite; nfluid += b.nfluid;
+  }
+  __device__ __forceinline__ double get(int i) const {
+    switch (i) {
+      case 0: return mass;
+      case 1: return energy;
+      case 2: return alpha;
+      case 3: return (double)u2max;
+      case 4: return Tmin <= (C)-3.0e38 || Tmin >= (C)3.0e38 ? (Tmin > 0 ? 1e300 : -1e300) : (double)Tmin;
+      case 5: return Tmax <= (C)-3.0e38 || Tmax >= (C)3.0e38 ? (Tmax > 0 ? 1e300 : -1e300) : (double)Tmax;
+      case 6: return (double)nonfinite;
+      case 7: return (double)nfluid;
+      case 8: return res_num;
+      default: return res_den;
+    }
+  }
+};
+
+// Per-thread accumulators in shared memory, one array per field (consecutive
+// threads hit consecutive banks).
+template <class C, int T>
+struct DiagSmem {
+  double mass[T], energy[T], alpha[T], res_num[T], res_den[T];
+  C u2max[T], Tmin[T], Tmax[T];
+  unsigned nonfinite[T], nfluid[T];
+  __device__ __forceinline__ void clear(int t) {
+    mass[t] = energy[t] = alpha[t] = res_num[t] = res_den[t] = 0;
+    u2max[t] = 0; Tmin[t] = (C)3.0e38; Tmax[t] = (C)-3.0e38;
+    nonfinite[t] = nfluid[t] = 0;
+  }
+  __device__ __forceinline__ void merge(int t, const DiagAcc<C>& b) {
+    mass[t] += b.mass; energy[t] += b.energy; alpha[t] += b.alpha; res_num[t] += b.res_num; res_den[t] += b.res_den;
+    u2max[t] = fmax(u2max[t], b.u2max); Tmin[t] = fmin(Tmin[t], b.Tmin); Tmax[t] = fmax(Tmax[t], b.Tmax);
+    nonfinite[t] += b.nonfinite; nfluid[t] += b.nfluid;
+  }
+  __device__ __forceinline__ DiagAcc<C> load(int t) const {
+    DiagAcc<C> a;
+    a.mass = mass[t]; a.energy = energy[t]; a.alpha = alpha[t]; a.res_num = res_num[t]; a.res_den = res_den[t];
+    a.u2max = u2max[t]; a.Tmin = Tmin[t]; a.Tmax = Tmax[t]; a.nonfinite = nonfinite[t]; a.nfluid = nfluid[t];
+    return a;
   }
 };
 
 // Block reduction with warp shuffles (FP64), one partial row per block.
-__device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row, size_t stride) {
+template <class C>
+__device__ __forceinline__ void block_reduce_store(const DiagAcc<C>& a, double* out_row, size_t stride) {
   __shared__ double sh[32][kNumDiag];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int nwarps = (blockDim.x + 31) >> 5;
 #pragma unroll
   for (int i = 0; i < kNumDiag; ++i) {
-    double v = a.v[i];
+    double v = a.get(i);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       const double w = __shfl_xor_sync(0xffffffffu, v, o);
@@ -487,19 +541,21 @@ __device__ __forceinline__ void block_reduce_store(DiagAcc& a, double* out_row, 
 
 // Flow part of one cell's diagnostics (and macro/residual outputs).
 template <class S>
-__device__ __forceinline__ void diag_flow(const StepParams<S>& p, DiagAcc& a, int c, typename Store<S>::C rho,
-                                          typename Store<S>::C ux, typename Store<S>::C uy,
-                                          typename Store<S>::C uz) {
-  a.v[0] += (double)rho;
+__device__ __forceinline__ void diag_flow(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& a, int c,
+                                          typename Store<S>::C rho, typename Store<S>::C ux,
+                                          typename Store<S>::C uy, typename Store<S>::C uz) {
+  using C = typename Store<S>::C;
+  a.mass += (double)rho;
+  // in double: exact products of FP32 inputs, so no contraction choice changes it
   const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
-  a.v[3] = fmax(a.v[3], u2);
-  if (!finite_(rho)) a.v[6] += 1;
-  a.v[7] += 1;
+  a.u2max = fmax(a.u2max, (C)u2);
+  if (!finite_(rho)) a.nonfinite += 1;
+  a.nfluid += 1;
   if (p.flags & LBM_STEP_RESIDUAL) {
     const double dx = (double)ux - p.uprev[c], dy = (double)uy - p.uprev[p.N + c],
                  dz = (double)uz - p.uprev[2 * p.N + c];
-    a.v[8] += dx * dx + dy * dy + dz * dz;
-    a.v[9] += u2;
+    a.res_num += dx * dx + dy * dy + dz * dz;
+    a.res_den += (double)ux * ux + (double)uy * uy + (double)uz * uz;
     p.uprev[c] = (float)ux;
     p.uprev[p.N + c] = (float)uy;
     p.uprev[2 * p.N + c] = (float)uz;
@@ -513,11 +569,12 @@ __device__ __forceinline__ void diag_flow(const StepParams<S>& p, DiagAcc& a, in
 }
 // Temperature part (every cell).
 template <class S>
-__device__ __forceinline__ void diag_thermal(const StepParams<S>& p, DiagAcc& a, int c, typename Store<S>::C T) {
-  a.v[1] += (double)T;
-  a.v[4] = fmin(a.v[4], (double)T);
-  a.v[5] = fmax(a.v[5], (double)T);
-  if (!finite_(T)) a.v[6] += 1;
+__device__ __forceinline__ void diag_thermal(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& a, int c,
+                                             typename Store<S>::C T) {
+  a.energy += (double)T;
+  a.Tmin = fmin(a.Tmin, T);
+  a.Tmax = fmax(a.Tmax, T);
+  if (!finite_(T)) a.nonfinite += 1;
   if (p.flags & LBM_STEP_MACRO) p.T_out[c] = T;
 }
 
@@ -583,7 +640,7 @@ struct GlobalPull {
 // the mask byte (read only by a peek pass over a reactive cell).  Returns whether
 // the cell is solid at the next parity.
 template <class L, class S, int COLL, int THERM, class Src = GlobalPull<L, S>>
-__device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc& acc, bool diag, bool peek, int c,
+__device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& acc, bool diag, bool peek, int c,
                                             const Nbhd& nb, uint32_t nbits, bool solid, bool reactive,
                                             uint8_t mk, const Src& src = Src()) {
   using K = Kern<L, S>;
@@ -602,11 +659,11 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc& acc
     C F[Q];
     src.template flow<PYRO>(p, nb, c, nbits, F);
     K::moments(p, F, rho, ux, uy, uz);
-    if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
     if (!peek) {
       K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
       K::store_flow(p, nb, c, nbits, F);
     }
+    if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);  // after the store: fewer live registers
   } else if constexpr (PYRO) {
     if (reactive) {
       if (peek) {
@@ -655,7 +712,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc& acc
     }
     if (diag) diag_thermal(p, acc, c, T);
   }
-  if (PYRO && diag && solid_next && reactive) acc.v[2] += (double)p.alpha[c];
+  if (PYRO && diag && solid_next && reactive) acc.alpha += (double)p.alpha[c];
   return solid_next;
 }
 
@@ -667,7 +724,7 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_bulk(const __grid_constant__ St
   const int y = blockIdx.y, z = blockIdx.z;
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
   const bool peek = (p.flags & kStepPeek) != 0;
-  DiagAcc acc;
+  DiagAcc<typename Store<S>::C> acc;
   if (diag) acc.clear();
 
   // Rank the tile's cells fluid first, then solid, then cells this kernel skips
@@ -768,7 +825,7 @@ __global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepPa
   constexpr int Q = L::Q, QT = L::QT;
   constexpr bool THERMAL = THERM >= 1;
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
-  DiagAcc acc;
+  DiagAcc<typename Store<S>::C> acc;
   if (diag) acc.clear();
   const int np = p.par ^ 1;
   const bool peek = (p.flags & kStepPeek) != 0;
@@ -919,7 +976,7 @@ __global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ Ste
   const int face = fid[blockIdx.y];
   const int i = blockIdx.x * blockDim.x + threadIdx.x;
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
-  DiagAcc acc;
+  DiagAcc<typename Store<S>::C> acc;
   if (diag) acc.clear();
   int x = 0, y = 0, z = 0;
   bool valid = false;
