@@ -199,11 +199,13 @@ LBM_API int64_t lbm_step_count(const lbm_handle* h);
  * device memory: e.g. a plug-in whose host application owns every device
  * allocation through its own pool, or a hook inside a latency-critical time
  * loop where a cudaMalloc, which may synchronise the device, is not allowed.
- * The lattice state must be bound; LBM_FIELD_SCRATCH need not be.  The
+ * The lattice state must be bound (with the cell-list bulk update, the lists
+ * in LBM_FIELD_SCRATCH are part of it; the tile form needs no SCRATCH).  The
  * reduction's scratch is a static device array held by every GPU that loads
  * the library until exit (about 2.6 MB): lattices whose launch plan needs more
- * than LBM_NOALLOC_MAX_ROWS partial rows (one per thread block, e.g. up to
- * about 128^3 cells in 3D) are rejected with LBM_ERR_SIZE.  The first call on
+ * than LBM_NOALLOC_MAX_ROWS partial rows (one per thread block: four per SM
+ * plus the boundary blocks in list form, one per row tile in tile form, e.g.
+ * about 128^3 cells) are rejected with LBM_ERR_SIZE.  The first call on
  * a device looks up the array's device address (make it before any stream
  * capture).  All calls share the array and each call rewrites every value it
  * reads, so calls that overlap on the GPU (different streams or handles at
