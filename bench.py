@@ -36,7 +36,9 @@ def parse(argv=None):
     ap.add_argument("--steps", type=int, default=600)
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pyro3d", choices=["pyro3d", "pyro2d", "flow2d"])
+    ap.add_argument("--workload", default="pyro3d", choices=["pyro3d", "pyro2d", "flow2d", "sweep2d"])
+    ap.add_argument("--instances", type=int, default=96, help="lattices of the sweep2d batch")
+    ap.add_argument("--graph-steps", type=int, default=100, help="steps per captured graph (sweep2d)")
     ap.add_argument("--size", type=int, default=0, help="edge length override (default: the workload's)")
     ap.add_argument("--precision", default="fp32", choices=["fp32", "fp16", "fp64"])
     ap.add_argument("--collision", default="")
@@ -82,6 +84,8 @@ def launches_per_step(cfg) -> int:
 
 def make_workload(args, seed):
     from lbm_porouschem_b200 import workloads
+    if args.workload == "sweep2d":        # the reference arm times one lattice of the sweep
+        return workloads.sweep2d(1, seed0=seed, precision=args.precision)[0]
     if args.workload == "pyro3d":
         n = args.size or 256
         w = workloads.pyro3d(n, seed=seed, precision=args.precision, collision=args.collision or "mrt")
@@ -212,6 +216,9 @@ def main(argv=None):
         print(json.dumps(line), flush=True)
         return 0
 
+    if args.workload == "sweep2d":
+        return sweep_main(args, world, rank, local)
+
     import torch
     import torch.distributed as dist
     from lbm_porouschem_b200 import workloads as W
@@ -323,6 +330,131 @@ def main(argv=None):
                                     "sample": f"{n} full steps of {w.name} (FP32 C restatement, OpenMP)"}
         print(json.dumps(line), flush=True)
     lat.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def sweep_main(args, world, rank, local):
+    """Parameter sweep: ``--instances`` lattices of uneven sizes stepped as one batch,
+    replayed from a CUDA graph of ``--graph-steps`` steps, against the same lattices
+    launched one at a time."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+    from lbm_porouschem_b200 import _native as N
+    from lbm_porouschem_b200 import workloads as W
+    from lbm_porouschem_b200.lattice import Lattice, LatticeBatch
+
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    dev = f"cuda:{local}"
+    ws = W.sweep2d(args.instances, seed0=rank_seed(args.seed, rank) * 1000, precision=args.precision,
+                   collision=args.collision or "bgk")
+    lats = []
+    for w in ws:
+        lat = Lattice(w.cfg, device=dev)
+        lat.set_geometry(w.solid, w.reactive)
+        lat.init(**w.init)
+        lats.append(lat)
+    torch.cuda.synchronize()
+    cells = sum(w.cfg.ncells for w in ws)
+    K = args.graph_steps + (args.graph_steps & 1)
+    batch = LatticeBatch(lats)
+    batch.step(max(4, args.warmup + (args.warmup & 1)))
+    batch.capture(K)
+    batch.replay()                      # warm replay (brings the state level with the counters)
+    batch.synchronize()
+    reps = max(1, args.steps // K)
+    rank_barrier(world)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(local)
+    clocks.start()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(batch.stream)
+    for _ in range(reps):
+        batch.replay()
+    e1.record(batch.stream)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    clk = clocks.stop()
+    ms_max = max_over_ranks(ms, world, dev)
+    value = job_mlups(cells, reps * K, world, ms_max)
+
+    # the same lattices launched one lattice at a time
+    seq_steps = max(2, min(40, args.steps // 10))
+    cur = torch.cuda.current_stream()
+    s0, s1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    cur.wait_stream(batch.stream)
+    s0.record(cur)
+    for _ in range(seq_steps):
+        for lat in lats:
+            lat.step(1)
+    s1.record(cur)
+    s1.synchronize()
+    seq_ms = max_over_ranks(s0.elapsed_time(s1), world, dev)
+    seq_value = job_mlups(cells, seq_steps, world, seq_ms)
+    batch.stream.wait_stream(cur)
+
+    # end to end: per graph replay, the side records of every lattice go host -> device,
+    # and every lattice's diagnostics come back
+    reps2 = max(1, min(reps, 3))
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    diag = None
+    for _ in range(reps2):
+        for lat in lats:
+            lat.stream = batch.stream
+            lat.set_sides(lat.cfg.sides)
+        batch.replay()
+        for lat in lats:
+            lat.compute(diag=True)
+            diag = lat.read_diag()
+    wall_ms = (time.perf_counter() - t0) * 1e3
+    for lat in lats:
+        lat.stream = None
+    e2e_ms = max_over_ranks(wall_ms, world, dev)
+    e2e_value = job_mlups(cells, reps2 * K, world, e2e_ms)
+
+    bytes_step = sum(W.bytes_per_lattice_update(w.cfg) * w.cfg.ncells for w in ws)
+    pk = ROOT / "MEASURED_PEAKS.json"
+    peaks = json.loads(pk.read_text()) if pk.exists() else {}
+    peak = float(peaks.get("hbm_gbs", 6650.0))
+    achieved = bytes_step / (ms / (reps * K) * 1e-3) / 1e9
+    if rank == 0:
+        sizes = {}
+        for w in ws:
+            sizes[f"{w.cfg.nx}x{w.cfg.ny}"] = sizes.get(f"{w.cfg.nx}x{w.cfg.ny}", 0) + 1
+        line = {
+            "metric": "coupled MLUPS", "value": round(value, 2), "unit": "MLUPS", "n_gpus": world,
+            "steps": reps * K, "warmup": args.warmup, "ms_per_step": round(ms_max / (reps * K), 4),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": {"fp32": "f32", "fp16": "f16-storage/f32", "fp64": "f64"}[args.precision],
+            "data": "synthetic (seeded disk packings, one parameter set per lattice)",
+            "config": {"workload": f"sweep2d: {len(ws)} D2Q9+D2Q5 {ws[0].cfg.collision.upper()} "
+                                   f"conjugate-heat+pyrolysis lattices, one batch, CUDA graph of {K} steps",
+                       "cells": cells, "sizes": sizes, "parallelism": f"replicas x{world}",
+                       "sequential_mlups": round(seq_value, 2), "sequential_steps": seq_steps,
+                       "batch_vs_sequential": round(value / seq_value, 2),
+                       "l2": "state larger than L2 (no flush needed)"},
+            "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
+                         "frac": round(achieved / peak, 4), "traffic": None,
+                         "note": "dense bytes per update x cells of all lattices / device time per batch step"},
+            "e2e": {"value": round(e2e_value, 2), "unit": "MLUPS",
+                    "h2d_bytes_per_step": len(ws) * ctypes.sizeof(N.lbm_side_desc),
+                    "d2h_bytes_per_step": len(ws) * 10 * 8, "steps": reps2 * K,
+                    "note": "one step = one graph replay of graph_steps lattice steps"},
+            "gpu_launches": reps * K * (3 if ws[0].cfg.pyro else 2),
+            "clocks": clk,
+            "diag_last": {k: diag[k] for k in ("mass", "energy", "umax", "nonfinite")},
+        }
+        print(json.dumps(line), flush=True)
+    batch.close()
+    for lat in lats:
+        lat.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

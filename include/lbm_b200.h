@@ -88,7 +88,7 @@ typedef struct lbm_desc {
   int32_t thermal;      /* LBM_THERMAL_* */
   int32_t pyro;         /* 1: Arrhenius pyrolysis with solid->fluid flip (needs thermal) */
   int32_t half_force_velocity; /* 1: u includes F/2 (reference: 0) */
-  int32_t reserved0;
+  int32_t bulk_form;    /* 0: cell lists from 65536 cells, else tile; 1: tile; 2: cell lists */
   double nu;            /* lattice viscosity visco*dt/dx^2 (_evolution.py:227-249) */
   double force[3];      /* body acceleration in lattice units (Guo forcing) */
   double tauT_fluid;    /* thermal relaxation time in fluid cells */
@@ -192,6 +192,27 @@ LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
 /* Lattice steps taken since lbm_init_equilibrium (tLattice counter,
  * src/LBM/LBM2D/_evolution.py:15). */
 LBM_API int64_t lbm_step_count(const lbm_handle* h);
+
+/* Batches: many initialised lattices (same dim, precision, collision, thermal and
+ * pyrolysis settings; sizes, geometries and parameters free; each created with
+ * bulk_form = 2) stepped together by one persistent launch per kernel, for
+ * parameter sweeps.  The reference runs one case per `lbm` process
+ * (src/LBM/app.py:16-680); a batch replaces a loop of step() calls over many
+ * solver objects.  The batch's tables live in a caller-owned device buffer of
+ * lbm_batch_required_bytes() bytes.  Both calls read the lattices' list headers
+ * and synchronise `stream`.  After lbm_batch_create, a lattice of the batch must
+ * not be re-initialised or stepped on its own while the batch is used. */
+typedef struct lbm_batch lbm_batch;
+LBM_API int32_t lbm_batch_required_bytes(lbm_handle* const* handles, int32_t n, void* stream, size_t* bytes);
+LBM_API int32_t lbm_batch_create(lbm_handle* const* handles, int32_t n, void* dev_buffer, size_t bytes,
+                                 void* stream, lbm_batch** out);
+/* Advance every lattice of the batch n steps (no diagnostics).  Issues no host
+ * synchronisation and no allocation, so it can be captured in a CUDA graph; after
+ * replaying a captured sequence of n steps call lbm_batch_advance(b, n) to move
+ * the step counters (n even: a sequence keeps the step parity it was captured at). */
+LBM_API int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream);
+LBM_API int32_t lbm_batch_advance(lbm_batch* b, int32_t n);
+LBM_API int32_t lbm_batch_destroy(lbm_batch* b);
 
 /* No counterpart in the reference.  The diagnostics of the current state (the
  * values lbm_compute_macro(h, LBM_STEP_DIAG, ...) + lbm_read_diag return),

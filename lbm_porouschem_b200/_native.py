@@ -43,6 +43,7 @@ EXPORTED = (
     "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_step", "lbm_compute_macro",
     "lbm_read_diag",
     "lbm_step_count", "lbm_diag_noalloc",
+    "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
 )
 LBM_NOALLOC_MAX_ROWS = 32768
 
@@ -59,7 +60,7 @@ class lbm_desc(C.Structure):
         ("struct_size", C.c_int32), ("dim", C.c_int32), ("nx", C.c_int32), ("ny", C.c_int32),
         ("nz", C.c_int32), ("collision", C.c_int32), ("precision", C.c_int32), ("eos", C.c_int32),
         ("thermal", C.c_int32), ("pyro", C.c_int32), ("half_force_velocity", C.c_int32),
-        ("reserved0", C.c_int32),
+        ("bulk_form", C.c_int32),
         ("nu", C.c_double), ("force", C.c_double * 3), ("tauT_fluid", C.c_double),
         ("tauT_solid", C.c_double), ("pyro_A", C.c_double), ("pyro_b", C.c_double),
         ("pyro_Ea", C.c_double), ("pyro_Tmin", C.c_double), ("T_ref", C.c_double),
@@ -125,6 +126,16 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_step_count.restype = i64
     lib.lbm_diag_noalloc.argtypes = [vp, C.POINTER(lbm_diag), vp]
     lib.lbm_diag_noalloc.restype = i32
+    lib.lbm_batch_required_bytes.argtypes = [C.POINTER(vp), i32, vp, C.POINTER(sz)]
+    lib.lbm_batch_required_bytes.restype = i32
+    lib.lbm_batch_create.argtypes = [C.POINTER(vp), i32, vp, sz, vp, C.POINTER(vp)]
+    lib.lbm_batch_create.restype = i32
+    lib.lbm_batch_step.argtypes = [vp, i32, vp]
+    lib.lbm_batch_step.restype = i32
+    lib.lbm_batch_advance.argtypes = [vp, i32]
+    lib.lbm_batch_advance.restype = i32
+    lib.lbm_batch_destroy.argtypes = [vp]
+    lib.lbm_batch_destroy.restype = i32
     if lib.lbm_abi_version() != 1:
         raise RuntimeError("liblbm_b200.so ABI version mismatch")
     _lib = lib

@@ -82,6 +82,7 @@ class LatticeConfig:
     rho0: float = 1.0
     T0: float = 0.0
     sides: list = field(default_factory=lambda: [SideBC() for _ in range(6)])
+    bulk_form: str = "auto"         # "auto" (cell lists from 65536 cells) | "tile" | "list"
 
     @property
     def shape(self) -> tuple:
@@ -127,6 +128,7 @@ class LatticeConfig:
         d.thermal = {"none": N.LBM_THERMAL_NONE, "conjugate": N.LBM_THERMAL_CONJUGATE}[self.thermal]
         d.pyro = int(self.pyro)
         d.half_force_velocity = int(self.half_force_velocity)
+        d.bulk_form = {"auto": 0, "tile": 1, "list": 2}[self.bulk_form]
         d.nu = self.nu
         for i in range(3):
             d.force[i] = float(self.force[i])

@@ -9,7 +9,9 @@
 #include <cstdlib>
 #include <cstring>
 #include <string>
+#include <vector>
 
+#include "batch_kernel.cuh"
 #include "list_kernel.cuh"
 #include "staged_kernel.cuh"
 #include "step_kernels.cuh"
@@ -94,7 +96,10 @@ inline Launch plan(const lbm_desc& d, int tx) {
   // outweigh what it saves); LBM_BULK=tile / list forces either form
   const char* b = getenv("LBM_BULK");
   L.N = (size_t)d.nx * d.ny * d.nz;
-  const bool force_tile = b && std::strcmp(b, "tile") == 0, force_list = b && std::strcmp(b, "list") == 0;
+  // the descriptor's bulk_form wins over LBM_BULK
+  const bool force_tile = d.bulk_form == 1 || (d.bulk_form == 0 && b && std::strcmp(b, "tile") == 0);
+  const bool force_list = d.bulk_form == 2 || (d.bulk_form == 0 && b && std::strcmp(b, "list") == 0);
+  if (force_list) L.staged = false;
   L.list = !L.staged && !force_tile && (force_list || L.N >= 65536);
   L.list_base = (int)((L.N + 64 + 31) / 32 * 32);
   L.list_cap = 2 * (size_t)L.list_base;
@@ -129,6 +134,23 @@ struct lbm_handle {
   int64_t step;
   lbm::capi::Launch L;
   bool diag_valid;
+  bool initialised;  // lbm_init_equilibrium ran (state and cell lists exist)
+};
+
+// A batch of lattices stepped together (batch_kernel.cuh).  Its device tables
+// live in a caller-owned buffer: parameters [n][2] | chunk table | boundary
+// block table.
+struct lbm_batch {
+  std::vector<lbm_handle*> hs;
+  void* scratch;
+  size_t bytes;
+  void* params;
+  int2* chunks;
+  int nchunks;
+  int4* bc;
+  int nbc;
+  int list_blocks;   // persistent grid of step_list_batch (128 threads each)
+  int flip_blocks;   // flip_cells_batch blocks per lattice
 };
 
 namespace lbm {
@@ -244,7 +266,11 @@ template <class Lt, class S>
 int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
                   const float* alpha, int solid_bit, cudaStream_t st);
 
+template <class Lt, class S>
+int dispatch_batch(lbm_batch* b, cudaStream_t st);
+
 #define LBM_EXTERN_INST(LT, ST)                                                                 \
+  extern template int dispatch_batch<LT, ST>(lbm_batch*, cudaStream_t);                         \
   extern template int dispatch_step<LT, ST>(lbm_handle*, StepParams<ST>, cudaStream_t);         \
   extern template int dispatch_init<LT, ST>(lbm_handle*, StepParams<ST>, const float*, const float*, \
                                             const float*, const float*, int, cudaStream_t);

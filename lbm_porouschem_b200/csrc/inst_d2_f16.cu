@@ -66,6 +66,33 @@ int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
 
+template <class Lt, class S, int COLL, int THERM>
+static void launch_batch(lbm_batch* b, cudaStream_t st) {
+  BatchArgs<S> a;
+  a.params = (const StepParams<S>*)b->params;
+  a.chunks = b->chunks;
+  a.nchunks = b->nchunks;
+  a.bc = b->bc;
+  a.nbc = b->nbc;
+  a.par = (int)(b->hs[0]->step & 1);
+  step_list_batch<Lt, S, COLL, THERM><<<b->list_blocks, 128, 0, st>>>(a);
+  if (b->nbc > 0) step_boundary_batch<Lt, S, COLL, THERM><<<b->nbc, 128, 0, st>>>(a);
+  if constexpr (THERM == 2) flip_cells_batch<Lt, S, COLL, THERM><<<dim3(b->flip_blocks, (unsigned)b->hs.size()), 256, 0, st>>>(a);
+}
+
+template <class Lt, class S>
+int dispatch_batch(lbm_batch* b, cudaStream_t st) {
+  const lbm_desc& d = b->hs[0]->d;
+  const int coll = d.collision;
+  const int therm = d.thermal ? (d.pyro ? 2 : 1) : 0;
+#define LBM_CASE(C_, T_) \
+  if (coll == C_ && therm == T_) { launch_batch<Lt, S, C_, T_>(b, st); return LBM_OK; }
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+#undef LBM_CASE
+  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
+}
+
 template <class Lt, class S>
 int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
                   const float* alpha, int solid_bit, cudaStream_t st) {
@@ -84,6 +111,7 @@ int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float*
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
 
+template int dispatch_batch<Lattice<2>, __half>(lbm_batch*, cudaStream_t);
 template int dispatch_step<Lattice<2>, __half>(lbm_handle*, StepParams<__half>, cudaStream_t);
 template int dispatch_init<Lattice<2>, __half>(lbm_handle*, StepParams<__half>, const float*, const float*, const float*,
                                      const float*, int, cudaStream_t);

@@ -34,6 +34,7 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "unknown collision");
   if (d->precision < LBM_PREC_FP32 || d->precision > LBM_PREC_FP64)
     return fail(LBM_ERR_ARG, "unknown precision");
+  if (d->bulk_form < 0 || d->bulk_form > 2) return fail(LBM_ERR_ARG, "bulk_form must be 0, 1 or 2");
   if (d->eos != LBM_EOS_IDEAL_GAS && d->eos != LBM_EOS_INCOMPRESSIBLE)
     return fail(LBM_ERR_ARG, "unknown eos");
   if (d->thermal != LBM_THERMAL_NONE && d->thermal != LBM_THERMAL_CONJUGATE)
@@ -108,6 +109,7 @@ static int build_lists(lbm_handle* h, cudaStream_t st) {
   return h->d.dim == 2 ? build_lists_t<Lattice<2>>(h, st) : build_lists_t<Lattice<3>>(h, st);
 }
 
+
 extern "C" {
 
 int32_t lbm_abi_version(void) { return LBM_ABI_VERSION; }
@@ -150,6 +152,7 @@ int32_t lbm_create(const lbm_desc* d, lbm_handle** out) {
   h->step = 0;
   h->L = plan(*d, default_tx(*d));
   h->diag_valid = false;
+  h->initialised = false;
   *out = h;
   return LBM_OK;
 }
@@ -202,6 +205,87 @@ static int check_bound(lbm_handle* h) {
     return fail(LBM_ERR_UNBOUND, "pyrolysis needs ALPHA and REL bound");
   return LBM_OK;
 }
+
+// ---------------------------------------------------------------- batches
+namespace {
+
+size_t params_bytes(const lbm_desc& d) {
+  if (d.precision == LBM_PREC_FP64) return sizeof(StepParams<double>);
+  if (d.precision == LBM_PREC_FP16) return sizeof(StepParams<__half>);
+  return sizeof(StepParams<float>);
+}
+
+// Checks the members of a batch and reads their list headers (synchronises st).
+int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector<std::vector<int>>& hdr) {
+  if (!hs || n < 1 || !hs[0]) return fail(LBM_ERR_ARG, "a batch needs at least one lattice");
+  const lbm_desc& d0 = hs[0]->d;
+  for (int i = 0; i < n; ++i) {
+    lbm_handle* h = hs[i];
+    if (!h) return fail(LBM_ERR_ARG, "batch member " + std::to_string(i) + " is NULL");
+    int rc = check_bound(h);
+    if (rc) return rc;
+    if (!h->initialised) return fail(LBM_ERR_ARG, "batch member " + std::to_string(i) + " is not initialised");
+    if (!h->L.list)
+      return fail(LBM_ERR_ARG, "batch member " + std::to_string(i) + " does not use cell lists (set bulk_form = 2)");
+    if (h->d.dim != d0.dim || h->d.precision != d0.precision || h->d.collision != d0.collision ||
+        h->d.thermal != d0.thermal || h->d.pyro != d0.pyro)
+      return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, thermal and pyro");
+    if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
+    for (int j = 0; j < i; ++j)
+      if (hs[j] == h) return fail(LBM_ERR_ARG, "a lattice appears twice in the batch");
+  }
+  hdr.assign(n, std::vector<int>(kLhSlots));
+  for (int i = 0; i < n; ++i)
+    LBM_CUDA_TRY(cudaMemcpyAsync(hdr[i].data(), scratch_lhdr(hs[i]), kLhSlots * sizeof(int), cudaMemcpyDeviceToHost, st));
+  LBM_CUDA_TRY(cudaStreamSynchronize(st));
+  return LBM_OK;
+}
+
+// Chunk table: per lattice its current fluid and solid chunks interleaved in
+// proportion, all lattices in order; then every lattice's room for cells that turn
+// fluid (empty until they do).  Boundary block table: (lattice, face, block).
+void batch_tables(lbm_handle* const* hs, int32_t n, const std::vector<std::vector<int>>& hdr,
+                  std::vector<int2>& chunks, std::vector<int4>& bc) {
+  chunks.clear();
+  bc.clear();
+  std::vector<int2> room;
+  for (int i = 0; i < n; ++i) {
+    const std::vector<int>& H = hdr[i];
+    const int fg = H[kLhFg], fe = H[kLhFe], sb = H[kLhSb], sg = H[kLhSg], se = H[kLhSe];
+    const int cf = (fe + 31) / 32, cs = (se - sb + 31) / 32;
+    const int cap = std::min(sb, 32 * cf + (se - sb));  // fluid entries the flips can add
+    const int cr = (cap + 31) / 32 - cf;
+    const long total = (long)cf + cs;
+    long fdone = 0;
+    for (long j = 0; j < total; ++j) {
+      const long f1 = ((j + 1) * cf) / total;
+      if (f1 > fdone) {
+        const int base = (int)(fdone * 32);
+        chunks.push_back(make_int2(i << 2 | 2 | (base < fg ? 1 : 0), base));
+        fdone = f1;
+      } else {
+        const int base = sb + (int)((j - fdone) * 32);
+        chunks.push_back(make_int2(i << 2 | (base < sg ? 1 : 0), base));
+      }
+    }
+    for (int r = 0; r < cr; ++r) room.push_back(make_int2(i << 2 | 2, 32 * (cf + r)));
+    const lbm_desc& d = hs[i]->d;
+    for (int f = 0; f < 6; ++f) {
+      if (!d.side[f].active) continue;
+      const int cells = f < 2 ? d.ny * d.nz : (f < 4 ? d.nx * d.nz : d.nx * d.ny);
+      for (int b = 0; b < (cells + 127) / 128; ++b) bc.push_back(make_int4(i, f, b, 0));
+    }
+  }
+  chunks.insert(chunks.end(), room.begin(), room.end());
+}
+
+size_t batch_bytes(lbm_handle* const* hs, int32_t n, size_t nchunks, size_t nbc) {
+  const size_t p = ((size_t)n * 2 * params_bytes(hs[0]->d) + 255) / 256 * 256;
+  const size_t c = (nchunks * sizeof(int2) + 255) / 256 * 256;
+  return p + c + nbc * sizeof(int4) + 256;
+}
+
+}  // namespace
 
 extern "C" {
 
@@ -260,6 +344,7 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
   }
   rc = build_lists(h, st);
   if (rc) return rc;
+  h->initialised = true;
   h->step = 0;
   h->diag_valid = false;
   return LBM_OK;
@@ -341,6 +426,102 @@ int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
   out->res_num = v[8]; out->res_den = v[9];
   out->step = h->step;
   if (v[6] > 0) return fail(LBM_ERR_NONFINITE, "diagnostics saw NaN/Inf");
+  return LBM_OK;
+}
+
+int32_t lbm_batch_required_bytes(lbm_handle* const* hs, int32_t n, void* stream, size_t* bytes) {
+  if (!bytes) return fail(LBM_ERR_ARG, "bytes is NULL");
+  std::vector<std::vector<int>> hdr;
+  int rc = batch_members(hs, n, (cudaStream_t)stream, hdr);
+  if (rc) return rc;
+  std::vector<int2> chunks;
+  std::vector<int4> bc;
+  batch_tables(hs, n, hdr, chunks, bc);
+  *bytes = batch_bytes(hs, n, chunks.size(), bc.size());
+  return LBM_OK;
+}
+
+int32_t lbm_batch_create(lbm_handle* const* hs, int32_t n, void* dev_scratch, size_t bytes, void* stream,
+                         lbm_batch** out) {
+  if (!out) return fail(LBM_ERR_ARG, "out is NULL");
+  if (!dev_scratch) return fail(LBM_ERR_ARG, "the batch needs a device buffer");
+  cudaStream_t st = (cudaStream_t)stream;
+  std::vector<std::vector<int>> hdr;
+  int rc = batch_members(hs, n, st, hdr);
+  if (rc) return rc;
+  std::vector<int2> chunks;
+  std::vector<int4> bc;
+  batch_tables(hs, n, hdr, chunks, bc);
+  const size_t need = batch_bytes(hs, n, chunks.size(), bc.size());
+  if (bytes < need) return fail(LBM_ERR_SIZE, "batch buffer too small: need " + std::to_string(need) + " bytes");
+  if (chunks.size() > (size_t)INT32_MAX || bc.size() > (size_t)INT32_MAX) return fail(LBM_ERR_SIZE, "batch too large");
+  lbm_batch* b = new lbm_batch();
+  b->hs.assign(hs, hs + n);
+  b->scratch = dev_scratch;
+  b->bytes = bytes;
+  const size_t pb = params_bytes(hs[0]->d);
+  char* base = (char*)dev_scratch;
+  b->params = base;
+  b->chunks = (int2*)(base + ((size_t)n * 2 * pb + 255) / 256 * 256);
+  b->nchunks = (int)chunks.size();
+  b->bc = (int4*)((char*)b->chunks + (chunks.size() * sizeof(int2) + 255) / 256 * 256);
+  b->nbc = (int)bc.size();
+  b->list_blocks = (int)std::max<long>(1, std::min<long>(((long)chunks.size() + 3) / 4,
+                                                          (long)sm_count() * (hs[0]->d.precision == LBM_PREC_FP64 ? 2 : 4)));
+  b->flip_blocks = 4;
+  // parameters of every lattice at both parities, staged on the host
+  std::vector<unsigned char> host((size_t)n * 2 * pb);
+  rc = with_types(hs[0], [&](auto lat, auto s) -> int {
+    using S = decltype(s);
+    (void)lat;
+    for (int i = 0; i < n; ++i)
+      for (int par = 0; par < 2; ++par) {
+        StepParams<S> p = make_params<S>(hs[i], par);
+        std::memcpy(host.data() + ((size_t)i * 2 + par) * pb, &p, pb);
+      }
+    return LBM_OK;
+  });
+  if (rc) { delete b; return rc; }
+  cudaError_t e = cudaMemcpyAsync(b->params, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !chunks.empty())
+    e = cudaMemcpyAsync(b->chunks, chunks.data(), chunks.size() * sizeof(int2), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess && !bc.empty())
+    e = cudaMemcpyAsync(b->bc, bc.data(), bc.size() * sizeof(int4), cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // the host staging vectors go out of scope
+  if (e != cudaSuccess) {
+    delete b;
+    return fail(LBM_ERR_CUDA, std::string("batch tables: ") + cudaGetErrorString(e));
+  }
+  *out = b;
+  return LBM_OK;
+}
+
+int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream) {
+  if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+  if (n < 0) return fail(LBM_ERR_ARG, "n must be >= 0");
+  cudaStream_t st = (cudaStream_t)stream;
+  for (int i = 0; i < n; ++i) {
+    const int rc = with_types(b->hs[0], [&](auto lat, auto s) -> int {
+      using Lt = decltype(lat);
+      using S = decltype(s);
+      return dispatch_batch<Lt, S>(b, st);
+    });
+    if (rc) return rc;
+    for (lbm_handle* h : b->hs) { h->step += 1; h->diag_valid = false; }
+  }
+  LBM_CUDA_TRY(cudaGetLastError());
+  return LBM_OK;
+}
+
+int32_t lbm_batch_advance(lbm_batch* b, int32_t n) {
+  if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+  if (n < 0 || (n & 1)) return fail(LBM_ERR_ARG, "n must be even and >= 0 (a captured sequence keeps the parity)");
+  for (lbm_handle* h : b->hs) { h->step += n; h->diag_valid = false; }
+  return LBM_OK;
+}
+
+int32_t lbm_batch_destroy(lbm_batch* b) {
+  delete b;
   return LBM_OK;
 }
 

@@ -819,11 +819,63 @@ __device__ __forceinline__ void list_turn_fluid(const StepParams<S>& p, int c, c
 //  3. its temperature populations collide as fluid with the heat source that
 //     step_bulk left in rel[B][X].
 template <class L, class S, int COLL, int THERM>
-__global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepParams<S> p) {
+__device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& acc, bool diag,
+                                         bool peek, size_t c0) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr int Q = L::Q, QT = L::QT;
   constexpr bool THERMAL = THERM >= 1;
+  const int np = p.par ^ 1;
+  const uint8_t mk = p.mask[c0];
+  if (!(((mk >> p.par) & 1) && !((mk >> np) & 1))) return;
+  const int c = (int)c0;
+  const int x = c % p.nx, y = (c / p.nx) % p.ny, z = c / (p.nx * p.ny);
+  const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
+  C rb, ux, uy, uz;
+  neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
+  if (peek) {
+    // recomputing the current state: report the state the cell was given
+    if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
+    return;
+  }
+  {
+    C mir[Q];
+    static_for<Q>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if constexpr (k > 0)
+        mir[k] = Store<S>::ld(p.fB, (size_t)L::opp(k) * p.N + c, fshift<L, S, L::opp(k)>(p));
+    });
+    static_for<Q>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if constexpr (k > 0) {
+        const int zc = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
+        if (!K::solid_bit(p, zc, p.par)) Store<S>::st(p.fB, (size_t)k * p.N + zc, mir[k], fshift<L, S, k>(p));
+      }
+    });
+  }
+  {
+    C F[Q];
+    K::feq_all(p, rb, ux, uy, uz, F);
+    K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
+    const uint32_t nbn = K::neighbour_bits(p, nb, np);
+    K::store_flow(p, nb, c, nbn, F);
+    if (p.lhdr) list_turn_fluid<L>(p, c, nb, nbn);
+  }
+  if constexpr (THERMAL) {
+    C G[QT];
+    K::pull_thermal(p, nb, c, G);
+    C T = 0;
+    static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
+    const C dS = p.relB[c];
+    p.relB[c] = (C)0;
+    K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
+    K::store_thermal(p, c, G);
+  }
+  if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
+}
+
+template <class L, class S, int COLL, int THERM>
+__global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepParams<S> p) {
   const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
   DiagAcc<typename Store<S>::C> acc;
   if (diag) acc.clear();
@@ -837,52 +889,7 @@ __global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepPa
   if (listed && !peek && blockIdx.x == 0 && threadIdx.x == 0) p.lhdr[kLhFlip0 + np] = 0;  // for the next pass
   for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
     const size_t c0 = listed ? (size_t)p.flips[(size_t)p.par * p.N + i] : i;
-    const uint8_t mk = p.mask[c0];
-    if (!(((mk >> p.par) & 1) && !((mk >> np) & 1))) continue;
-    const int c = (int)c0;
-    const int x = c % p.nx, y = (c / p.nx) % p.ny, z = c / (p.nx * p.ny);
-    const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-    C rb, ux, uy, uz;
-    neighbour_mean<L, S>(p, x, y, z, rb, ux, uy, uz);
-    if (peek) {
-      // recomputing the current state: report the state the cell was given
-      if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
-      continue;
-    }
-    {
-      C mir[Q];
-      static_for<Q>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        if constexpr (k > 0)
-          mir[k] = Store<S>::ld(p.fB, (size_t)L::opp(k) * p.N + c, fshift<L, S, L::opp(k)>(p));
-      });
-      static_for<Q>([&](auto kk) {
-        constexpr int k = decltype(kk)::value;
-        if constexpr (k > 0) {
-          const int zc = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-          if (!K::solid_bit(p, zc, p.par)) Store<S>::st(p.fB, (size_t)k * p.N + zc, mir[k], fshift<L, S, k>(p));
-        }
-      });
-    }
-    {
-      C F[Q];
-      K::feq_all(p, rb, ux, uy, uz, F);
-      K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
-      const uint32_t nbn = K::neighbour_bits(p, nb, np);
-      K::store_flow(p, nb, c, nbn, F);
-      if (p.lhdr) list_turn_fluid<L>(p, c, nb, nbn);
-    }
-    if constexpr (THERMAL) {
-      C G[QT];
-      K::pull_thermal(p, nb, c, G);
-      C T = 0;
-      static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
-      const C dS = p.relB[c];
-      p.relB[c] = (C)0;
-      K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
-      K::store_thermal(p, c, G);
-    }
-    if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
+    flip_one<L, S, COLL, THERM>(p, acc, diag, peek, c0);
   }
   if (diag) block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blockIdx.x), (size_t)p.partial_rows);
 }
@@ -964,20 +971,14 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
   }
 }
 
-// One thread per boundary cell.  blockIdx.y selects an active face; a cell on
-// several active faces is owned by the lowest-numbered one.
+// Boundary cell i of face `face` (a cell on several active faces is owned by the
+// lowest-numbered one): NEE state, collision, store.
 template <class L, class S, int COLL, int THERM>
-__global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ StepParams<S> p, int4 faces01,
-                                                      int2 faces2) {
+__device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, int i,
+                                              DiagAcc<typename Store<S>::C>& acc, bool diag) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
-  const int fid[6] = {faces01.x, faces01.y, faces01.z, faces01.w, faces2.x, faces2.y};
-  const int face = fid[blockIdx.y];
-  const int i = blockIdx.x * blockDim.x + threadIdx.x;
-  const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
-  DiagAcc<typename Store<S>::C> acc;
-  if (diag) acc.clear();
   int x = 0, y = 0, z = 0;
   bool valid = false;
   if (face == 0 || face == 1) {
@@ -998,23 +999,35 @@ __global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ Ste
       if (on) valid = false;
     }
   }
-  if (valid) {
-    const int c = x + p.nx * (y + p.ny * z);
-    MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z);
-    if (diag) {
-      diag_flow(p, acc, c, s.rho, s.ux, s.uy, s.uz);
-      if (THERMAL) diag_thermal(p, acc, c, s.T);
-    }
-    if (!(p.flags & kStepPeek)) {
-      const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-      K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
-      K::store_flow(p, nb, c, K::neighbour_bits(p, nb, p.par), s.F);
-      if constexpr (THERMAL) {
-        K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
-        K::store_thermal(p, c, s.G);
-      }
+  if (!valid) return;
+  const int c = x + p.nx * (y + p.ny * z);
+  MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z);
+  if (diag) {
+    diag_flow(p, acc, c, s.rho, s.ux, s.uy, s.uz);
+    if (THERMAL) diag_thermal(p, acc, c, s.T);
+  }
+  if (!(p.flags & kStepPeek)) {
+    const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
+    K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
+    K::store_flow(p, nb, c, K::neighbour_bits(p, nb, p.par), s.F);
+    if constexpr (THERMAL) {
+      K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
+      K::store_thermal(p, c, s.G);
     }
   }
+}
+
+// One thread per boundary cell; blockIdx.y selects an active face.
+template <class L, class S, int COLL, int THERM>
+__global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ StepParams<S> p, int4 faces01,
+                                                      int2 faces2) {
+  const int fid[6] = {faces01.x, faces01.y, faces01.z, faces01.w, faces2.x, faces2.y};
+  const int face = fid[blockIdx.y];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const bool diag = (p.flags & (LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) != 0;
+  DiagAcc<typename Store<S>::C> acc;
+  if (diag) acc.clear();
+  boundary_cell<L, S, COLL, THERM>(p, face, i, acc, diag);
   if (diag) {
     const int blk = blockIdx.x + gridDim.x * blockIdx.y;
     block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blk), (size_t)p.partial_rows);

@@ -9,7 +9,8 @@ without CUDA or without the built library raises.
 from __future__ import annotations
 
 import ctypes
-from typing import Optional
+import os
+from typing import Optional, Sequence
 
 import numpy as np
 import torch
@@ -39,10 +40,10 @@ class Lattice:
         self.device = torch.device(device)
         self.stream = stream
         self._desc = cfg.to_desc()
-        import os
         self._staged_env = os.environ.get("LBM_STAGED", "0")[:1] == "1"
-        bulk = os.environ.get("LBM_BULK", "")
+        bulk = cfg.bulk_form if cfg.bulk_form != "auto" else os.environ.get("LBM_BULK", "")
         self._tile_env = bulk == "tile" or (bulk != "list" and cfg.ncells < 65536)
+        self._list_forced = bulk == "list"
         h = ctypes.c_void_p()
         N.check(self.lib.lbm_create(ctypes.byref(self._desc), ctypes.byref(h)))
         self._h = h
@@ -86,7 +87,7 @@ class Lattice:
         """Form of the bulk update this lattice runs: "list" (cell lists; the default from
         65536 cells, or LBM_BULK=list), "tile" (smaller lattices, or LBM_BULK=tile) or
         "staged" (LBM_STAGED=1); fixed when the lattice is created."""
-        if self._staged():
+        if self._staged() and not self._list_forced:
             return "staged"
         return "tile" if self._tile_env else "list"
 
@@ -221,6 +222,83 @@ class Lattice:
             self.lib.lbm_destroy(self._h)
             self._h = ctypes.c_void_p()
         self.buf.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+class LatticeBatch:
+    """Many initialised lattices stepped together (one persistent launch per kernel).
+
+    The lattices must share dim, precision, collision, thermal and pyrolysis
+    settings and use cell lists (``LatticeConfig(bulk_form="list")``); sizes,
+    geometries and parameters are free.  ``capture(n)`` records ``n`` steps (even)
+    as a CUDA graph that ``replay()`` runs again without host work per step."""
+
+    def __init__(self, lattices: Sequence[Lattice], stream: Optional[torch.cuda.Stream] = None):
+        if not lattices:
+            raise ValueError("a batch needs at least one lattice")
+        self.lattices = list(lattices)
+        self.lib = self.lattices[0].lib
+        self.device = self.lattices[0].device
+        self.stream = stream if stream is not None else torch.cuda.Stream(device=self.device)
+        for lat in self.lattices:
+            (lat.stream or torch.cuda.current_stream(lat.device)).synchronize()
+        n = len(self.lattices)
+        self._hs = (ctypes.c_void_p * n)(*[lat._h.value for lat in self.lattices])
+        nbytes = ctypes.c_size_t()
+        s = ctypes.c_void_p(int(self.stream.cuda_stream))
+        N.check(self.lib.lbm_batch_required_bytes(self._hs, n, s, ctypes.byref(nbytes)))
+        self.buf = torch.empty(max(int(nbytes.value), 256), dtype=torch.uint8, device=self.device)
+        b = ctypes.c_void_p()
+        N.check(self.lib.lbm_batch_create(self._hs, n, ctypes.c_void_p(self.buf.data_ptr()), self.buf.numel(), s,
+                                          ctypes.byref(b)))
+        self._b = b
+        self.graph: Optional[torch.cuda.CUDAGraph] = None
+        self._graph_steps = 0
+        self._counted = False
+
+    @property
+    def ncells(self) -> int:
+        return sum(lat.cfg.ncells for lat in self.lattices)
+
+    def step(self, n: int = 1) -> None:
+        N.check(self.lib.lbm_batch_step(self._b, int(n), ctypes.c_void_p(int(self.stream.cuda_stream))))
+
+    def capture(self, n: int) -> None:
+        """Record n batch steps (n even) as a CUDA graph.  Capturing runs no kernel but
+        moves the step counters by n; the first replay() brings the state level with
+        them, every later replay advances both."""
+        if n <= 0 or n % 2:
+            raise ValueError("a captured sequence must have an even number of steps")
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            N.check(self.lib.lbm_batch_step(self._b, int(n), ctypes.c_void_p(int(self.stream.cuda_stream))))
+        self.graph, self._graph_steps, self._counted = g, n, True
+
+    def replay(self) -> None:
+        if self.graph is None:
+            raise RuntimeError("capture() first")
+        with torch.cuda.stream(self.stream):
+            self.graph.replay()
+        if self._counted:
+            self._counted = False
+        else:
+            N.check(self.lib.lbm_batch_advance(self._b, self._graph_steps))
+
+    def synchronize(self) -> None:
+        self.stream.synchronize()
+
+    def close(self) -> None:
+        if getattr(self, "_b", None) is not None and self._b.value:
+            self.stream.synchronize()
+            self.graph = None
+            self.lib.lbm_batch_destroy(self._b)
+            self._b = ctypes.c_void_p()
 
     def __del__(self):
         try:

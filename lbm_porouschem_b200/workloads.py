@@ -11,6 +11,9 @@ physics runs at test sizes.
   thermal tau 0.6 fluid / 0.9 solid, disks r ~ U[10, 20] at porosity 0.45 (512 x 256).
 - ``pyro3d``: D3Q19 (MRT) + D3Q7 + pyrolysis, rho 1.001 -> 1.0 along x, periodic
   in y and z, spheres r ~ U[6, 12] at porosity 0.40 (256^3).
+- ``sweep2d``: a parameter sweep of ``pyro2d``-type lattices, one seed each: size drawn
+  from {128x64, 256x128, 512x256, 1024x512}, porosity ~ U[0.35, 0.65] (overlapping
+  disks r ~ U[0.04, 0.08] ny), flow tau ~ U[0.6, 1.2], inlet T ~ U[0.5, 1.0] (96 lattices).
 Pyrolysis: k = A exp(-E/(R T_K)), T_K = 300 + 500 T, A = 1e8 1/s, E = 1.25e5 J/mol,
 dt = 1e-4 s per step, dH = 4e5 J/kg (endothermic), c_s = 1000 J/(kg K), char yield
 0.25, rho_s = 1 (lattice), a cell turns fluid below reactive fraction 0.01.
@@ -117,3 +120,27 @@ def algorithmic_bytes_per_step(cfg: LatticeConfig, solid: np.ndarray) -> int:
         cb = 8 if cfg.precision == "fp64" else 4
         b += nsolid * 4 * cb   # alpha read + write, release write, release read by neighbours
     return b
+
+
+SWEEP_SIZES = ((128, 64), (256, 128), (512, 256), (1024, 512))
+
+
+def sweep2d(n: int = 96, seed0: int = 0, precision: str = "fp32", collision: str = "bgk",
+            sizes=SWEEP_SIZES) -> list[Workload]:
+    """Lattices of a parameter sweep (uneven sizes), each with cell lists so that they
+    can be stepped as one batch."""
+    out = []
+    for i in range(n):
+        rng = np.random.default_rng(10_000 + seed0 + i)
+        nx, ny = sizes[int(rng.integers(len(sizes)))]
+        phi = float(rng.uniform(0.35, 0.65))
+        tau = float(rng.uniform(0.6, 1.2))
+        t_in = float(rng.uniform(0.5, 1.0))
+        cfg = _pyro_cfg(2, nx, ny, 1, precision, collision, 1.0005, walls=True)
+        cfg.nu = (tau - 0.5) / 3.0
+        cfg.sides[0].T = t_in
+        cfg.bulk_form = "list"
+        solid = packing((nx, ny), 0.04 * ny, 0.08 * ny, phi, seed0 + i, periodic=(False, False), margin=2)
+        out.append(Workload(f"sweep2d_{i:03d}_{nx}x{ny}", cfg, solid, solid.copy(),
+                            {"rho": 1.0, "u": (0.0, 0.0, 0.0), "T": 0.0}))
+    return out
