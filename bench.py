@@ -365,6 +365,9 @@ def sweep_main(args, world, rank, local):
     K = args.graph_steps + (args.graph_steps & 1)
     batch = LatticeBatch(lats)
     batch.step(max(4, args.warmup + (args.warmup & 1)))
+    tuning = batch.tune(steps=4)           # persistent grid picked by timing (real steps)
+    if batch.lattices[0].nsteps & 1:
+        batch.step(1)
     batch.capture(K)
     batch.replay()                      # warm replay (brings the state level with the counters)
     batch.synchronize()
@@ -439,6 +442,8 @@ def sweep_main(args, world, rank, local):
                        "cells": cells, "sizes": sizes, "parallelism": f"replicas x{world}",
                        "sequential_mlups": round(seq_value, 2), "sequential_steps": seq_steps,
                        "batch_vs_sequential": round(value / seq_value, 2),
+                       "tuned_blocks_per_sm": batch.blocks_per_sm,
+                       "tuning_ms_per_step": {str(k): round(v, 4) for k, v in tuning.items()},
                        "l2": "state larger than L2 (no flush needed)"},
             "roofline": {"bound": "hbm", "achieved": round(achieved, 1), "peak": peak, "unit": "GB/s",
                          "frac": round(achieved / peak, 4), "traffic": None,

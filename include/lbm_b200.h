@@ -212,6 +212,9 @@ LBM_API int32_t lbm_batch_create(lbm_handle* const* handles, int32_t n, void* de
  * the step counters (n even: a sequence keeps the step parity it was captured at). */
 LBM_API int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream);
 LBM_API int32_t lbm_batch_advance(lbm_batch* b, int32_t n);
+/* Persistent grid of the batch's bulk kernel: blocks of 128 threads per SM (1-4;
+ * 1-2 in FP64; default the most that stay resident).  For launch-shape tuning. */
+LBM_API int32_t lbm_batch_set_blocks(lbm_batch* b, int32_t blocks_per_sm);
 LBM_API int32_t lbm_batch_destroy(lbm_batch* b);
 
 /* No counterpart in the reference.  The diagnostics of the current state (the

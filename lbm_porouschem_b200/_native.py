@@ -44,6 +44,7 @@ EXPORTED = (
     "lbm_read_diag",
     "lbm_step_count", "lbm_diag_noalloc",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
+    "lbm_batch_set_blocks",
 )
 LBM_NOALLOC_MAX_ROWS = 32768
 
@@ -134,6 +135,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_batch_step.restype = i32
     lib.lbm_batch_advance.argtypes = [vp, i32]
     lib.lbm_batch_advance.restype = i32
+    lib.lbm_batch_set_blocks.argtypes = [vp, i32]
+    lib.lbm_batch_set_blocks.restype = i32
     lib.lbm_batch_destroy.argtypes = [vp]
     lib.lbm_batch_destroy.restype = i32
     if lib.lbm_abi_version() != 1:

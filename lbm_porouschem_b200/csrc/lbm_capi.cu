@@ -513,6 +513,15 @@ int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream) {
   return LBM_OK;
 }
 
+int32_t lbm_batch_set_blocks(lbm_batch* b, int32_t blocks_per_sm) {
+  if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
+  const int cap = b->hs[0]->d.precision == LBM_PREC_FP64 ? 2 : 4;  // resident blocks at the register cap
+  if (blocks_per_sm < 1 || blocks_per_sm > cap)
+    return fail(LBM_ERR_ARG, "blocks_per_sm must be 1.." + std::to_string(cap));
+  b->list_blocks = (int)std::max<long>(1, std::min<long>(((long)b->nchunks + 3) / 4, (long)sm_count() * blocks_per_sm));
+  return LBM_OK;
+}
+
 int32_t lbm_batch_advance(lbm_batch* b, int32_t n) {
   if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
   if (n < 0 || (n & 1)) return fail(LBM_ERR_ARG, "n must be even and >= 0 (a captured sequence keeps the parity)");

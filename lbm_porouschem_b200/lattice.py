@@ -268,6 +268,26 @@ class LatticeBatch:
     def step(self, n: int = 1) -> None:
         N.check(self.lib.lbm_batch_step(self._b, int(n), ctypes.c_void_p(int(self.stream.cuda_stream))))
 
+    def tune(self, steps: int = 4, candidates=None) -> dict:
+        """Pick the persistent grid (blocks per SM) of the bulk kernel by timing ``steps``
+        real batch steps per candidate (they advance the lattices); keeps the fastest.
+        Returns {blocks_per_sm: ms per step}.  Call before capture()."""
+        fp64 = self.lattices[0].cfg.precision == "fp64"
+        cands = candidates or ((1, 2) if fp64 else (2, 3, 4))
+        times = {}
+        for bps in cands:
+            N.check(self.lib.lbm_batch_set_blocks(self._b, int(bps)))
+            self.step(2)                       # settle
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(self.stream)
+            self.step(steps)
+            e1.record(self.stream)
+            e1.synchronize()
+            times[bps] = e0.elapsed_time(e1) / steps
+        self.blocks_per_sm = min(times, key=times.get)
+        N.check(self.lib.lbm_batch_set_blocks(self._b, int(self.blocks_per_sm)))
+        return times
+
     def capture(self, n: int) -> None:
         """Record n batch steps (n even) as a CUDA graph.  Capturing runs no kernel but
         moves the step counters by n; the first replay() brings the state level with

@@ -86,3 +86,21 @@ def test_batch_members_are_checked():
     ws[1].cfg.precision = "fp64"
     with pytest.raises(LBMNativeError, match="share"):
         LatticeBatch(_make(ws))
+
+
+def test_batch_tune_steps_are_real_steps():
+    from lbm_porouschem_b200.lattice import LatticeBatch
+    ws = _fast(workloads.sweep2d(3, seed0=11, sizes=SIZES))
+    single, batched = _make(ws), _make(ws)
+    batch = LatticeBatch(batched)
+    times = batch.tune(steps=2, candidates=(2, 4))
+    assert set(times) == {2, 4} and batch.blocks_per_sm in (2, 4)
+    batch.step(6)
+    batch.synchronize()
+    n = batched[0].nsteps
+    assert n == 2 * (2 + 2) + 6
+    for lat in single:
+        lat.step(n)
+    for a, b in zip(single, batched):
+        _same(a, b)
+    batch.close()
