@@ -45,6 +45,9 @@ EXPORTED = (
     "lbm_step_count", "lbm_diag_noalloc",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
     "lbm_batch_set_blocks",
+    "lbm_nn_conv", "lbm_nn_conv_wgrad", "lbm_nn_bias_grad", "lbm_nn_flip_weights", "lbm_nn_avgpool2",
+    "lbm_nn_avgpool2_bwd", "lbm_nn_upsample2", "lbm_nn_upsample2_bwd", "lbm_nn_mse", "lbm_nn_adam",
+    "lbm_nn_relu_bwd", "lbm_nn_to_bf16",
 )
 LBM_NOALLOC_MAX_ROWS = 32768
 
@@ -137,6 +140,24 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_batch_advance.restype = i32
     lib.lbm_batch_set_blocks.argtypes = [vp, i32]
     lib.lbm_batch_set_blocks.restype = i32
+    f32 = C.c_float
+    nn = {
+        "lbm_nn_conv": [vp, i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_conv_wgrad": [vp, i32, i32, vp, i32, i32, vp, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_bias_grad": [vp, i32, i32, i32, i32, vp, vp],
+        "lbm_nn_flip_weights": [vp, vp, i32, i32, i32, vp],
+        "lbm_nn_avgpool2": [vp, i32, i32, vp, i32, i32, i32, i32, vp],
+        "lbm_nn_avgpool2_bwd": [vp, vp, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_upsample2": [vp, vp, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_upsample2_bwd": [vp, i32, i32, vp, i32, i32, i32, i32, vp],
+        "lbm_nn_mse": [vp, vp, vp, sz, f32, vp, vp, i32, vp],
+        "lbm_nn_adam": [vp, vp, vp, vp, vp, sz, f32, f32, f32, f32, i32, f32, vp],
+        "lbm_nn_relu_bwd": [vp, i32, i32, vp, i32, i32, i32, i32, vp],
+        "lbm_nn_to_bf16": [vp, vp, sz, vp],
+    }
+    for name, args in nn.items():
+        getattr(lib, name).argtypes = args
+        getattr(lib, name).restype = i32
     lib.lbm_batch_destroy.argtypes = [vp]
     lib.lbm_batch_destroy.restype = i32
     if lib.lbm_abi_version() != 1:

@@ -153,7 +153,9 @@ class Lattice:
             if tt is not None:
                 self._view(N.LBM_FIELD_T, cd).copy_(tt.to(cd))
         if N.LBM_FIELD_UPREV in self.buf:
-            self._view(N.LBM_FIELD_UPREV, torch.float32).zero_()
+            # residual reference: the initial velocity (the first residual measures
+            # the change since the start)
+            self._view(N.LBM_FIELD_UPREV, torch.float32).copy_(uu)
 
     def set_sides(self, sides) -> None:
         """Change boundary values (not types) between steps; a pinned host->device copy."""

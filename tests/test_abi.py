@@ -13,6 +13,7 @@ from lbm_porouschem_b200.config import LatticeConfig, SideBC
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "lbm_b200.h"
+HEADERS = sorted((ROOT / "include").glob("*.h"))
 
 
 @pytest.fixture(scope="module")
@@ -23,7 +24,7 @@ def lib():
 
 
 def _declared():
-    txt = HEADER.read_text()
+    txt = "\n".join(h.read_text() for h in HEADERS)
     return sorted(set(re.findall(r"LBM_API\s+[\w\s\*]+?\b(lbm_\w+)\s*\(", txt)))
 
 

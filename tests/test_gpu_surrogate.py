@@ -1,0 +1,194 @@
+"""The warm-start surrogate: its kernels against torch on the CPU in float64 (with the
+same bf16-rounded inputs), the U-Net's gradients against torch autograd, and an
+end-to-end case where the trained network shortens the relaxation.
+
+Tolerances: a single convolution carries one bf16 rounding of its output (relative
+error ~4e-3): 1e-2.  The U-Net keeps bf16 activations through 18 layers while the
+reference keeps float64: gradients agree in direction (cosine > 0.99) and norm (10 %).
+"""
+import ctypes
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+pytestmark = pytest.mark.gpu
+
+
+def _lib():
+    from lbm_porouschem_b200 import _native as N
+    return N, N.load()
+
+
+def _p(t):
+    return ctypes.c_void_p(t.data_ptr())
+
+
+def _s():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def _ref_conv(x, w, k, bias=None):
+    """x: NHWC float64, w: [Cout][k*k][Cin] float64 -> NHWC."""
+    Cout, _, Cin = w.shape
+    wt = w.reshape(Cout, k, k, Cin).permute(0, 3, 1, 2)
+    y = F.conv2d(x.permute(0, 3, 1, 2), wt, bias, padding=k // 2)
+    return y.permute(0, 2, 3, 1)
+
+
+def _rel(a, b):
+    return float((a - b).norm() / b.norm())
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_conv_forward_with_slices(k):
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(k)
+    B, H, W, Cin, Cout = 2, 12, 20, 16, 40
+    buf_in = torch.randn(B, H, W, 24, generator=g).to(torch.bfloat16)    # input = channels 8..23
+    w = (torch.randn(Cout, k * k, Cin, generator=g) * 0.2).to(torch.bfloat16)
+    bias = torch.randn(Cout, generator=g)
+    out = torch.zeros(B, H, W, 48, dtype=torch.bfloat16)                  # output = channels 8..47
+    d_in, d_w, d_b, d_out = buf_in.cuda(), w.cuda(), bias.cuda(), out.cuda()
+    N.check(lib.lbm_nn_conv(_p(d_in), 24, 8, _p(d_w), _p(d_b), None, _p(d_out), None, 48, 8,
+                            B, H, W, Cin, Cout, k, 1, 0, _s()))
+    got = d_out.cpu().double()
+    ref = torch.relu(_ref_conv(buf_in[..., 8:].double(), w.double(), k, bias.double()))
+    assert _rel(got[..., 8:], ref) < 1e-2
+    assert torch.all(got[..., :8] == 0)
+
+
+def test_conv_wgrad_dgrad_bias_match_autograd():
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(5)
+    B, H, W, Cin, Cout, k = 2, 16, 16, 16, 32, 3
+    x = torch.randn(B, H, W, Cin, generator=g).to(torch.bfloat16)
+    w = (torch.randn(Cout, 9, Cin, generator=g) * 0.2).to(torch.bfloat16)
+    dy = torch.randn(B, H, W, Cout, generator=g).to(torch.bfloat16)
+    xr = x.double().requires_grad_(True)
+    wr = w.double().requires_grad_(True)
+    br = torch.zeros(Cout, dtype=torch.float64, requires_grad=True)
+    yr = _ref_conv(xr, wr, k, br)
+    yr.backward(dy.double())
+    dx_, w_, dy_ = x.cuda(), w.cuda(), dy.cuda()
+    dw = torch.zeros(Cout, 9, Cin, device="cuda")
+    db = torch.zeros(Cout, device="cuda")
+    wt = torch.empty(Cin, 9, Cout, dtype=torch.bfloat16, device="cuda")
+    dxo = torch.empty(B, H, W, Cin, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_conv_wgrad(_p(dx_), Cin, 0, _p(dy_), Cout, 0, _p(dw), B, H, W, Cin, Cout, k, _s()))
+    N.check(lib.lbm_nn_bias_grad(_p(dy_), Cout, 0, B * H * W, Cout, _p(db), _s()))
+    N.check(lib.lbm_nn_flip_weights(_p(w_), _p(wt), Cout, 9, Cin, _s()))
+    N.check(lib.lbm_nn_conv(_p(dy_), Cout, 0, _p(wt), None, None, _p(dxo), None, Cin, 0, B, H, W, Cout, Cin, k, 0, 0,
+                            _s()))
+    assert _rel(dw.cpu().double(), wr.grad) < 1e-3                        # FP32 accumulation, no bf16 output
+    assert _rel(db.cpu().double(), br.grad) < 1e-3
+    assert _rel(dxo.cpu().double(), xr.grad) < 1e-2
+
+
+def test_pool_upsample_and_their_gradients():
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(2)
+    B, H, W, C = 2, 8, 12, 16
+    x = torch.randn(B, H, W, 32, generator=g).to(torch.bfloat16)         # slice = channels 16..31
+    d = x.cuda()
+    p = torch.empty(B, H // 2, W // 2, C, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_avgpool2(_p(d), 32, 16, _p(p), B, H, W, C, _s()))
+    ref = F.avg_pool2d(x[..., 16:].double().permute(0, 3, 1, 2), 2).permute(0, 2, 3, 1)
+    assert _rel(p.cpu().double(), ref) < 1e-2
+    up = torch.zeros(B, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_upsample2(_p(p), _p(up), 32, 0, B, H // 2, W // 2, C, _s()))
+    refu = F.interpolate(p.cpu().double().permute(0, 3, 1, 2), scale_factor=2, mode="nearest").permute(0, 2, 3, 1)
+    assert torch.equal(up[..., :C].cpu().double(), refu)
+    gd = torch.empty(B, H // 2, W // 2, C, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_upsample2_bwd(_p(up), 32, 0, _p(gd), B, H // 2, W // 2, C, _s()))
+    assert _rel(gd.cpu().double(), 4 * p.cpu().double()) < 1e-2
+    gi = torch.ones(B, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_avgpool2_bwd(_p(p), _p(gi), 32, 16, B, H, W, C, 1, _s()))
+    refg = 1 + 0.25 * F.interpolate(p.cpu().double().permute(0, 3, 1, 2), scale_factor=2).permute(0, 2, 3, 1)
+    assert _rel(gi[..., 16:].cpu().double(), refg) < 1e-2
+    assert torch.all(gi[..., :16].cpu() == 1)
+
+
+def _torch_unet(net, x):
+    """The same network in float64 on the CPU, with the network's (bf16) weights."""
+    from lbm_porouschem_b200.surrogate import LAYERS
+    W = {k: net.wb[k].cpu().double().requires_grad_(True) for k in LAYERS}
+    Bb = {k: net.b[k].cpu().double().requires_grad_(True) for k in LAYERS}
+
+    def conv(name, t):
+        L = LAYERS[name]
+        y = _ref_conv(t, W[name], L.k, Bb[name])
+        return torch.relu(y) if L.relu else y
+
+    def pool(t):
+        return F.avg_pool2d(t.permute(0, 3, 1, 2), 2).permute(0, 2, 3, 1)
+
+    def up(t):
+        return F.interpolate(t.permute(0, 3, 1, 2), scale_factor=2, mode="nearest").permute(0, 2, 3, 1)
+
+    e0 = conv("e0b", conv("e0a", x))
+    e1 = conv("e1b", conv("e1a", pool(e0)))
+    e2 = conv("e2b", conv("e2a", pool(e1)))
+    b3 = conv("b3b", conv("b3a", pool(e2)))
+    d2 = conv("d2b", conv("d2a", torch.cat([up(conv("r3", b3)), e2], -1)))
+    d1 = conv("d1b", conv("d1a", torch.cat([up(conv("r2", d2)), e1], -1)))
+    d0 = conv("d0b", conv("d0a", torch.cat([up(conv("r1", d1)), e0], -1)))
+    return conv("out", d0), W, Bb
+
+
+def test_unet_gradients_match_autograd():
+    from lbm_porouschem_b200.surrogate import UNet
+    net = UNet(seed=3)
+    g = torch.Generator().manual_seed(4)
+    B, S = 2, 16
+    x = torch.randn(B, S, S, 8, generator=g)
+    x[..., 6:] = 0
+    t = torch.randn(B, S, S, 8, generator=g)
+    wgt = torch.zeros(B, S, S, 8)
+    wgt[..., :4] = 1
+    y = net.forward(x.cuda())
+    loss = net.loss_grad(t.cuda(), wgt.cuda())
+    net.backward(B, S)
+    yr, W, Bb = _torch_unet(net, x.to(torch.bfloat16).double())
+    lr = ((yr - t.double()) ** 2 * wgt.double()).sum() / wgt.sum()
+    lr.backward()
+    assert _rel(y.cpu().double(), yr.detach()) < 5e-2
+    assert abs(loss - lr.item()) / lr.item() < 5e-2
+    for name in ("out", "d0a", "r2", "b3b", "e1a", "e0a"):
+        a = net.dw[name].cpu().double().flatten()
+        b = W[name].grad.flatten()
+        cos = float(a @ b / (a.norm() * b.norm()))
+        assert cos > 0.99, (name, cos)
+        assert abs(float(a.norm() / b.norm()) - 1) < 0.1, name
+        ab = net.db[name].cpu().double()
+        assert _rel(ab, Bb[name].grad) < 0.1, name
+
+
+def test_warm_start_gain():
+    """Train on 96 solved 32x32 cases.  On 6 held-out cases the prediction is a better
+    initial state than rest (velocity and temperature), and the relaxation from it
+    converges to the cold start's permeability; the step counts are printed (at this
+    size and training length the saving is small; 64x64 with 1024 cases: see the
+    warm-start profile)."""
+    from lbm_porouschem_b200 import surrogate as SG
+    S = 32
+    train_cases = [SG.make_case(S, 100 + i) for i in range(96)]
+    test_cases = [SG.make_case(S, 900 + i) for i in range(6)]
+    info = SG.solve_cases(train_cases, tol=1e-6, check=100, max_steps=60_000)
+    assert info["converged"] >= 0.9 * len(train_cases)
+    used = [c for c in train_cases if c.converged]
+    x = SG.inputs(used)
+    t, w = SG.targets(used)
+    net = SG.UNet(seed=0)
+    hist = SG.train(net, x, t, w, epochs=150, batch=8, lr=2e-3)
+    assert hist["loss"][-1] < 0.2 * hist["loss"][0]
+    res = SG.evaluate(net, test_cases, tol=1e-6, check=100, max_steps=60_000)
+    m = res["mean"]
+    print({k: round(v, 5) for k, v in m.items()})
+    for r in res["cases"]:
+        print(r)
+    assert m["cases_converged"] >= 4, m
+    assert m["pre_err_u"] < 1.0, m          # rest is 100 % off
+    assert m["pre_err_T"] < 0.5, m          # a zero temperature field is 100 % off
+    assert m["k_rel_diff_max"] < 1e-2, m    # both runs stop at a residual of 1e-6 per 100 steps
