@@ -56,6 +56,9 @@ extern "C" {
 #define LBM_EOS_INCOMPRESSIBLE 1
 #define LBM_THERMAL_NONE 0
 #define LBM_THERMAL_CONJUGATE 1  /* one temperature distribution over fluid and solid */
+#define LBM_THERMAL_TWOFIELD 2   /* the reference's TF (fluid) and TS (solid) fields: with a binary
+                                    mask they never exchange heat, so fluid-solid links are
+                                    adiabatic (src/LBM/LBM2D/_evolution.py:69-95, :197-200) */
 #define LBM_BC_PERIODIC 0        /* util/flag.py:89-94 BC */
 #define LBM_BC_ZEROGRADIENT 1
 #define LBM_BC_FIXEDVALUE 2
@@ -86,7 +89,7 @@ typedef struct lbm_desc {
   int32_t precision;    /* LBM_PREC_* */
   int32_t eos;          /* LBM_EOS_* */
   int32_t thermal;      /* LBM_THERMAL_* */
-  int32_t pyro;         /* 1: Arrhenius pyrolysis with solid->fluid flip (needs thermal) */
+  int32_t pyro;         /* 1: Arrhenius pyrolysis with solid->fluid flip (needs the conjugate field) */
   int32_t half_force_velocity; /* 1: u includes F/2 (reference: 0) */
   int32_t bulk_form;    /* 0: cell lists from 65536 cells, else tile; 1: tile; 2: cell lists */
   double nu;            /* lattice viscosity visco*dt/dx^2 (_evolution.py:227-249) */

@@ -25,7 +25,7 @@ LBM_ERR_TIMEOUT = 6
 LBM_COLL_BGK, LBM_COLL_MRT = 0, 1
 LBM_PREC_FP32, LBM_PREC_FP16, LBM_PREC_FP64 = 0, 1, 2
 LBM_EOS_IDEAL_GAS, LBM_EOS_INCOMPRESSIBLE = 0, 1
-LBM_THERMAL_NONE, LBM_THERMAL_CONJUGATE = 0, 1
+LBM_THERMAL_NONE, LBM_THERMAL_CONJUGATE, LBM_THERMAL_TWOFIELD = 0, 1, 2
 LBM_BC_PERIODIC, LBM_BC_ZEROGRADIENT, LBM_BC_FIXEDVALUE = 0, 1, 2
 LBM_MASK_SOLID = 3
 LBM_MASK_REACTIVE = 4

@@ -64,7 +64,7 @@ class LatticeConfig:
     nu: float = 0.1                 # lattice viscosity; tau = 3 nu/rho + 1/2 (ideal gas)
     force: tuple = (0.0, 0.0, 0.0)  # body acceleration (lattice units)
     half_force_velocity: bool = False
-    thermal: str = "none"           # "none" | "conjugate"
+    thermal: str = "none"           # "none" | "conjugate" | "two_field" (reference TF/TS, adiabatic interface)
     tauT_fluid: float = 0.6
     tauT_solid: float = 0.9
     pyro: bool = False
@@ -125,7 +125,8 @@ class LatticeConfig:
         d.collision = {"bgk": N.LBM_COLL_BGK, "mrt": N.LBM_COLL_MRT}[self.collision]
         d.precision = {"fp32": N.LBM_PREC_FP32, "fp16": N.LBM_PREC_FP16, "fp64": N.LBM_PREC_FP64}[self.precision]
         d.eos = {"ideal_gas": N.LBM_EOS_IDEAL_GAS, "incompressible": N.LBM_EOS_INCOMPRESSIBLE}[self.eos]
-        d.thermal = {"none": N.LBM_THERMAL_NONE, "conjugate": N.LBM_THERMAL_CONJUGATE}[self.thermal]
+        d.thermal = {"none": N.LBM_THERMAL_NONE, "conjugate": N.LBM_THERMAL_CONJUGATE,
+                     "two_field": N.LBM_THERMAL_TWOFIELD}[self.thermal]
         d.pyro = int(self.pyro)
         d.half_force_velocity = int(self.half_force_velocity)
         d.bulk_form = {"auto": 0, "tile": 1, "list": 2}[self.bulk_form]

@@ -37,10 +37,10 @@ static int validate(const lbm_desc* d) {
   if (d->bulk_form < 0 || d->bulk_form > 2) return fail(LBM_ERR_ARG, "bulk_form must be 0, 1 or 2");
   if (d->eos != LBM_EOS_IDEAL_GAS && d->eos != LBM_EOS_INCOMPRESSIBLE)
     return fail(LBM_ERR_ARG, "unknown eos");
-  if (d->thermal != LBM_THERMAL_NONE && d->thermal != LBM_THERMAL_CONJUGATE)
+  if (d->thermal != LBM_THERMAL_NONE && d->thermal != LBM_THERMAL_CONJUGATE && d->thermal != LBM_THERMAL_TWOFIELD)
     return fail(LBM_ERR_ARG, "unknown thermal mode");
-  if (d->pyro && d->thermal == LBM_THERMAL_NONE)
-    return fail(LBM_ERR_ARG, "pyrolysis needs the thermal field");
+  if (d->pyro && d->thermal != LBM_THERMAL_CONJUGATE)
+    return fail(LBM_ERR_ARG, "pyrolysis needs the conjugate thermal field (heat reaches a reacting cell through it)");
   if (!(d->nu > 0)) return fail(LBM_ERR_ARG, "nu must be > 0");
   if (d->thermal && !(d->tauT_fluid > 0.5 && d->tauT_solid > 0.5))
     return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");

@@ -97,6 +97,7 @@ struct StepParams {
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
+  int adiabatic;   // two-field temperature: no heat across fluid-solid links
   double* partials;    // SoA: partials[i * partial_rows + block]
   int partial_rows;
   int block_offset;
@@ -430,10 +431,22 @@ struct Kern {
       }
     });
   }
-  __device__ __forceinline__ static void store_thermal(const P& p, int c, const C G[QT]) {
+  // Post-collision temperature populations of cell c.  Two-field mode (the
+  // reference's TF / TS, which never exchange heat across a binary mask): a link
+  // to a cell of the other phase is adiabatic, so c stores its population in the
+  // slot the neighbour would have filled, f[opp k][c+e_k], which c pulls back next
+  // step; the neighbour does the same into f[k][c].  Every slot is still written
+  // once and every pull stays unconditional.  nbits: bit k set if c + e_k is solid.
+  __device__ __forceinline__ static void store_thermal(const P& p, const Nbhd& nb, int c, const C G[QT],
+                                                       uint32_t nbits, bool solid) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      Store<S>::st(p.gB, (size_t)k * p.N + c, G[k], gshift<L, S, k>(p));
+      size_t idx = (size_t)k * p.N + c;
+      if constexpr (k > 0) {
+        if (p.adiabatic && (((nbits >> k) & 1) != (uint32_t)solid))
+          idx = (size_t)L::opp(k) * p.N + nb.at(L::ex(k), L::ey(k), L::ez(k));
+      }
+      Store<S>::st(p.gB, idx, G[k], gshift<L, S, k>(p));
     });
   }
 
@@ -708,7 +721,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
       const bool fl = !solid;
       K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
                          fl ? uz : (C)0, dS);
-      K::store_thermal(p, c, G);
+      K::store_thermal(p, nb, c, G, nbits, solid);
     }
     if (diag) diag_thermal(p, acc, c, T);
   }
@@ -869,7 +882,7 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
     K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
-    K::store_thermal(p, c, G);
+    K::store_thermal(p, nb, c, G, 0u, false);  // pyrolysis runs with the conjugate field only
   }
   if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
 }
@@ -1008,11 +1021,12 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   }
   if (!(p.flags & kStepPeek)) {
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
+    const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
     K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
-    K::store_flow(p, nb, c, K::neighbour_bits(p, nb, p.par), s.F);
+    K::store_flow(p, nb, c, nbits, s.F);
     if constexpr (THERMAL) {
       K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
-      K::store_thermal(p, c, s.G);
+      K::store_thermal(p, nb, c, s.G, nbits, false);
     }
   }
 }
@@ -1067,7 +1081,7 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
     C G[QT];
     if (solid) K::geq_all((C)T_in[c], (C)0, (C)0, (C)0, G);
     else K::geq_all((C)T_in[c], ux, uy, uz, G);
-    K::store_thermal(p, (int)c, G);
+    K::store_thermal(p, nb, (int)c, G, nbits, solid);
   }
   if constexpr (PYRO) {
     p.alpha[c] = alpha_in ? (C)alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? (C)1 : (C)0);

@@ -8,7 +8,9 @@ src/LBM/LBM3D/__init__.py:11-62, and run every step through the C ABI.
 
 Supported on the CUDA path: constant viscosity (IDEAL_GAS or INCOMPRESSIBLE),
 binary solid masks with halfway bounce-back, body force (Guo), BGK or MRT,
-the conjugate temperature field (one distribution over fluid and solid), the
+the reference's two temperature fields (TF in fluid, TS in solid; with a binary mask
+they exchange no heat, so the interface is adiabatic), or with pyrolysis the conjugate
+temperature field (one distribution over fluid and solid), the
 single-step pyrolysis model with solid->fluid flip, and NEE boundaries
 (inlet / outlet / wall / symmetric, temperature fixedValue / zeroGradient).
 Features of the reference outside that set raise NotImplementedError with the
@@ -166,7 +168,7 @@ class _SolverBase:
     def description(self) -> str:
         d = f"{self.name}: {self.nx} x {self.ny} x {self.nz} lattice, dx={self.dx}, dt={self.dt}\n"
         d += f"  collision {self.collision.upper()}, storage {self.precision}, viscosity (LU) {self._nu_lu():.6g}\n"
-        d += f"  thermal {'conjugate' if self.TEMPERATURE else 'off'}, pyrolysis {'on' if self._pyro else 'off'}\n"
+        d += f"  thermal {self._thermal_mode()}, pyrolysis {'on' if self._pyro else 'off'}\n"
         return d
 
     # ------------------------------------------------------------ setters (src/LBM/LBM2D/_io.py)
@@ -262,7 +264,7 @@ class _SolverBase:
         self.TS.set_s_BC_value(i, T)
 
     def set_heat_exchange_surface(self, surface):
-        pass  # the conjugate field exchanges heat through the interface itself
+        pass  # binary masks only: no exchange (two fields) or exchange through the interface (conjugate)
 
     def set_heat_exchange_coef(self, coef):
         pass
@@ -312,6 +314,13 @@ class _SolverBase:
             self._reactive = np.asarray(reactive, dtype=bool).reshape(self._shape)
 
     # ------------------------------------------------------------ configuration
+    def _thermal_mode(self) -> str:
+        """The reference's TF / TS fields (adiabatic interface), or the conjugate field
+        that pyrolysis needs (the reacting solid is heated through the interface)."""
+        if not self.TEMPERATURE:
+            return "none"
+        return "conjugate" if self._pyro else "two_field"
+
     def _nu_lu(self) -> float:
         return self.visco * self.dt / self.dx ** 2
 
@@ -341,7 +350,7 @@ class _SolverBase:
             dim=self.DIM, nx=self.nx, ny=self.ny, nz=self.nz, collision=self.collision, precision=self.precision,
             eos="ideal_gas" if self.EOS == FLUID_STATE_EQUATION.IDEAL_GAS else "incompressible",
             nu=self._nu_lu(), force=self.body_force, half_force_velocity=self.half_force_velocity,
-            thermal="conjugate" if self.TEMPERATURE else "none", sides=self._sides())
+            thermal=self._thermal_mode(), sides=self._sides())
         if self.TEMPERATURE:
             cfg.tauT_fluid = self._tau_T(self.TF.thermal_diff)
             cfg.tauT_solid = self._tau_T(self.TS.thermal_diff)

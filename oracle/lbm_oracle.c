@@ -73,7 +73,7 @@ typedef struct orc_cfg {
     double nu;               /* lattice viscosity (visco*dt/dx^2), _evolution.py:227-249 */
     double force[3];         /* body acceleration (new; reference volume_force = 0) */
     int half_force_velocity; /* 1: u = (sum e f + F/2)/rho.  Reference: 0 (_evolution.py:123-130) */
-    int thermal;             /* 0 none, 1 conjugate single field */
+    int thermal;             /* 0 none, 1 conjugate single field, 2 two fields (TF / TS) */
     double tauT_fluid, tauT_solid;
     int pyro;
     double pyro_A, pyro_b, pyro_Ea, pyro_Tmin;  /* Arrhenius, LBM2D/_chemical.py:198-212 */
@@ -339,9 +339,11 @@ static void collide_stream(orc* o) {
                 else o->F[c*Q + o->opp[k]] = fo[k];                      /* :78-79 halfway bounce-back */
             }
         }
-        if (o->c.thermal == 1) {
+        if (o->c.thermal >= 1) {
             /* conjugate single field: fluid geq advects (TF.geq), solid geq = w T (TS.geq,
-             * LBM2D/_thermal.py:162-166); the source enters as geq(dS) (_evolution.py:54-58) */
+             * LBM2D/_thermal.py:162-166); the source enters as geq(dS) (_evolution.py:54-58).
+             * Two fields: TF streams only between fluid cells and TS only between solid
+             * cells (_evolution.py:69-95), so a link to the other phase bounces back */
             REAL tauT = solid ? (REAL)o->c.tauT_solid : (REAL)o->c.tauT_fluid;
             for (int k = 0; k < QT; ++k) {
                 REAL gk = o->g[c*QT + k];
@@ -349,7 +351,11 @@ static void collide_stream(orc* o) {
                 REAL src = o->wt[k]*o->dS[c];
                 go[k] = gk - (REAL)1/tauT*(gk - ge) + src;
             }
-            for (int k = 0; k < QT; ++k) o->G[nbr(o, c, k, +1)*QT + k] = go[k];
+            for (int k = 0; k < QT; ++k) {
+                long ip = nbr(o, c, k, +1);
+                if (o->c.thermal == 2 && k > 0 && is_solid(o->mask, ip) != solid) o->G[c*QT + o->opp[k]] = go[k];
+                else o->G[ip*QT + k] = go[k];
+            }
         }
     }
     /* pyrolysis gas release: a reacting solid cell pushes rel*w_k into each fluid
@@ -388,7 +394,7 @@ static void macro(orc* o) {
             o->rho[c] = r;
             for (int d = 0; d < 3; ++d) o->u[c*3 + d] = j[d];
         }
-        if (o->c.thermal == 1) {
+        if (o->c.thermal >= 1) {
             REAL Tc = 0;
             for (int k = 0; k < QT; ++k) { Tc += o->G[c*QT + k]; o->g[c*QT + k] = o->G[c*QT + k]; }
             o->T[c] = Tc;
@@ -450,7 +456,7 @@ static void nee_cell(orc* o, const orc_side* s, long b, long i) {
     else if (s->rho_type == ORC_BC_ZEROGRAD) o->rho[b] = o->rho[i];
     for (int k = 0; k < Q; ++k)
         o->f[b*Q + k] = feq(o, k, o->rho[b], ub) + (o->f[i*Q + k] - feq(o, k, o->rho[i], ui));
-    if (o->c.thermal == 1) {
+    if (o->c.thermal >= 1) {
         if (s->T_type == ORC_BC_FIXED) o->T[b] = (REAL)s->T;
         else if (s->T_type == ORC_BC_ZEROGRAD) o->T[b] = o->T[i];
         for (int k = 0; k < QT; ++k) {

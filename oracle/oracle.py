@@ -106,7 +106,7 @@ class Oracle:
         for i in range(3):
             c.force[i] = float(cfg.force[i])
         c.half_force_velocity = int(cfg.half_force_velocity)
-        c.thermal = 0 if cfg.thermal == "none" else 1
+        c.thermal = {"none": 0, "conjugate": 1, "two_field": 2}[cfg.thermal]
         c.tauT_fluid, c.tauT_solid = cfg.tauT_fluid, cfg.tauT_solid
         c.pyro = int(cfg.pyro)
         c.pyro_A, c.pyro_b, c.pyro_Ea, c.pyro_Tmin = cfg.pyro_A, cfg.pyro_b, cfg.pyro_Ea, cfg.pyro_Tmin

@@ -160,3 +160,24 @@ def test_nee_pressure_channel(oracle_mod):
     assert np.std(flux) / np.mean(flux) < 1e-2
     assert np.allclose(f["T"][0, :], 1.0)
     assert abs(f["rho"][0, ny // 2] - 1.001) < 1e-12
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_two_field_interface_is_adiabatic(oracle_mod, dim):
+    """Two-field temperature (the reference's TF / TS with a binary mask): no heat crosses
+    the fluid-solid interface, so with periodic sides the fluid and the solid each keep
+    their own total temperature, while the conjugate field exchanges it."""
+    shape = (16, 12) if dim == 2 else (12, 10, 8)
+    solid = np.zeros(shape, dtype=bool)
+    solid[4:9, 3:8] = True
+    T0 = np.where(solid, 1.0, 0.0)
+    tot = {}
+    for mode in ("two_field", "conjugate"):
+        cfg = LatticeConfig(dim=dim, nx=shape[0], ny=shape[1], nz=(1 if dim == 2 else shape[2]), nu=0.1,
+                            thermal=mode, tauT_fluid=0.7, tauT_solid=0.9)
+        o = _run(oracle_mod, cfg, solid, 200, T=T0)
+        T = o.fields()["T"].reshape(shape)
+        tot[mode] = (T[solid].sum(), T[~solid].sum())
+    assert abs(tot["two_field"][0] - solid.sum()) < 1e-9
+    assert abs(tot["two_field"][1]) < 1e-9
+    assert tot["conjugate"][1] > 0.1 * solid.sum()

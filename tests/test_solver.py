@@ -42,6 +42,7 @@ def test_setters_map_to_lattice_config():
     assert (cfg.dim, cfg.nx, cfg.ny, cfg.nz) == (2, 64, 32, 1)
     assert cfg.nu == pytest.approx(2e-5 * 1e-4 / 1e-6)             # visco dt / dx^2
     assert cfg.tau() == pytest.approx(3 * cfg.nu + 0.5)
+    assert cfg.thermal == "two_field"                                  # the reference's TF / TS
     # D2Q5: tau = 3 D + 1/2 with D = diff dt / dx^2 (src/LBM/LBM2D/_scalarField.py tau)
     assert cfg.tauT_fluid == pytest.approx(3 * 3e-5 * 1e-4 / 1e-6 + 0.5)
     assert cfg.tauT_solid == pytest.approx(3 * 1e-5 * 1e-4 / 1e-6 + 0.5)
@@ -137,7 +138,7 @@ def test_solver_steps_like_lattice():
         s.step()
     got = {"rho": s.rho.to_numpy(), "v": s.v.to_numpy(), "T": s.TF.S.to_numpy()}
 
-    cfg = LatticeConfig(dim=2, nx=64, ny=32, nz=1, nu=2e-5 * 1e-4 / 1e-6, thermal="conjugate",
+    cfg = LatticeConfig(dim=2, nx=64, ny=32, nz=1, nu=2e-5 * 1e-4 / 1e-6, thermal="two_field",
                         tauT_fluid=3 * 3e-5 * 1e-4 / 1e-6 + 0.5, tauT_solid=3 * 1e-5 * 1e-4 / 1e-6 + 0.5,
                         T_ref=300.0, T_scale=500.0,
                         sides=[SideBC.inlet((0.01, 0.0, 0.0), FIXED_VALUE, 1.0),
