@@ -1,115 +1,8 @@
-// Explicit instantiation of the step/init launchers for one lattice and one
-// storage precision (split out so the kernels compile in parallel).
-#include "capi_internal.cuh"
+// Launchers for D3Q19 + D3Q7 with FP64 storage.
+#include "launch.cuh"
 
 namespace lbm {
 namespace capi {
-
-template <class Lt, class S, int COLL, int THERM, int MODE>
-static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st) {
-  constexpr size_t smem = list_smem_bytes<Lt, S>(128);
-  if (smem > 0) {
-    // opt in above the 48 KB default: with the static reduction buffer the total can
-    // pass it even when the stages alone do not
-    static bool attr_set = false;  // one attribute call per process and instantiation
-    if (!attr_set) {
-      cudaFuncSetAttribute(step_list<Lt, S, COLL, THERM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr_set = true;
-    }
-  }
-  step_list<Lt, S, COLL, THERM, MODE><<<L.bulk_blocks, 128, smem, st>>>(p);
-}
-
-template <class Lt, class S, int COLL, int THERM>
-static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
-  const Launch& L = h->L;
-  if (L.staged) {
-    using LY = StagedLayout<Lt, S, kStagedTile>;
-    constexpr size_t smem = (size_t)kStagedStages * LY::STAGE_BYTES;
-    static bool attr_set = false;  // one attribute call per process and instantiation
-    if (!attr_set) {
-      cudaFuncSetAttribute(step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
-    }
-    step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages><<<L.bulk_blocks, kStagedTile, smem, st>>>(p);
-  } else if (L.list) {
-    if (p.flags & kStepPeek) launch_list<Lt, S, COLL, THERM, 2>(L, p, st);
-    else if (p.flags) launch_list<Lt, S, COLL, THERM, 1>(L, p, st);
-    else launch_list<Lt, S, COLL, THERM, 0>(L, p, st);
-  } else {
-    step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
-  }
-  if (L.nfaces > 0) {
-    p.block_offset = L.bulk_blocks;
-    const int4 f01 = make_int4(L.faces[0], L.faces[1], L.faces[2], L.faces[3]);
-    const int2 f2 = make_int2(L.faces[4], L.faces[5]);
-    step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, st>>>(p, f01, f2);
-  }
-  if constexpr (THERM == 2) {
-    // after the boundary kernel: it moves mirrored populations of boundary cells too
-    p.block_offset = L.bulk_blocks + L.bc_blocks;
-    flip_cells<Lt, S, COLL, THERM><<<L.flip_blocks, 256, 0, st>>>(p);
-  }
-}
-
-template <class Lt, class S>
-int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
-  const int coll = h->d.collision;
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
-#define LBM_CASE(C_, T_) \
-  if (coll == C_ && therm == T_) { launch_step<Lt, S, C_, T_>(h, p, st); return LBM_OK; }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
-#undef LBM_CASE
-  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
-}
-
-template <class Lt, class S, int COLL, int THERM>
-static void launch_batch(lbm_batch* b, cudaStream_t st) {
-  BatchArgs<S> a;
-  a.params = (const StepParams<S>*)b->params;
-  a.chunks = b->chunks;
-  a.nchunks = b->nchunks;
-  a.bc = b->bc;
-  a.nbc = b->nbc;
-  a.par = (int)(b->hs[0]->step & 1);
-  step_list_batch<Lt, S, COLL, THERM><<<b->list_blocks, 128, 0, st>>>(a);
-  if (b->nbc > 0) step_boundary_batch<Lt, S, COLL, THERM><<<b->nbc, 128, 0, st>>>(a);
-  if constexpr (THERM == 2) flip_cells_batch<Lt, S, COLL, THERM><<<dim3(b->flip_blocks, (unsigned)b->hs.size()), 256, 0, st>>>(a);
-}
-
-template <class Lt, class S>
-int dispatch_batch(lbm_batch* b, cudaStream_t st) {
-  const lbm_desc& d = b->hs[0]->d;
-  const int coll = d.collision;
-  const int therm = d.thermal ? (d.pyro ? 2 : 1) : 0;
-#define LBM_CASE(C_, T_) \
-  if (coll == C_ && therm == T_) { launch_batch<Lt, S, C_, T_>(b, st); return LBM_OK; }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
-#undef LBM_CASE
-  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
-}
-
-template <class Lt, class S>
-int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
-                  const float* alpha, int solid_bit, cudaStream_t st) {
-  const int coll = h->d.collision;
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
-  const int bs = 256;
-  const unsigned nb = (unsigned)((h->N + bs - 1) / bs);
-#define LBM_CASE(C_, T_)                                                                       \
-  if (coll == C_ && therm == T_) {                                                             \
-    init_equilibrium_kernel<Lt, S, C_, T_><<<nb, bs, 0, st>>>(p, rho, u, T, alpha, solid_bit); \
-    return LBM_OK;                                                                             \
-  }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
-#undef LBM_CASE
-  return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
-}
 
 template int dispatch_batch<Lattice<3>, double>(lbm_batch*, cudaStream_t);
 template int dispatch_step<Lattice<3>, double>(lbm_handle*, StepParams<double>, cudaStream_t);

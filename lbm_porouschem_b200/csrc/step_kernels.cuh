@@ -919,8 +919,15 @@ struct MState {
 // State of cell (x,y,z) after the first PASS+1 NEE passes (0: x sides,
 // 1: y sides, 2: z sides), in the reference's loop order
 // (src/LBM/LBM3D/_boundary.py:15-68).  PASS = -1 is the post-stream macro state.
+// With needT false the temperature part (G, T) is left unset.
+//
+// NEE replaces every population of a side cell from its inner neighbour's; of
+// the side cell's own state only what its side's types keep (PERIODIC) is used.
+// So the own state is computed only for such a side: at an inlet or outlet the
+// cell pulls nothing of its own, which halves its loads and drops the sectors it
+// would pull across the periodic wrap.
 template <class L, class S, bool THERMAL, bool PYRO, int PASS>
-__device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z) {
+__device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, int y, int z, bool needT) {
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   MState<L, S> s;
@@ -932,12 +939,13 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
     K::moments(p, s.F, s.rho, s.ux, s.uy, s.uz);
     s.T = 0;
     if constexpr (THERMAL) {
-      K::pull_thermal(p, nb, c, s.G);
-      static_for<L::QT>([&](auto kk) { s.T += s.G[decltype(kk)::value]; });
+      if (needT) {
+        K::pull_thermal(p, nb, c, s.G);
+        static_for<L::QT>([&](auto kk) { s.T += s.G[decltype(kk)::value]; });
+      }
     }
     return s;
   } else {
-    s = bc_state<L, S, THERMAL, PYRO, PASS - 1>(p, x, y, z);
     int side = -1, ix = x, iy = y, iz = z;
     if constexpr (PASS == 0) {
       if ((p.active & 1) && x == 0) { side = 0; ix = 1; }
@@ -949,9 +957,15 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
       if ((p.active & 16) && z == 0) { side = 4; iz = 1; }
       else if ((p.active & 32) && z == p.nz - 1) { side = 5; iz = p.nz - 2; }
     }
-    if (side < 0) return s;
-    const MState<L, S> in = bc_state<L, S, THERMAL, PYRO, PASS - 1>(p, ix, iy, iz);
+    if (side < 0) return bc_state<L, S, THERMAL, PYRO, PASS - 1>(p, x, y, z, needT);
     const lbm_side_desc& sd = p.sides[side];
+    const bool ownT = THERMAL && needT && sd.T_type == LBM_BC_PERIODIC;
+    if (sd.v_type == LBM_BC_PERIODIC || sd.rho_type == LBM_BC_PERIODIC || ownT) {
+      s = bc_state<L, S, THERMAL, PYRO, PASS - 1>(p, x, y, z, ownT);
+    } else {
+      s.rho = s.ux = s.uy = s.uz = s.T = (C)0;  // all set below (F and G entirely)
+    }
+    const MState<L, S> in = bc_state<L, S, THERMAL, PYRO, PASS - 1>(p, ix, iy, iz, needT);
     // _boundary.py:54-65 (flow), _scalarField.py:83-92 (scalar)
     if (sd.v_type == LBM_BC_FIXEDVALUE) { s.ux = (C)sd.v[0]; s.uy = (C)sd.v[1]; s.uz = (C)sd.v[2]; }
     else if (sd.v_type == LBM_BC_ZEROGRADIENT) { s.ux = in.ux; s.uy = in.uy; s.uz = in.uz; }
@@ -968,7 +982,7 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
       s.F[k] = (evb + odb) + (in.F[k] - (evi + odi));
       s.F[o] = (evb - odb) + (in.F[o] - (evi - odi));
     });
-    if constexpr (THERMAL) {
+    if (THERMAL && needT) {
       if (sd.T_type == LBM_BC_FIXEDVALUE) s.T = (C)sd.T;
       else if (sd.T_type == LBM_BC_ZEROGRADIENT) s.T = in.T;
       static_for<L::QT>([&](auto kk) {
@@ -1014,7 +1028,7 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   }
   if (!valid) return;
   const int c = x + p.nx * (y + p.ny * z);
-  MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z);
+  MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z, THERMAL);
   if (diag) {
     diag_flow(p, acc, c, s.rho, s.ux, s.uy, s.uz);
     if (THERMAL) diag_thermal(p, acc, c, s.T);

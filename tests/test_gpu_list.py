@@ -9,7 +9,7 @@ import numpy as np
 import pytest
 
 from lbm_porouschem_b200 import workloads
-from lbm_porouschem_b200.config import LatticeConfig, SideBC
+from lbm_porouschem_b200.config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
 
 pytestmark = pytest.mark.gpu
 
@@ -101,6 +101,44 @@ def test_list_equals_tile_mostly_wrapping_cells(monkeypatch):
         a, _, _ = _run(w, n, "list", monkeypatch)
         b, _, _ = _run(w, n, "tile", monkeypatch)
         _same(a, b)
+
+
+class _W:
+    pass
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_list_equals_tile_with_corner_cells(dim, monkeypatch):
+    """Every side active in 2D (x, y and z in 3D, odd sizes): corner cells take two or
+    three NEE passes, some with a side's own state (PERIODIC types keep it), some
+    without."""
+    rng = np.random.default_rng(15 + dim)
+    shape = (45, 37) if dim == 2 else (21, 19, 13)
+    solid = rng.random(shape) < 0.25
+    keep = np.zeros(shape, dtype=bool)
+    keep[tuple(slice(2, n - 2) for n in shape)] = True
+    solid &= keep                           # sides and their inner neighbours fluid
+    sides = [SideBC.inlet((0.02, 0.0, 0.0), FIXED_VALUE, 1.0),
+             SideBC.outlet(1.0),                                   # T keeps the cell's own
+             SideBC.wall(FIXED_VALUE, 0.5),
+             SideBC(True, PERIODIC, FIXED_VALUE, ZERO_GRADIENT)]  # v keeps the cell's own
+    sides += ([SideBC.wall(ZERO_GRADIENT), SideBC(True, ZERO_GRADIENT, PERIODIC, FIXED_VALUE, T=0.2)]
+              if dim == 3 else [SideBC(), SideBC()])
+    nz = shape[2] if dim == 3 else 1
+    cfg = LatticeConfig(dim=dim, nx=shape[0], ny=shape[1], nz=nz, collision="mrt", nu=0.05, thermal="conjugate",
+                        pyro=True, pyro_A=1.2e11, heat_norm=0.02, gas_coef=0.05, sides=sides)
+    w = _W()
+    w.cfg, w.solid, w.reactive = cfg, solid, solid
+    w.init = {"rho": 1.0, "u": (0.0, 0.0, 0.0), "T": 1.0}
+    a, da, pa = _run(w, 70, "list", monkeypatch, diag=True)
+    b, db, pb = _run(w, 70, "tile", monkeypatch, diag=True)
+    assert np.isfinite(a["u"]).all()
+    _same(a, b)
+    for k in ("mass", "energy", "solid_alpha", "nfluid"):
+        assert da[k] == pytest.approx(db[k], rel=1e-12), k
+        assert pa[k] == pytest.approx(pb[k], rel=1e-12), k
+    for k in ("umax", "Tmin", "Tmax"):
+        assert da[k] == db[k] and pa[k] == pb[k], k
 
 
 @pytest.mark.parametrize("x", [0, 1, 30, 31])

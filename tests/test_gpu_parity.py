@@ -270,3 +270,35 @@ def test_two_field_thermal_fp64(oracle_mod, dim):
     g, r = _compare(lat, o, 1e-10, 1e-10, 1e-10)
     # the solid keeps its temperature: no heat crosses the interface
     assert np.allclose(g["T"].reshape(shape)[solid], 0.5, atol=1e-12)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_nee_every_side_mixed_types_fp64(oracle_mod, dim):
+    """Every side active, with v, rho and T each fixed, extrapolated or kept (PERIODIC
+    type: the side cell's own post-stream value) on some side; corner cells take two or
+    three NEE passes.  FP64 kernels vs the FP64 oracle, conjugate heat with pyrolysis."""
+    from lbm_porouschem_b200.config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, SideBC
+    rng = np.random.default_rng(31 + dim)
+    shape = (36, 28) if dim == 2 else (20, 17, 14)
+    solid = rng.random(shape) < 0.2
+    keep = np.zeros(shape, dtype=bool)
+    keep[tuple(slice(2, n - 2) for n in shape)] = True
+    solid &= keep
+    sides = [SideBC.inlet((0.02, 0.005, 0.0), FIXED_VALUE, 1.0),
+             SideBC.outlet(1.0),
+             SideBC.wall(FIXED_VALUE, 0.5),
+             SideBC(True, PERIODIC, FIXED_VALUE, ZERO_GRADIENT, rho=1.001)]
+    sides += ([SideBC.wall(ZERO_GRADIENT), SideBC(True, ZERO_GRADIENT, PERIODIC, FIXED_VALUE, T=0.2)]
+              if dim == 3 else [SideBC(), SideBC()])
+    cfg = LatticeConfig(dim=dim, nx=shape[0], ny=shape[1], nz=(1 if dim == 2 else shape[2]), collision="mrt",
+                        nu=0.05, thermal="conjugate", pyro=True, pyro_A=1.2e11, heat_norm=0.02, gas_coef=0.05,
+                        precision="fp64", sides=sides)
+
+    class W:
+        pass
+
+    w = W()
+    w.cfg, w.solid, w.reactive = cfg, solid, solid
+    w.init = {"rho": 1.0, "u": (0.0, 0.0, 0.0), "T": 0.8}
+    lat, o = _run_pair(oracle_mod, w, 120, "f64")
+    _compare(lat, o, 1e-10, 1e-10, 1e-10)
