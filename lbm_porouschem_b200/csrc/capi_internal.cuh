@@ -230,7 +230,6 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
     }
     p.mrt_sn[r] = n2 > 0 ? (C)(d.mrt_s[r] / n2) : (C)0;
   }
-  p.adiabatic = d.thermal == LBM_THERMAL_TWOFIELD;
   p.itauT_f = d.thermal ? (C)1 / (C)d.tauT_fluid : (C)0;
   p.itauT_s = d.thermal ? (C)1 / (C)d.tauT_solid : (C)0;
   p.rho0 = (C)d.rho0; p.T0 = (C)d.T0;
@@ -242,6 +241,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;
   p.err = h->ptr[LBM_FIELD_SCRATCH] ? scratch_err(h) : nullptr;
   p.flags = 0;
+  p.adiabatic = d.thermal == LBM_THERMAL_TWOFIELD;
   p.partials = h->ptr[LBM_FIELD_SCRATCH] ? scratch_partials(h) : nullptr;
   p.partial_rows = partial_rows(h->L);
   p.block_offset = 0;

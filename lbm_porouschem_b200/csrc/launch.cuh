@@ -59,11 +59,11 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
 template <class Lt, class S>
 int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const int coll = h->d.collision;
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
+  const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_step<Lt, S, C_, T_>(h, p, st); return LBM_OK; }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -86,11 +86,11 @@ template <class Lt, class S>
 int dispatch_batch(lbm_batch* b, cudaStream_t st) {
   const lbm_desc& d = b->hs[0]->d;
   const int coll = d.collision;
-  const int therm = d.thermal ? (d.pyro ? 2 : 1) : 0;
+  const int therm = d.thermal ? (d.pyro ? 2 : (d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_batch<Lt, S, C_, T_>(b, st); return LBM_OK; }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -99,7 +99,7 @@ template <class Lt, class S>
 int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
                   const float* alpha, int solid_bit, cudaStream_t st) {
   const int coll = h->d.collision;
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : 1) : 0;
+  const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
   const int bs = 256;
   const unsigned nb = (unsigned)((h->N + bs - 1) / bs);
 #define LBM_CASE(C_, T_)                                                                       \
@@ -107,8 +107,8 @@ int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float*
     init_equilibrium_kernel<Lt, S, C_, T_><<<nb, bs, 0, st>>>(p, rho, u, T, alpha, solid_bit); \
     return LBM_OK;                                                                             \
   }
-  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2)
-  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2)
+  LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
+  LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }

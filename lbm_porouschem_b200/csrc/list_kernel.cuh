@@ -19,9 +19,9 @@
 // temperature field solid cells have no work and are not listed either.
 //
 // step_list<> is a persistent kernel: each warp walks chunks of 32 entries
-// (fluid chunks first, then solid chunks, strided over all warps so that every
-// block gets the same mix), loading the next chunk's entry while it updates the
-// current one.  The per-cell arithmetic is cell_update<>, shared with the tile
+// (fluid and solid chunks interleaved in proportion, strided over all warps so
+// that every block gets the same mix), loading the next chunk's entry while it
+// updates the current one.  The per-cell arithmetic is cell_update<>, shared with the tile
 // kernel, so both forms give the same fields bit for bit.
 //
 // A cell that turns fluid (flip_cells<>) marks its solid entry dead, appends a
@@ -424,7 +424,9 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ St
         const SP src{stage0 + st * stage_elems, stride};
         solid_next = cell_update<L, S, COLL, THERM>(p, cacc, diag, peek, c, nb, nbits, solid, reactive, mk, src);
       } else {
-        solid_next = cell_update<L, S, COLL, THERM>(p, cacc, diag, peek, c, nb, nbits, solid, reactive, mk);
+        // the ordinary step takes store_thermal<>'s run-time form (fewer spills)
+        solid_next = cell_update<L, S, COLL, THERM, GlobalPull<L, S>, MODE == 0>(p, cacc, diag, peek, c, nb, nbits,
+                                                                                 solid, reactive, mk);
       }
       if (diag) s_acc.merge(threadIdx.x, cacc);
       if (!peek) {

@@ -328,7 +328,7 @@ __global__ void __launch_bounds__(TILE, (std::is_same<S, double>::value ? 1 : 4)
           const bool fl = !solid;
           K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
                              fl ? uz : (C)0, dS);
-          K::store_thermal(p, nb, c, G, nbits, solid);
+          K::template store_thermal<THERM == 3>(p, nb, c, G, nbits, solid);
         }
         if (diag) diag_thermal(p, acc, c, T);
       }

@@ -97,7 +97,7 @@ struct StepParams {
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
-  int adiabatic;   // two-field temperature: no heat across fluid-solid links
+  int adiabatic;   // two-field temperature (store_thermal<>'s run-time form)
   double* partials;    // SoA: partials[i * partial_rows + block]
   int partial_rows;
   int block_offset;
@@ -437,13 +437,19 @@ struct Kern {
   // slot the neighbour would have filled, f[opp k][c+e_k], which c pulls back next
   // step; the neighbour does the same into f[k][c].  Every slot is still written
   // once and every pull stays unconditional.  nbits: bit k set if c + e_k is solid.
+  // ADIA (the two-field kernels) selects the adiabatic links at compile time; RT
+  // tests p.adiabatic at run time instead.  The run-time form is what the ordinary
+  // step of the list kernel uses: with it that loop is register-allocated with fewer
+  // spills (256^3 D3Q19-MRT + D3Q7 + pyrolysis, FP32: 11.7 against 11.3 GLUPS), while
+  // in the diagnostics step it costs spills that nearly double the time.
+  template <bool ADIA, bool RT = false>
   __device__ __forceinline__ static void store_thermal(const P& p, const Nbhd& nb, int c, const C G[QT],
                                                        uint32_t nbits, bool solid) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       size_t idx = (size_t)k * p.N + c;
-      if constexpr (k > 0) {
-        if (p.adiabatic && (((nbits >> k) & 1) != (uint32_t)solid))
+      if constexpr ((ADIA || RT) && k > 0) {
+        if ((ADIA || p.adiabatic) && ((nbits >> k) & 1) != (uint32_t)solid)
           idx = (size_t)L::opp(k) * p.N + nb.at(L::ex(k), L::ey(k), L::ez(k));
       }
       Store<S>::st(p.gB, idx, G[k], gshift<L, S, k>(p));
@@ -627,7 +633,8 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
 }
 
 // ------------------------------------------------------------------ kernels
-// THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis.
+// THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis, 3 two-field
+// (adiabatic fluid-solid links).
 
 // Where cell_update<> takes its post-stream populations from: straight from the
 // input buffers in HBM (this source), or from copies staged in shared memory
@@ -652,7 +659,7 @@ struct GlobalPull {
 // the diagnostics.  nbits: bit k set if c + e_k is solid at this parity.  mk is
 // the mask byte (read only by a peek pass over a reactive cell).  Returns whether
 // the cell is solid at the next parity.
-template <class L, class S, int COLL, int THERM, class Src = GlobalPull<L, S>>
+template <class L, class S, int COLL, int THERM, class Src = GlobalPull<L, S>, bool RT = false>
 __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& acc, bool diag, bool peek, int c,
                                             const Nbhd& nb, uint32_t nbits, bool solid, bool reactive,
                                             uint8_t mk, const Src& src = Src()) {
@@ -721,7 +728,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
       const bool fl = !solid;
       K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
                          fl ? uz : (C)0, dS);
-      K::store_thermal(p, nb, c, G, nbits, solid);
+      K::template store_thermal<THERM == 3, RT>(p, nb, c, G, nbits, solid);
     }
     if (diag) diag_thermal(p, acc, c, T);
   }
@@ -882,7 +889,7 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
     K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
-    K::store_thermal(p, nb, c, G, 0u, false);  // pyrolysis runs with the conjugate field only
+    K::template store_thermal<false>(p, nb, c, G, 0u, false);  // pyrolysis runs with the conjugate field only
   }
   if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
 }
@@ -1040,7 +1047,7 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
     K::store_flow(p, nb, c, nbits, s.F);
     if constexpr (THERMAL) {
       K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
-      K::store_thermal(p, nb, c, s.G, nbits, false);
+      K::template store_thermal<THERM == 3>(p, nb, c, s.G, nbits, false);
     }
   }
 }
@@ -1095,7 +1102,7 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
     C G[QT];
     if (solid) K::geq_all((C)T_in[c], (C)0, (C)0, (C)0, G);
     else K::geq_all((C)T_in[c], ux, uy, uz, G);
-    K::store_thermal(p, nb, (int)c, G, nbits, solid);
+    K::template store_thermal<THERM == 3>(p, nb, (int)c, G, nbits, solid);
   }
   if constexpr (PYRO) {
     p.alpha[c] = alpha_in ? (C)alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? (C)1 : (C)0);
