@@ -175,6 +175,19 @@ LBM_API int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, vo
 LBM_API int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,
                              const float* alpha, void* stream);
 
+/* Continue from a saved state instead of initialising (checkpoint / resume).
+ * The caller has filled the bound buffers with the state saved before step
+ * `step` was taken: the half of F and of G that step reads (half step & 1 of the
+ * A/B pair), MASK, ALPHA, the REL plane step & 1, and UPREV.  Sets the step
+ * counter, makes both parity bits of every mask byte equal to bit step & 1 (so a
+ * cell that turned fluid on the last saved pass is fluid for both), checks the
+ * side layers as lbm_init_equilibrium does (and synchronises `stream` once when a
+ * side is active) and rebuilds the cell lists.  Stepping on from here gives the
+ * same fields, bit for bit, as the run that saved the state.  No reference
+ * counterpart: the reference's export_snapshot is a reserved no-op
+ * (src/LBM/LBM2D/_io.py:589-598) and it has no restart. */
+LBM_API int32_t lbm_resume(lbm_handle* h, int64_t step, void* stream);
+
 /* Advance n lattice steps.  Replaces step() / step_kernel()
  * (src/LBM/LBM2D/_evolution.py:12-25, src/LBM/LBM3D/_evolution.py:11-25). */
 LBM_API int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream);

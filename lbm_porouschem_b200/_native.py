@@ -40,7 +40,7 @@ LBM_STEP_RESIDUAL = 4
 
 EXPORTED = (
     "lbm_abi_version", "lbm_last_error", "lbm_required_bytes", "lbm_create", "lbm_destroy",
-    "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_step", "lbm_compute_macro",
+    "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_resume", "lbm_step", "lbm_compute_macro",
     "lbm_read_diag",
     "lbm_step_count", "lbm_diag_noalloc",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
@@ -120,6 +120,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_set_sides.restype = i32
     lib.lbm_init_equilibrium.argtypes = [vp, vp, vp, vp, vp, vp]
     lib.lbm_init_equilibrium.restype = i32
+    lib.lbm_resume.argtypes = [vp, i64, vp]
+    lib.lbm_resume.restype = i32
     lib.lbm_step.argtypes = [vp, i32, i32, vp]
     lib.lbm_step.restype = i32
     lib.lbm_compute_macro.argtypes = [vp, i32, vp]

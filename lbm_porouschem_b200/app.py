@@ -8,8 +8,10 @@ GPU; ``collision`` / ``precision`` select BGK|MRT and fp32|fp16|fp64), ``spaceCo
 (single-step pyrolysis of reactive solid zones), ``boundaryCondition`` (inlet / outlet / wall /
 periodic flow sides, fixedValue / zeroGradient / periodic temperature), ``geometry`` (sphere,
 cylinder, cone, box voxelised analytically at cell centres), ``initialCondition`` (flow, thermal,
-concrete / substract solids) and ``outputControl`` (log interval; ``vtk`` writes ``.npz`` field
-files). Options outside that set stop the run with NotImplementedError naming the option.
+concrete / substract solids) and ``outputControl`` (log interval; ``vtk`` writes ``.vts`` files
+and the ``.pvd`` series; ``snapshot`` writes checkpoints).  ``timeControl.restart`` names a
+checkpoint to continue from instead of initialising (no reference counterpart).  Options outside
+that set stop the run with NotImplementedError naming the option.
 """
 from __future__ import annotations
 
@@ -262,10 +264,20 @@ def application(config: dict, logger: logging.Logger, max_steps: int | None = No
             import shutil
             shutil.rmtree(export_path, ignore_errors=True)
         os.makedirs(export_path, exist_ok=True)
-        lb.exportPath = export_path
+        lb.set_vtk_path(export_path)
+    # src/LBM/app.py:639-643, 670-671 (the reference's export_snapshot is empty)
+    snap = oc.get("snapshot") or {}
+    snapshot_every = int(round(float(snap.get("interval", 100)) / lb.dt)) if snap else 0
+    if snap.get("path"):
+        lb.snapshotPath = snap["path"]
 
-    logger.info("Simulation initializing...")
-    lb.init_simulation()
+    restart = tc.get("restart")
+    if restart:
+        logger.info(f"Continuing from {restart}")
+        lb.load_snapshot(restart)
+    else:
+        logger.info("Simulation initializing...")
+        lb.init_simulation()
     logger.info(lb.description())
     cells = lb.nx * lb.ny * lb.nz
     pre = time.time()
@@ -278,18 +290,10 @@ def application(config: dict, logger: logging.Logger, max_steps: int | None = No
             logger.info(f"Execution time:{dtw:.2f} s , Collapsed time:{time.time() - start:.2f} s, MLUPS = {mlups:.2f}")
             logger.info(lb.log_info())
         if export_every and lb.tLattice % export_every == 0:
-            export_npz(lb, export_path)
+            lb.export_VTK_pyvista()
+        if snapshot_every and lb.tLattice % snapshot_every == 0:
+            lb.export_snapshot(config)
         lb.step()
         steps += 1
     logger.info("LBM finished.")
     return lb
-
-
-def export_npz(lb, path: str) -> str:
-    """Field snapshot in place of the reference's VTK export: rho, v, solid (and T)."""
-    out = {"rho": lb.rho.to_numpy(), "v": lb.v.to_numpy(), "solid": lb.solid.to_numpy()}
-    if lb.TEMPERATURE:
-        out["T"] = lb.TF.get_physical_value(lb.TF.S.to_numpy())
-    fn = os.path.join(path, f"{lb.name}_{lb.tLattice:08d}.npz")
-    np.savez_compressed(fn, **out)
-    return fn

@@ -105,6 +105,20 @@ class LatticeConfig:
         c.sides = [dataclasses.replace(s) for s in (kw.get("sides") or self.sides)]
         return c
 
+    def to_dict(self) -> dict:
+        """Plain JSON-able form (checkpoints)."""
+        d = dataclasses.asdict(self)
+        d["mrt_rates"] = {str(k): v for k, v in self.mrt_rates.items()}
+        return d
+
+    @staticmethod
+    def from_dict(d: dict) -> "LatticeConfig":
+        d = dict(d)
+        d["force"] = tuple(d["force"])
+        d["mrt_rates"] = {int(k): float(v) for k, v in d.get("mrt_rates", {}).items()}
+        d["sides"] = [SideBC(**{**s, "v": tuple(s["v"])}) for s in d["sides"]]
+        return LatticeConfig(**d)
+
     def tau(self, rho: float = 1.0) -> float:
         nu = self.nu / rho if self.eos == "ideal_gas" else self.nu
         return 3.0 * nu + 0.5

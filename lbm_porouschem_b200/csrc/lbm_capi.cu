@@ -75,6 +75,38 @@ static __global__ void __launch_bounds__(256) check_sides_kernel(const uint8_t* 
   }
 }
 
+// Both parity bits of every mask byte from bit `bit` (the state a resumed run
+// reads first); the reactive bit is kept.
+static __global__ void __launch_bounds__(256) normalise_mask_kernel(uint8_t* mask, size_t N, int bit) {
+  const size_t stride = (size_t)gridDim.x * blockDim.x;
+  for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += stride) {
+    const uint8_t m = mask[c];
+    mask[c] = (uint8_t)((m & ~LBM_MASK_SOLID) | (((m >> bit) & 1) ? LBM_MASK_SOLID : 0u));
+  }
+}
+
+// Side-layer check (check_sides_kernel); synchronises st when a side is active.
+static int check_sides(lbm_handle* h, cudaStream_t st) {
+  int active = 0;
+  for (int s = 0; s < 6; ++s) if (h->d.side[s].active) active |= 1 << s;
+  int flag = 0;
+  LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
+  if (active) {
+    check_sides_kernel<<<2 * sm_count(), 256, 0, st>>>((const uint8_t*)h->ptr[LBM_FIELD_MASK], h->d.nx, h->d.ny,
+                                                      h->d.nz, active, h->N, scratch_err(h));
+    LBM_CUDA_TRY(cudaGetLastError());
+    LBM_CUDA_TRY(cudaMemcpyAsync(&flag, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
+    LBM_CUDA_TRY(cudaStreamSynchronize(st));
+  }
+  if (flag & 4) {
+    LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
+    return fail(LBM_ERR_ARG,
+                "a solid cell lies on an active (NEE) side or next to one; the two outer layers of an active "
+                "side must be fluid");
+  }
+  return LBM_OK;
+}
+
 // Cell lists of the step_list kernel from the (normalised) mask; runs after the
 // equilibrium initialisation, on the caller's stream.
 template <class Lt>
@@ -323,29 +355,31 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
   });
   if (rc) return rc;
   LBM_CUDA_TRY(cudaGetLastError());
-  {
-    int active = 0;
-    for (int s = 0; s < 6; ++s) if (h->d.side[s].active) active |= 1 << s;
-    int flag = 0;
-    LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
-    if (active) {
-      check_sides_kernel<<<2 * sm_count(), 256, 0, st>>>((const uint8_t*)h->ptr[LBM_FIELD_MASK], h->d.nx, h->d.ny,
-                                                        h->d.nz, active, h->N, scratch_err(h));
-      LBM_CUDA_TRY(cudaGetLastError());
-      LBM_CUDA_TRY(cudaMemcpyAsync(&flag, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
-      LBM_CUDA_TRY(cudaStreamSynchronize(st));
-    }
-    if (flag & 4) {
-      LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
-      return fail(LBM_ERR_ARG,
-                  "a solid cell lies on an active (NEE) side or next to one; the two outer layers of an active "
-                  "side must be fluid");
-    }
-  }
+  rc = check_sides(h, st);
+  if (rc) return rc;
   rc = build_lists(h, st);
   if (rc) return rc;
   h->initialised = true;
   h->step = 0;
+  h->diag_valid = false;
+  return LBM_OK;
+}
+
+int32_t lbm_resume(lbm_handle* h, int64_t step, void* stream) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  if (step < 0) return fail(LBM_ERR_ARG, "step must be >= 0");
+  int rc = check_bound(h);
+  if (rc) return rc;
+  cudaStream_t st = (cudaStream_t)stream;
+  LBM_CUDA_TRY(cudaMemcpyAsync(scratch_sides(h), h->d.side, kCtrlBytes, cudaMemcpyHostToDevice, st));
+  normalise_mask_kernel<<<2 * sm_count(), 256, 0, st>>>((uint8_t*)h->ptr[LBM_FIELD_MASK], h->N, (int)(step & 1));
+  LBM_CUDA_TRY(cudaGetLastError());
+  rc = check_sides(h, st);
+  if (rc) return rc;
+  rc = build_lists(h, st);  // both parity bits are equal now, so parity 0 lists the current state
+  if (rc) return rc;
+  h->initialised = true;
+  h->step = step;
   h->diag_valid = false;
   return LBM_OK;
 }

@@ -9,6 +9,7 @@ without CUDA or without the built library raises.
 from __future__ import annotations
 
 import ctypes
+import json
 import os
 from typing import Optional, Sequence
 
@@ -216,6 +217,85 @@ class Lattice:
         m = self.mask.cpu().numpy()
         out["solid"] = from_flat(((m >> par) & 1).astype(bool), cfg.shape)
         return out
+
+    # ------------------------------------------------------- checkpoint / resume
+    def _state_arrays(self) -> dict:
+        """Device state the next step reads, as host arrays (storage precision)."""
+        cfg, n = self.cfg, self.cfg.ncells
+        half = self.nsteps & 1
+        sd, cd = _STORE_DTYPE[cfg.precision], _COMPUTE_DTYPE[cfg.precision]
+        (self.stream or torch.cuda.current_stream()).synchronize()
+        out = {"f": self._view(N.LBM_FIELD_F, sd).view(2, cfg.Q, n)[half].cpu().numpy(),
+               "mask": self.mask.cpu().numpy()}
+        if N.LBM_FIELD_G in self.buf:
+            out["g"] = self._view(N.LBM_FIELD_G, sd).view(2, cfg.QT, n)[half].cpu().numpy()
+        if N.LBM_FIELD_ALPHA in self.buf:
+            out["alpha"] = self._view(N.LBM_FIELD_ALPHA, cd).cpu().numpy()
+        if N.LBM_FIELD_REL in self.buf:
+            out["rel"] = self._view(N.LBM_FIELD_REL, cd).view(2, n)[half].cpu().numpy()
+        for fid, name in ((N.LBM_FIELD_RHO, "rho"), (N.LBM_FIELD_U, "u"), (N.LBM_FIELD_T, "T")):
+            if fid in self.buf:
+                out[name] = self._view(fid, cd).cpu().numpy()
+        if N.LBM_FIELD_UPREV in self.buf:
+            out["uprev"] = self._view(N.LBM_FIELD_UPREV, torch.float32).cpu().numpy()
+        return out
+
+    def save_checkpoint(self, path) -> str:
+        """Write the state to ``path`` (numpy .npz, uncompressed): the halves of the flow and
+        temperature populations and the gas-release plane that the next step reads, the
+        mask, reactive fraction, residual reference and macro planes, in their device
+        precision, with the step count and the configuration.  ``Lattice.load_checkpoint``
+        continues from it with the same fields, bit for bit.  (The reference has no
+        restart; its export_snapshot is a reserved no-op, src/LBM/LBM2D/_io.py:589-598.)"""
+        if not self.nsteps and self._init_fields is None:
+            raise RuntimeError("nothing to save: the lattice is not initialised")
+        meta = {"format": "lbm_b200 checkpoint", "version": 1, "step": self.nsteps,
+                "config": self.cfg.to_dict()}
+        arrays = self._state_arrays()
+        path = os.fspath(path)
+        with open(path, "wb") as fh:
+            np.savez(fh, meta=np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8), **arrays)
+        return path
+
+    @classmethod
+    def load_checkpoint(cls, path, device: str | torch.device = "cuda",
+                        stream: Optional[torch.cuda.Stream] = None) -> "Lattice":
+        """A new lattice holding the state saved by ``save_checkpoint`` (lbm_resume)."""
+        with np.load(os.fspath(path)) as z:
+            meta = json.loads(bytes(z["meta"]).decode())
+            if meta.get("format") != "lbm_b200 checkpoint" or meta.get("version") != 1:
+                raise ValueError(f"{path}: not an lbm_b200 checkpoint (version 1)")
+            lat = cls(LatticeConfig.from_dict(meta["config"]), device=device, stream=stream)
+            lat._restore({k: z[k] for k in z.files if k != "meta"}, int(meta["step"]))
+        return lat
+
+    def _restore(self, arrays: dict, step: int) -> None:
+        cfg, n = self.cfg, self.cfg.ncells
+        half = step & 1
+        sd, cd = _STORE_DTYPE[cfg.precision], _COMPUTE_DTYPE[cfg.precision]
+
+        def put(dst: torch.Tensor, name: str):
+            a = arrays.get(name)
+            if a is None or a.size != dst.numel():
+                raise ValueError(f"checkpoint field {name!r} is missing or has the wrong size")
+            dst.copy_(torch.from_numpy(np.ascontiguousarray(a).reshape(dst.shape)).to(self.device))
+
+        with self._on_stream():
+            put(self._view(N.LBM_FIELD_F, sd).view(2, cfg.Q, n)[half], "f")
+            put(self.mask, "mask")
+            if N.LBM_FIELD_G in self.buf:
+                put(self._view(N.LBM_FIELD_G, sd).view(2, cfg.QT, n)[half], "g")
+            if N.LBM_FIELD_ALPHA in self.buf:
+                put(self._view(N.LBM_FIELD_ALPHA, cd), "alpha")
+            if N.LBM_FIELD_REL in self.buf:
+                put(self._view(N.LBM_FIELD_REL, cd).view(2, n)[half], "rel")
+            for fid, name in ((N.LBM_FIELD_RHO, "rho"), (N.LBM_FIELD_U, "u"), (N.LBM_FIELD_T, "T")):
+                if fid in self.buf:
+                    put(self._view(fid, cd), name)
+            if N.LBM_FIELD_UPREV in self.buf:
+                put(self._view(N.LBM_FIELD_UPREV, torch.float32), "uprev")
+            N.check(self.lib.lbm_resume(self._h, int(step), self._s()))
+        self._init_fields = {}
 
     def close(self) -> None:
         if getattr(self, "buf", None):

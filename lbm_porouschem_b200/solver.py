@@ -19,12 +19,14 @@ reason instead of silently running something else.
 from __future__ import annotations
 
 import logging
+import os
 from typing import Callable, Optional
 
 import numpy as np
 
 from .config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
 from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, SOURCE_TERM, VISCOSITY_MODEL
+from .vtk import PVDWriter, write_vts
 
 _BC_CODE = {BC.periodic: PERIODIC, BC.zeroGradient: ZERO_GRADIENT, BC.fixedValue: FIXED_VALUE}
 _log = logging.getLogger("LBM 2D logger")
@@ -145,6 +147,11 @@ class _SolverBase:
         self.GetVariableFunc: list[Callable] = []
         self.exportPath = "vtk"
         self.snapshotPath = "snapshot.yaml"
+        self.PVD = PVDWriter(self.exportPath, name)
+        # node coordinates of the VTK grid (src/LBM/LBM2D/_core.py:38-40)
+        self.x = np.linspace(0, X, self.nx)
+        self.y = np.linspace(0, Y, self.ny)
+        self.z = np.linspace(0, Z, self.nz)
         self.rho = Field(self, "rho", 0, 1.0)
         self.v = Field(self, "v", 3, 0.0)
         self.solid = Field(self, "solid", 0, 0.0)
@@ -174,6 +181,7 @@ class _SolverBase:
     # ------------------------------------------------------------ setters (src/LBM/LBM2D/_io.py)
     def set_vtk_path(self, path):
         self.exportPath = path
+        self.PVD.exportPath = path
 
     def init_field(self, field: Field, param):
         field.from_numpy(_as_array(param, self._shape))
@@ -455,14 +463,55 @@ class _SolverBase:
                   f"Max temperature : {self.TF.get_physical_value(d['Tmax']):.7f}")
         return p
 
-    def export_snapshot(self, config=None):
-        pass  # the reference's snapshot export is a no-op too (src/LBM/LBM2D/_io.py:589-598)
+    def export_snapshot(self, config=None) -> Optional[str]:
+        """Checkpoint of the lattice state (Lattice.save_checkpoint) to
+        ``<snapshotPath stem>_<tLattice>.npz``; ``load_snapshot`` continues from it bit for
+        bit.  The reference reserves this call for a binary dump and leaves it empty
+        (src/LBM/LBM2D/_io.py:589-598)."""
+        if self._lat is None:
+            return None
+        stem = os.path.splitext(self.snapshotPath)[0] if self.snapshotPath else self.name
+        path = f"{stem}_{self.tLattice}.npz"
+        os.makedirs(os.path.dirname(path) or ".", exist_ok=True)
+        return self._lat.save_checkpoint(path)
+
+    def load_snapshot(self, path: str, device="cuda") -> None:
+        """Continue from a checkpoint written by ``export_snapshot`` (in place of
+        init_simulation; no reference counterpart).  The checkpoint's lattice settings
+        replace this solver's."""
+        from .lattice import Lattice
+        if self._lat is not None:
+            self._lat.close()
+        self._lat = Lattice.load_checkpoint(path, device=device)
+        self._cfg = self._lat.cfg
+        self.tLattice = self._lat.nsteps
+        self.t = self.tLattice * self.dt
+        self._cache = None
+        self._cache_step = -1
 
     def check_python(self):
         pass
 
-    def export_VTK_pyvista(self):
-        raise NotImplementedError("VTK export (pyvista) is not on the CUDA path; read fields with to_numpy()")
+    def export_VTK_pyvista(self) -> str:
+        """``exportPath/name_<tLattice>.vts`` and the ``exportPath/name.pvd`` time series
+        (src/LBM/LBM2D/_io.py:621-635), written without pyvista (lbm_porouschem_b200.vtk).
+        Point data under the reference's names: solid, rho, velocity and, with the
+        temperature field, Tf and Ts in K (one field here: equal arrays); with pyrolysis
+        also the reactive fraction alpha."""
+        os.makedirs(self.exportPath, exist_ok=True)
+        data = {"solid": self.solid.to_numpy(), "rho": self.rho.to_numpy(), "velocity": self.v.to_numpy()}
+        if self.TEMPERATURE:
+            T = self.TF.get_physical_value(self.TF.S.to_numpy())
+            data["Tf"] = T
+            data["Ts"] = T
+        if self._lat is not None and self._lat.cfg.pyro and self._lat.nsteps > 0:
+            data["alpha"] = self._state()["alpha"]
+        fn = os.path.join(self.exportPath, f"{self.name}_{self.tLattice}.vts")
+        write_vts(fn, data, self._shape, coords=(self.x, self.y, self.z))
+        self.PVD.exportPath = self.exportPath
+        self.PVD.add(self.tLattice * self.dt, os.path.basename(fn))
+        self.PVD.write()
+        return fn
 
     def close(self):
         if self._lat is not None:

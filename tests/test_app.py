@@ -122,7 +122,9 @@ def test_cli_runs_case(tmp_path, monkeypatch):
     p.write_text(yaml.safe_dump(cfg))
     monkeypatch.chdir(tmp_path)
     assert run(["-c", str(p), "-v", "0"]) == 0
-    files = sorted((tmp_path / "out").glob("*.npz"))
-    assert len(files) == 3                                           # t = 0, 10, 20
-    d = np.load(files[-1])
-    assert np.isfinite(d["rho"]).all() and d["T"].max() > 300.0     # the hot inlet has warmed the fluid
+    from lbm_porouschem_b200.vtk import read_pvd, read_vts
+    series = read_pvd(str(next((tmp_path / "out").glob("*.pvd"))))
+    assert [f for _, f in series] == [f"{cfg['basic']['name']}_{t}.vts" for t in (0, 10, 20)]
+    d = read_vts(str(tmp_path / "out" / series[-1][1]))
+    assert np.isfinite(d["rho"]).all() and d["Tf"].max() > 300.0    # the hot inlet has warmed the fluid
+    assert d["velocity"].shape == (d["rho"].size, 3)
