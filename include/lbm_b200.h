@@ -253,6 +253,28 @@ LBM_API int32_t lbm_batch_destroy(lbm_batch* b);
 #define LBM_NOALLOC_MAX_ROWS 32768
 LBM_API int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream);
 
+/* ------------------------------------------------------ geometry: STL meshes
+ * Replace StlReader.voxel_stl (src/LBM/GEO/STL.py:147-268, called by
+ * load_stl, src/LBM/LBM2D/_io.py:489-495) after the mesh has been read and
+ * scaled / rotated / translated on the host.  The reference voxelises with
+ * pyvista and samples the voxels onto the grid; here a cell is solid when its
+ * centre ((i+0.5)dx, (j+0.5)dx, (k+0.5)dx; the 2D lattice is the plane z = 0)
+ * lies inside the closed mesh, by ray parity along x. */
+
+/* Bytes of the work buffer lbm_voxelise_stl needs (dim 2: nz = 1). */
+LBM_API int32_t lbm_stl_work_bytes(int32_t nx, int32_t ny, int32_t nz, int32_t dim, size_t* bytes);
+
+/* triangles: device float32 [ntri][3 vertices][x, y, z] in the lattice's physical
+ * units (cell size dx).  Writes solid[c] (uint8 0/1) and, if `surface` is not
+ * NULL, surface[c] (float32): the reference's surface weight of a solid cell from
+ * its solid face neighbours (3D 6..0 solid: 0, 1, 1.414, 2, 3, 4, 6; 2D 4..0: 0,
+ * 1, 1.414, 2, 4), counted on a grid padded by one cell as the reference's is;
+ * 0 for fluid cells.  Cell c = x + nx*(y + ny*z).  `work` (device,
+ * lbm_stl_work_bytes) holds the toggle bits and the padded voxels. */
+LBM_API int32_t lbm_voxelise_stl(const float* triangles, int64_t ntri, int32_t nx, int32_t ny, int32_t nz,
+                                 int32_t dim, double dx, void* work, size_t work_bytes, uint8_t* solid,
+                                 float* surface, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

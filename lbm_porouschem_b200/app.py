@@ -78,7 +78,12 @@ def voxelise(shape: dict, grid, dx: float) -> np.ndarray:
                 continue                                      # 2D: the box spans the plane
             inside &= np.abs(d[k]) <= 0.5 * ext
     elif kind == "stl":
-        raise NotImplementedError("geometry type 'stl' (mesh voxelisation) is not on the CUDA path")
+        # src/LBM/app.py:466-473: path, scale, translate, rotate; voxelised on the GPU
+        from .stl import place, read_stl, voxelise as stl_voxelise
+        tri = place(read_stl(shape["path"]), shape.get("scale", [1, 1, 1]), shape.get("translate"),
+                    shape.get("rotate"))
+        dim = 3 if X.shape[2] > 1 else 2                       # the 2D grid is one z = 0 plane
+        inside, _ = stl_voxelise(tri, X.shape, dx, dim)
     else:
         raise ValueError(f"geometry type {kind!r} not valid")
     return inside.astype(np.float64)

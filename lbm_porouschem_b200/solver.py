@@ -292,8 +292,12 @@ class _SolverBase:
     def load_cantera(self, file):
         raise NotImplementedError("Cantera mechanisms are not on the CUDA path; use set_pyrolysis()")
 
-    def load_stl(self, *a, **k):
-        raise NotImplementedError("STL voxelisation is not on the CUDA path; pass a solid mask to add_solid()")
+    def load_stl(self, stl_path, scale=(1.0, 1.0, 1.0), translate=(0, 0, 0), rotate=(0, 0, 0), **kwargs):
+        """(voxel_array, surface_array) of an STL mesh on this lattice
+        (src/LBM/LBM2D/_io.py:489-495), voxelised on the GPU (lbm_porouschem_b200.stl)."""
+        from .stl import StlReader
+        r = StlReader(self.X, self.Y, self.Z, self.dx, self.DIM, logger=kwargs.get("logger"))
+        return r.voxel_stl(stl_path, scale, translate, rotate)
 
     # ------------------------------------------------------------ new settings of the CUDA path
     def set_body_force(self, g, half_force_velocity: bool = True):

@@ -80,8 +80,6 @@ def test_voxelise_shapes_3d():
     assert cone[20, 20, 11] == 1 and cone[28, 20, 11] == 1 and cone[28, 20, 28] == 0
     box = voxelise({"type": "box", "center": [20, 20, 20], "size": [10, 6, 4]}, g, dx)
     assert box.sum() == 10 * 6 * 4
-    with pytest.raises(NotImplementedError):
-        voxelise({"type": "stl", "path": "x.stl"}, g, dx)
 
 
 def test_build_case_from_yaml():
