@@ -30,6 +30,28 @@ extern "C" {
 #define LBM_NN_ERR_ARG LBM_ERR_ARG
 #define LBM_NN_ERR_CUDA LBM_ERR_CUDA
 
+/* The 3D forms of the four calls above (NDHWC, B x D x H x W pixels, x fastest;
+ * 3 x 3 x 3 or 1 x 1 x 1 taps in z, y, x order with x fastest, weights
+ * [Cout][taps][Cin]; 2 x 2 x 2 pooling and nearest upsampling; D, H, W are the
+ * input's sizes).  For the 3D variant of the warm-start network (16 base
+ * channels); lbm_nn_flip_weights, bias_grad, mse, adam, relu_bwd and to_bf16
+ * serve both. */
+LBM_API int32_t lbm_nn_conv3d(const void* in, int32_t in_cstride, int32_t in_coff, const void* w, const float* bias,
+                              const void* gate, void* out_bf16, float* out_f32, int32_t out_cstride, int32_t out_coff,
+                              int32_t B, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout, int32_t ksize,
+                              int32_t relu, int32_t accumulate, void* stream);
+LBM_API int32_t lbm_nn_conv3d_wgrad(const void* in, int32_t in_cstride, int32_t in_coff, const void* dout,
+                                    int32_t dout_cstride, int32_t dout_coff, float* dw, int32_t B, int32_t D, int32_t H,
+                                    int32_t W, int32_t Cin, int32_t Cout, int32_t ksize, void* stream);
+LBM_API int32_t lbm_nn_avgpool2_3d(const void* in, int32_t in_cstride, int32_t in_coff, void* out, int32_t B,
+                                   int32_t D, int32_t H, int32_t W, int32_t C, void* stream);
+LBM_API int32_t lbm_nn_avgpool2_3d_bwd(const void* dout, void* din, int32_t din_cstride, int32_t din_coff, int32_t B,
+                                       int32_t D, int32_t H, int32_t W, int32_t C, int32_t accumulate, void* stream);
+LBM_API int32_t lbm_nn_upsample2_3d(const void* in, void* out, int32_t out_cstride, int32_t out_coff, int32_t B,
+                                    int32_t D, int32_t H, int32_t W, int32_t C, void* stream);
+LBM_API int32_t lbm_nn_upsample2_3d_bwd(const void* dout, int32_t dout_cstride, int32_t dout_coff, void* din,
+                                        int32_t B, int32_t D, int32_t H, int32_t W, int32_t C, void* stream);
+
 /* out = act(conv(in, w) + bias), same padding, stride 1, ksize 1 or 3, on the
  * tensor cores (bf16 inputs, FP32 accumulation).  act: ReLU if relu; then, if
  * gate is not NULL, out = 0 where gate <= 0 (gate laid out like out: the ReLU

@@ -48,6 +48,8 @@ EXPORTED = (
     "lbm_nn_conv", "lbm_nn_conv_wgrad", "lbm_nn_bias_grad", "lbm_nn_flip_weights", "lbm_nn_avgpool2",
     "lbm_nn_avgpool2_bwd", "lbm_nn_upsample2", "lbm_nn_upsample2_bwd", "lbm_nn_mse", "lbm_nn_adam",
     "lbm_nn_relu_bwd", "lbm_nn_to_bf16",
+    "lbm_nn_conv3d", "lbm_nn_conv3d_wgrad", "lbm_nn_avgpool2_3d", "lbm_nn_avgpool2_3d_bwd", "lbm_nn_upsample2_3d",
+    "lbm_nn_upsample2_3d_bwd",
 )
 LBM_NOALLOC_MAX_ROWS = 32768
 
@@ -160,6 +162,12 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
         "lbm_nn_adam": [vp, vp, vp, vp, vp, sz, f32, f32, f32, f32, i32, f32, vp],
         "lbm_nn_relu_bwd": [vp, i32, i32, vp, i32, i32, i32, i32, vp],
         "lbm_nn_to_bf16": [vp, vp, sz, vp],
+        "lbm_nn_conv3d": [vp, i32, i32, vp, vp, vp, vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_conv3d_wgrad": [vp, i32, i32, vp, i32, i32, vp, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_avgpool2_3d": [vp, i32, i32, vp, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_avgpool2_3d_bwd": [vp, vp, i32, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_upsample2_3d": [vp, vp, i32, i32, i32, i32, i32, i32, i32, vp],
+        "lbm_nn_upsample2_3d_bwd": [vp, i32, i32, vp, i32, i32, i32, i32, i32, vp],
     }
     for name, args in nn.items():
         getattr(lib, name).argtypes = args

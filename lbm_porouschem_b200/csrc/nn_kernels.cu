@@ -41,9 +41,23 @@ struct ConvArgs {
   bf16* out;                 // bf16 output, or
   float* out_f32;            // FP32 output (one of the two)
   int out_cstride, out_coff;
-  int B, H, W, Cin, Cout, ks;  // ks = 1 or 3
-  int relu, accumulate;        // accumulate: out += result (bf16 / f32)
+  int B, D, H, W, Cin, Cout, ks;  // ks = 1 or 3; D = 1 in 2D
+  int nd;                         // spatial dimensions: 2 (taps ks^2) or 3 (taps ks^3)
+  int relu, accumulate;           // accumulate: out += result (bf16 / f32)
 };
+
+// Input pixel that tap `tap` of output pixel p reads (NDHWC, x fastest; taps in
+// z, y, x order, x fastest); false where the tap falls outside (zero padding).
+__device__ __forceinline__ bool tap_pixel(int p, int tap, int D, int H, int W, int ks, int nd, size_t& q) {
+  const int half = ks / 2;
+  const int x = p % W, y = (p / W) % H, zb = p / (W * H);
+  const int z = zb % D, b = zb / D;
+  const int xx = x + tap % ks - half, yy = y + (tap / ks) % ks - half;
+  const int zz = nd == 3 ? z + tap / (ks * ks) - half : z;
+  if (xx < 0 || xx >= W || yy < 0 || yy >= H || zz < 0 || zz >= D) return false;
+  q = ((size_t)(b * D + zz) * H + yy) * W + xx;
+  return true;
+}
 
 __device__ __forceinline__ void mma_bf16(float c[4], const uint32_t a[4], const uint32_t b[2]) {
   asm volatile(
@@ -90,9 +104,9 @@ __global__ void __launch_bounds__(128) conv_igemm(const ConvArgs a) {
   __shared__ __align__(16) bf16 Bs[kBN][kBK + kPad];
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  const int P = a.B * a.H * a.W;
+  const int P = a.B * a.D * a.H * a.W;
   const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
-  const int taps = a.ks * a.ks, half = a.ks / 2;
+  const int taps = a.nd == 3 ? a.ks * a.ks * a.ks : a.ks * a.ks;
   const int K = taps * a.Cin;
   float acc[2][4][4];
 #pragma unroll
@@ -113,10 +127,9 @@ __global__ void __launch_bounds__(128) conv_igemm(const ConvArgs a) {
       uint4 v = make_uint4(0, 0, 0, 0);
       if (p < P && k < K) {
         const int tap = k / a.Cin, c = k - tap * a.Cin;
-        const int x = p % a.W, y = (p / a.W) % a.H, b = p / (a.W * a.H);
-        const int yy = y + tap / a.ks - half, xx = x + tap % a.ks - half;
-        if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
-          v = *reinterpret_cast<const uint4*>(a.in + ((size_t)(b * a.H + yy) * a.W + xx) * a.in_cstride + a.in_coff + c);
+        size_t q;
+        if (tap_pixel(p, tap, a.D, a.H, a.W, a.ks, a.nd, q))
+          v = *reinterpret_cast<const uint4*>(a.in + q * a.in_cstride + a.in_coff + c);
       }
       *reinterpret_cast<uint4*>(&As[mi][kc]) = v;
     }
@@ -172,7 +185,7 @@ struct WgradArgs {
   const bf16* dout;
   int dout_cstride, dout_coff;
   float* dw;
-  int B, H, W, Cin, Cout, ks;
+  int B, D, H, W, Cin, Cout, ks, nd;
   int pix_per_split;
 };
 
@@ -181,8 +194,8 @@ __global__ void __launch_bounds__(128) conv_wgrad(const WgradArgs a) {
   __shared__ __align__(16) bf16 Bs[kBN][kBK + kPad];  // [tap*Cin + c][pixel]
   const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
   const int wm = (warp & 1) * 32, wn = (warp >> 1) * 32;
-  const int P = a.B * a.H * a.W;
-  const int taps = a.ks * a.ks, half = a.ks / 2, Kc = taps * a.Cin;
+  const int P = a.B * a.D * a.H * a.W;
+  const int taps = a.nd == 3 ? a.ks * a.ks * a.ks : a.ks * a.ks, Kc = taps * a.Cin;
   const int m0 = blockIdx.x * kBM, n0 = blockIdx.y * kBN;
   const int p_begin = blockIdx.z * a.pix_per_split;
   const int p_end = min(P, p_begin + a.pix_per_split);
@@ -217,10 +230,9 @@ __global__ void __launch_bounds__(128) conv_wgrad(const WgradArgs a) {
       uint4 v = make_uint4(0, 0, 0, 0);
       if (p < p_end && k < Kc) {
         const int tap = k / a.Cin, c = k - tap * a.Cin;
-        const int x = p % a.W, y = (p / a.W) % a.H, b = p / (a.W * a.H);
-        const int yy = y + tap / a.ks - half, xx = x + tap % a.ks - half;
-        if (yy >= 0 && yy < a.H && xx >= 0 && xx < a.W)
-          v = *reinterpret_cast<const uint4*>(a.in + ((size_t)(b * a.H + yy) * a.W + xx) * a.in_cstride + a.in_coff + c);
+        size_t q;
+        if (tap_pixel(p, tap, a.D, a.H, a.W, a.ks, a.nd, q))
+          v = *reinterpret_cast<const uint4*>(a.in + q * a.in_cstride + a.in_coff + c);
       }
       const bf16* e8 = reinterpret_cast<const bf16*>(&v);
 #pragma unroll
@@ -275,58 +287,83 @@ __global__ void flip_weights(const bf16* w, bf16* wt, int Cout, int taps, int Ci
   wt[((size_t)c * taps + (taps - 1 - t)) * Cout + n] = w[i];
 }
 
-// 2x2 average pooling of a channel slice (H, W even).
-__global__ void avgpool2(const bf16* in, int in_cstride, int in_coff, bf16* out, int B, int H, int W, int C) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  const int Ho = H / 2, Wo = W / 2;
-  if (i >= (size_t)B * Ho * Wo * C) return;
-  const int c = (int)(i % C);
-  const size_t po = i / C;
-  const int x = (int)(po % Wo), y = (int)((po / Wo) % Ho), b = (int)(po / ((size_t)Wo * Ho));
-  float s = 0.f;
-#pragma unroll
-  for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-    for (int dx = 0; dx < 2; ++dx)
-      s += __bfloat162float(in[((size_t)(b * H + 2 * y + dy) * W + 2 * x + dx) * in_cstride + in_coff + c]);
-  out[i] = __float2bfloat16_rn(0.25f * s);
+// Pixel (b, z, y, x) of a B x D x H x W grid (x fastest).
+struct Pix {
+  int b, z, y, x;
+  __device__ __forceinline__ Pix(size_t p, int D, int H, int W) {
+    x = (int)(p % W);
+    y = (int)((p / W) % H);
+    const size_t zb = p / ((size_t)W * H);
+    z = (int)(zb % D);
+    b = (int)(zb / D);
+  }
+};
+__device__ __forceinline__ size_t pix(int b, int z, int y, int x, int D, int H, int W) {
+  return ((size_t)(b * D + z) * H + y) * W + x;
 }
 
-// Gradient of avgpool2: every input pixel receives a quarter of its window's
-// gradient; accumulate adds it to what the slice holds.
-__global__ void avgpool2_bwd(const bf16* dout, bf16* din, int din_cstride, int din_coff, int B, int H, int W, int C,
-                             int accumulate) {
+// 2x2 (3D: 2x2x2) average pooling of a channel slice (D, H, W even; D = 1 in 2D).
+__global__ void avgpool2(const bf16* in, int in_cstride, int in_coff, bf16* out, int B, int D, int H, int W, int C,
+                         int nd) {
   const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= (size_t)B * H * W * C) return;
+  const int Do = nd == 3 ? D / 2 : D, Ho = H / 2, Wo = W / 2, nz = nd == 3 ? 2 : 1;
+  if (i >= (size_t)B * Do * Ho * Wo * C) return;
+  const int c = (int)(i % C);
+  const Pix o(i / C, Do, Ho, Wo);
+  float s = 0.f;
+  for (int dz = 0; dz < nz; ++dz)
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+      for (int dx = 0; dx < 2; ++dx)
+        s += __bfloat162float(
+            in[pix(o.b, nz * o.z + dz, 2 * o.y + dy, 2 * o.x + dx, D, H, W) * in_cstride + in_coff + c]);
+  out[i] = __float2bfloat16_rn(s / (4.0f * nz));
+}
+
+// Gradient of avgpool2: every input pixel receives its share of its window's
+// gradient; accumulate adds it to what the slice holds.
+__global__ void avgpool2_bwd(const bf16* dout, bf16* din, int din_cstride, int din_coff, int B, int D, int H, int W,
+                             int C, int nd, int accumulate) {
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= (size_t)B * D * H * W * C) return;
   const int c = (int)(i % C);
   const size_t p = i / C;
-  const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
-  const float g = 0.25f * __bfloat162float(dout[((size_t)(b * (H / 2) + y / 2) * (W / 2) + x / 2) * C + c]);
+  const Pix q(p, D, H, W);
+  const int nz = nd == 3 ? 2 : 1;
+  const float g = __bfloat162float(dout[pix(q.b, q.z / nz, q.y / 2, q.x / 2, D / nz, H / 2, W / 2) * C + c]) /
+                  (4.0f * nz);
   const size_t o = p * din_cstride + din_coff + c;
   din[o] = __float2bfloat16_rn(accumulate ? __bfloat162float(din[o]) + g : g);
 }
 
-// Nearest 2x upsampling into a channel slice, and its gradient (2x2 sums).
-__global__ void upsample2(const bf16* in, bf16* out, int out_cstride, int out_coff, int B, int H, int W, int C) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over the output (2H x 2W)
-  if (i >= (size_t)B * 4 * H * W * C) return;
+// Nearest 2x upsampling (3D: in z too) into a channel slice, and its gradient
+// (sums over each 2x2 / 2x2x2 block).
+__global__ void upsample2(const bf16* in, bf16* out, int out_cstride, int out_coff, int B, int D, int H, int W, int C,
+                          int nd) {
+  const int nz = nd == 3 ? 2 : 1;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over the output
+  if (i >= (size_t)B * nz * D * 4 * H * W * C) return;
   const int c = (int)(i % C);
   const size_t p = i / C;
-  const int x = (int)(p % (2 * W)), y = (int)((p / (2 * W)) % (2 * H)), b = (int)(p / ((size_t)4 * W * H));
-  out[p * out_cstride + out_coff + c] = in[((size_t)(b * H + y / 2) * W + x / 2) * C + c];
+  const Pix o(p, nz * D, 2 * H, 2 * W);
+  out[p * out_cstride + out_coff + c] = in[pix(o.b, o.z / nz, o.y / 2, o.x / 2, D, H, W) * C + c];
 }
-__global__ void upsample2_bwd(const bf16* dout, int dout_cstride, int dout_coff, bf16* din, int B, int H, int W, int C) {
-  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over din (H x W)
-  if (i >= (size_t)B * H * W * C) return;
+__global__ void upsample2_bwd(const bf16* dout, int dout_cstride, int dout_coff, bf16* din, int B, int D, int H, int W,
+                              int C, int nd) {
+  const int nz = nd == 3 ? 2 : 1;
+  const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;  // over din
+  if (i >= (size_t)B * D * H * W * C) return;
   const int c = (int)(i % C);
-  const size_t p = i / C;
-  const int x = (int)(p % W), y = (int)((p / W) % H), b = (int)(p / ((size_t)W * H));
+  const Pix q(i / C, D, H, W);
   float s = 0.f;
+  for (int dz = 0; dz < nz; ++dz)
 #pragma unroll
-  for (int dy = 0; dy < 2; ++dy)
+    for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-    for (int dx = 0; dx < 2; ++dx)
-      s += __bfloat162float(dout[((size_t)(b * 2 * H + 2 * y + dy) * 2 * W + 2 * x + dx) * dout_cstride + dout_coff + c]);
+      for (int dx = 0; dx < 2; ++dx)
+        s += __bfloat162float(dout[pix(q.b, nz * q.z + dz, 2 * q.y + dy, 2 * q.x + dx, nz * D, 2 * H, 2 * W) *
+                                       dout_cstride + dout_coff + c]);
   din[i] = __float2bfloat16_rn(s);
 }
 
@@ -391,6 +428,84 @@ int check_launch(const char* what) {
 
 bool aligned16(const void* p) { return ((uintptr_t)p & 15) == 0; }
 
+int conv_nd(const void* in, int32_t in_cstride, int32_t in_coff, const void* w, const float* bias, const void* gate,
+            void* out_bf16, float* out_f32, int32_t out_cstride, int32_t out_coff, int32_t B, int32_t D, int32_t H,
+            int32_t W, int32_t Cin, int32_t Cout, int32_t ksize, int32_t relu, int32_t accumulate, int nd,
+            void* stream) {
+  if (!in || !w || (!out_bf16 && !out_f32) || (out_bf16 && out_f32))
+    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: in, w and exactly one output are required");
+  if (ksize != 1 && ksize != 3) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: ksize must be 1 or 3");
+  if (Cin % 8 || in_cstride % 8 || in_coff % 8 || B < 1 || D < 1 || H < 1 || W < 1 || Cout < 1 ||
+      in_coff + Cin > in_cstride || out_coff + Cout > out_cstride)
+    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: channel counts/offsets must be multiples of 8 and fit");
+  if ((double)B * D * H * W >= 2147483647.0) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: too many pixels");
+  if (!aligned16(in) || !aligned16(w)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: in and w must be 16-byte aligned");
+  ConvArgs a{(const bf16*)in, in_cstride, in_coff, (const bf16*)w, bias, (const bf16*)gate, (bf16*)out_bf16, out_f32,
+             out_cstride, out_coff, B, D, H, W, Cin, Cout, ksize, nd, relu, accumulate};
+  const size_t P = (size_t)B * D * H * W;
+  const dim3 grid((unsigned)((P + kBM - 1) / kBM), (unsigned)((Cout + kBN - 1) / kBN));
+  conv_igemm<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
+  return check_launch("conv_igemm");
+}
+
+int wgrad_nd(const void* in, int32_t in_cstride, int32_t in_coff, const void* dout, int32_t dout_cstride,
+             int32_t dout_coff, float* dw, int32_t B, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
+             int32_t ksize, int nd, void* stream) {
+  if (!in || !dout || !dw) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: NULL argument");
+  if (ksize != 1 && ksize != 3) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: ksize must be 1 or 3");
+  if (Cin % 8 || Cout % 8 || in_cstride % 8 || in_coff % 8 || dout_cstride % 8 || dout_coff % 8 ||
+      in_coff + Cin > in_cstride || dout_coff + Cout > dout_cstride || B < 1 || D < 1 || H < 1 || W < 1)
+    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: channel counts/offsets must be multiples of 8 and fit");
+  if ((double)B * D * H * W >= 2147483647.0) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: too many pixels");
+  if (!aligned16(in) || !aligned16(dout)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: 16-byte alignment");
+  const int P = B * D * H * W;
+  const int Kc = (nd == 3 ? ksize * ksize * ksize : ksize * ksize) * Cin;
+  const int mt = (Cout + kBM - 1) / kBM, nt = (Kc + kBN - 1) / kBN;
+  // enough pixel splits to fill the GPU (about 4 blocks per SM), each a multiple of 32 pixels
+  int splits = std::max(1, 148 * 4 / std::max(1, mt * nt));
+  int pps = (P + splits - 1) / splits;
+  pps = (pps + kBK - 1) / kBK * kBK;
+  splits = (P + pps - 1) / pps;
+  WgradArgs a{(const bf16*)in, in_cstride, in_coff, (const bf16*)dout, dout_cstride, dout_coff, dw, B, D, H, W, Cin,
+              Cout, ksize, nd, pps};
+  conv_wgrad<<<dim3(mt, nt, splits), 128, 0, (cudaStream_t)stream>>>(a);
+  return check_launch("conv_wgrad");
+}
+
+int pool_nd(const void* in, int32_t in_cstride, int32_t in_coff, void* out, int32_t B, int32_t D, int32_t H, int32_t W,
+            int32_t C, int nd, void* stream) {
+  if (H % 2 || W % 2 || (nd == 3 && D % 2)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_avgpool2: sizes must be even");
+  const size_t n = (size_t)B * (nd == 3 ? D / 2 : D) * (H / 2) * (W / 2) * C;
+  avgpool2<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)in, in_cstride, in_coff, (bf16*)out, B, D,
+                                                                 H, W, C, nd);
+  return check_launch("avgpool2");
+}
+
+int pool_bwd_nd(const void* dout, void* din, int32_t din_cstride, int32_t din_coff, int32_t B, int32_t D, int32_t H,
+                int32_t W, int32_t C, int32_t accumulate, int nd, void* stream) {
+  if (H % 2 || W % 2 || (nd == 3 && D % 2)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_avgpool2_bwd: sizes must be even");
+  const size_t n = (size_t)B * D * H * W * C;
+  avgpool2_bwd<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dout, (bf16*)din, din_cstride,
+                                                                     din_coff, B, D, H, W, C, nd, accumulate);
+  return check_launch("avgpool2_bwd");
+}
+
+int up_nd(const void* in, void* out, int32_t out_cstride, int32_t out_coff, int32_t B, int32_t D, int32_t H, int32_t W,
+          int32_t C, int nd, void* stream) {
+  const size_t n = (size_t)B * (nd == 3 ? 2 * D : D) * 4 * H * W * C;
+  upsample2<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)in, (bf16*)out, out_cstride, out_coff, B,
+                                                                   D, H, W, C, nd);
+  return check_launch("upsample2");
+}
+
+int up_bwd_nd(const void* dout, int32_t dout_cstride, int32_t dout_coff, void* din, int32_t B, int32_t D, int32_t H,
+              int32_t W, int32_t C, int nd, void* stream) {
+  const size_t n = (size_t)B * D * H * W * C;
+  upsample2_bwd<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dout, dout_cstride, dout_coff,
+                                                                      (bf16*)din, B, D, H, W, C, nd);
+  return check_launch("upsample2_bwd");
+}
+
 }  // namespace
 
 extern "C" {
@@ -399,42 +514,28 @@ int32_t lbm_nn_conv(const void* in, int32_t in_cstride, int32_t in_coff, const v
                     const void* gate, void* out_bf16, float* out_f32, int32_t out_cstride, int32_t out_coff,
                     int32_t B, int32_t H, int32_t W, int32_t Cin, int32_t Cout, int32_t ksize, int32_t relu,
                     int32_t accumulate, void* stream) {
-  if (!in || !w || (!out_bf16 && !out_f32) || (out_bf16 && out_f32))
-    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: in, w and exactly one output are required");
-  if (ksize != 1 && ksize != 3) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: ksize must be 1 or 3");
-  if (Cin % 8 || in_cstride % 8 || in_coff % 8 || B < 1 || H < 1 || W < 1 || Cout < 1 ||
-      in_coff + Cin > in_cstride || out_coff + Cout > out_cstride)
-    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: channel counts/offsets must be multiples of 8 and fit");
-  if (!aligned16(in) || !aligned16(w)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv: in and w must be 16-byte aligned");
-  ConvArgs a{(const bf16*)in, in_cstride, in_coff, (const bf16*)w, bias, (const bf16*)gate, (bf16*)out_bf16, out_f32,
-             out_cstride, out_coff, B, H, W, Cin, Cout, ksize, relu, accumulate};
-  const size_t P = (size_t)B * H * W;
-  const dim3 grid((unsigned)((P + kBM - 1) / kBM), (unsigned)((Cout + kBN - 1) / kBN));
-  conv_igemm<<<grid, 128, 0, (cudaStream_t)stream>>>(a);
-  return check_launch("conv_igemm");
+  return conv_nd(in, in_cstride, in_coff, w, bias, gate, out_bf16, out_f32, out_cstride, out_coff, B, 1, H, W, Cin,
+                 Cout, ksize, relu, accumulate, 2, stream);
+}
+
+int32_t lbm_nn_conv3d(const void* in, int32_t in_cstride, int32_t in_coff, const void* w, const float* bias,
+                      const void* gate, void* out_bf16, float* out_f32, int32_t out_cstride, int32_t out_coff,
+                      int32_t B, int32_t D, int32_t H, int32_t W, int32_t Cin, int32_t Cout, int32_t ksize,
+                      int32_t relu, int32_t accumulate, void* stream) {
+  return conv_nd(in, in_cstride, in_coff, w, bias, gate, out_bf16, out_f32, out_cstride, out_coff, B, D, H, W, Cin,
+                 Cout, ksize, relu, accumulate, 3, stream);
 }
 
 int32_t lbm_nn_conv_wgrad(const void* in, int32_t in_cstride, int32_t in_coff, const void* dout, int32_t dout_cstride,
                           int32_t dout_coff, float* dw, int32_t B, int32_t H, int32_t W, int32_t Cin, int32_t Cout,
                           int32_t ksize, void* stream) {
-  if (!in || !dout || !dw) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: NULL argument");
-  if (ksize != 1 && ksize != 3) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: ksize must be 1 or 3");
-  if (Cin % 8 || Cout % 8 || in_cstride % 8 || in_coff % 8 || dout_cstride % 8 || dout_coff % 8 ||
-      in_coff + Cin > in_cstride || dout_coff + Cout > dout_cstride)
-    return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: channel counts/offsets must be multiples of 8 and fit");
-  if (!aligned16(in) || !aligned16(dout)) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_conv_wgrad: 16-byte alignment");
-  const int P = B * H * W;
-  const int Kc = ksize * ksize * Cin;
-  const int mt = (Cout + kBM - 1) / kBM, nt = (Kc + kBN - 1) / kBN;
-  // enough pixel splits to fill the GPU (about 4 blocks per SM), each a multiple of 32 pixels
-  int splits = std::max(1, 148 * 4 / std::max(1, mt * nt));
-  int pps = (P + splits - 1) / splits;
-  pps = (pps + kBK - 1) / kBK * kBK;
-  splits = (P + pps - 1) / pps;
-  WgradArgs a{(const bf16*)in, in_cstride, in_coff, (const bf16*)dout, dout_cstride, dout_coff, dw, B, H, W, Cin, Cout,
-              ksize, pps};
-  conv_wgrad<<<dim3(mt, nt, splits), 128, 0, (cudaStream_t)stream>>>(a);
-  return check_launch("conv_wgrad");
+  return wgrad_nd(in, in_cstride, in_coff, dout, dout_cstride, dout_coff, dw, B, 1, H, W, Cin, Cout, ksize, 2, stream);
+}
+
+int32_t lbm_nn_conv3d_wgrad(const void* in, int32_t in_cstride, int32_t in_coff, const void* dout,
+                            int32_t dout_cstride, int32_t dout_coff, float* dw, int32_t B, int32_t D, int32_t H,
+                            int32_t W, int32_t Cin, int32_t Cout, int32_t ksize, void* stream) {
+  return wgrad_nd(in, in_cstride, in_coff, dout, dout_cstride, dout_coff, dw, B, D, H, W, Cin, Cout, ksize, 3, stream);
 }
 
 int32_t lbm_nn_bias_grad(const void* dout, int32_t cstride, int32_t coff, int32_t P, int32_t Cout, float* dbias,
@@ -454,35 +555,38 @@ int32_t lbm_nn_flip_weights(const void* w, void* wt, int32_t Cout, int32_t taps,
 
 int32_t lbm_nn_avgpool2(const void* in, int32_t in_cstride, int32_t in_coff, void* out, int32_t B, int32_t H, int32_t W,
                         int32_t C, void* stream) {
-  if (H % 2 || W % 2) return lbm::capi::fail(LBM_NN_ERR_ARG, "lbm_nn_avgpool2: H and W must be even");
-  const size_t n = (size_t)B * (H / 2) * (W / 2) * C;
-  avgpool2<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)in, in_cstride, in_coff, (bf16*)out, B, H,
-                                                                 W, C);
-  return check_launch("avgpool2");
+  return pool_nd(in, in_cstride, in_coff, out, B, 1, H, W, C, 2, stream);
+}
+int32_t lbm_nn_avgpool2_3d(const void* in, int32_t in_cstride, int32_t in_coff, void* out, int32_t B, int32_t D,
+                           int32_t H, int32_t W, int32_t C, void* stream) {
+  return pool_nd(in, in_cstride, in_coff, out, B, D, H, W, C, 3, stream);
 }
 
 int32_t lbm_nn_avgpool2_bwd(const void* dout, void* din, int32_t din_cstride, int32_t din_coff, int32_t B, int32_t H,
                             int32_t W, int32_t C, int32_t accumulate, void* stream) {
-  const size_t n = (size_t)B * H * W * C;
-  avgpool2_bwd<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dout, (bf16*)din, din_cstride,
-                                                                     din_coff, B, H, W, C, accumulate);
-  return check_launch("avgpool2_bwd");
+  return pool_bwd_nd(dout, din, din_cstride, din_coff, B, 1, H, W, C, accumulate, 2, stream);
+}
+int32_t lbm_nn_avgpool2_3d_bwd(const void* dout, void* din, int32_t din_cstride, int32_t din_coff, int32_t B, int32_t D,
+                               int32_t H, int32_t W, int32_t C, int32_t accumulate, void* stream) {
+  return pool_bwd_nd(dout, din, din_cstride, din_coff, B, D, H, W, C, accumulate, 3, stream);
 }
 
 int32_t lbm_nn_upsample2(const void* in, void* out, int32_t out_cstride, int32_t out_coff, int32_t B, int32_t H,
                          int32_t W, int32_t C, void* stream) {
-  const size_t n = (size_t)B * 4 * H * W * C;
-  upsample2<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)in, (bf16*)out, out_cstride, out_coff, B,
-                                                                   H, W, C);
-  return check_launch("upsample2");
+  return up_nd(in, out, out_cstride, out_coff, B, 1, H, W, C, 2, stream);
+}
+int32_t lbm_nn_upsample2_3d(const void* in, void* out, int32_t out_cstride, int32_t out_coff, int32_t B, int32_t D,
+                            int32_t H, int32_t W, int32_t C, void* stream) {
+  return up_nd(in, out, out_cstride, out_coff, B, D, H, W, C, 3, stream);
 }
 
 int32_t lbm_nn_upsample2_bwd(const void* dout, int32_t dout_cstride, int32_t dout_coff, void* din, int32_t B, int32_t H,
                              int32_t W, int32_t C, void* stream) {
-  const size_t n = (size_t)B * H * W * C;
-  upsample2_bwd<<<blocks_for(n, 256), 256, 0, (cudaStream_t)stream>>>((const bf16*)dout, dout_cstride, dout_coff,
-                                                                      (bf16*)din, B, H, W, C);
-  return check_launch("upsample2_bwd");
+  return up_bwd_nd(dout, dout_cstride, dout_coff, din, B, 1, H, W, C, 2, stream);
+}
+int32_t lbm_nn_upsample2_3d_bwd(const void* dout, int32_t dout_cstride, int32_t dout_coff, void* din, int32_t B,
+                                int32_t D, int32_t H, int32_t W, int32_t C, void* stream) {
+  return up_bwd_nd(dout, dout_cstride, dout_coff, din, B, D, H, W, C, 3, stream);
 }
 
 int32_t lbm_nn_mse(const float* pred, const float* target, const float* weight, size_t n, float scale, void* grad,

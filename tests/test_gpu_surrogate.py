@@ -195,3 +195,82 @@ def test_warm_start_gain():
     assert m["pre_err_u"] < 1.0, m          # rest is 100 % off
     assert m["pre_err_T"] < 0.5, m          # a zero temperature field is 100 % off
     assert m["k_rel_diff_max"] < 1e-2, m    # both runs stop at a residual of 1e-6 per 100 steps
+
+
+# ----------------------------------------------------------------------------- 3D kernels
+def _ref_conv3d(x, w, k, bias=None):
+    """x: NDHWC float64, w: [Cout][k^3][Cin] (taps z, y, x; x fastest) -> NDHWC."""
+    Cout, _, Cin = w.shape
+    wt = w.reshape(Cout, k, k, k, Cin).permute(0, 4, 1, 2, 3)
+    y = F.conv3d(x.permute(0, 4, 1, 2, 3), wt, bias, padding=k // 2)
+    return y.permute(0, 2, 3, 4, 1)
+
+
+@pytest.mark.parametrize("k", [1, 3])
+def test_conv3d_forward_with_slices(k):
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(10 + k)
+    B, D, H, W, Cin, Cout = 2, 6, 8, 10, 16, 40
+    buf_in = torch.randn(B, D, H, W, 24, generator=g).to(torch.bfloat16)
+    w = (torch.randn(Cout, k ** 3, Cin, generator=g) * 0.15).to(torch.bfloat16)
+    bias = torch.randn(Cout, generator=g)
+    out = torch.zeros(B, D, H, W, 48, dtype=torch.bfloat16)
+    d_in, d_w, d_b, d_out = buf_in.cuda(), w.cuda(), bias.cuda(), out.cuda()
+    N.check(lib.lbm_nn_conv3d(_p(d_in), 24, 8, _p(d_w), _p(d_b), None, _p(d_out), None, 48, 8,
+                              B, D, H, W, Cin, Cout, k, 1, 0, _s()))
+    got = d_out.cpu().double()
+    ref = torch.relu(_ref_conv3d(buf_in[..., 8:].double(), w.double(), k, bias.double()))
+    assert _rel(got[..., 8:], ref) < 1e-2
+    assert torch.all(got[..., :8] == 0)
+
+
+def test_conv3d_wgrad_dgrad_bias_match_autograd():
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(15)
+    B, D, H, W, Cin, Cout, k = 2, 6, 6, 8, 16, 16, 3
+    x = torch.randn(B, D, H, W, Cin, generator=g).to(torch.bfloat16)
+    w = (torch.randn(Cout, 27, Cin, generator=g) * 0.15).to(torch.bfloat16)
+    dy = torch.randn(B, D, H, W, Cout, generator=g).to(torch.bfloat16)
+    xr = x.double().requires_grad_(True)
+    wr = w.double().requires_grad_(True)
+    br = torch.zeros(Cout, dtype=torch.float64, requires_grad=True)
+    _ref_conv3d(xr, wr, k, br).backward(dy.double())
+    dx_, w_, dy_ = x.cuda(), w.cuda(), dy.cuda()
+    dw = torch.zeros(Cout, 27, Cin, device="cuda")
+    db = torch.zeros(Cout, device="cuda")
+    wt = torch.empty(Cin, 27, Cout, dtype=torch.bfloat16, device="cuda")
+    dxo = torch.empty(B, D, H, W, Cin, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_conv3d_wgrad(_p(dx_), Cin, 0, _p(dy_), Cout, 0, _p(dw), B, D, H, W, Cin, Cout, k, _s()))
+    N.check(lib.lbm_nn_bias_grad(_p(dy_), Cout, 0, B * D * H * W, Cout, _p(db), _s()))
+    N.check(lib.lbm_nn_flip_weights(_p(w_), _p(wt), Cout, 27, Cin, _s()))
+    N.check(lib.lbm_nn_conv3d(_p(dy_), Cout, 0, _p(wt), None, None, _p(dxo), None, Cin, 0, B, D, H, W, Cout, Cin, k,
+                              0, 0, _s()))
+    assert _rel(dw.cpu().double(), wr.grad) < 1e-3
+    assert _rel(db.cpu().double(), br.grad) < 1e-3
+    assert _rel(dxo.cpu().double(), xr.grad) < 1e-2
+
+
+def test_pool3d_upsample3d_and_their_gradients():
+    N, lib = _lib()
+    g = torch.Generator().manual_seed(12)
+    B, D, H, W, C = 2, 4, 6, 8, 16
+    x = torch.randn(B, D, H, W, 32, generator=g).to(torch.bfloat16)     # slice = channels 16..31
+    d = x.cuda()
+    p = torch.empty(B, D // 2, H // 2, W // 2, C, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_avgpool2_3d(_p(d), 32, 16, _p(p), B, D, H, W, C, _s()))
+    cf = lambda t: t.permute(0, 4, 1, 2, 3)           # noqa: E731  NDHWC -> NCDHW
+    cl = lambda t: t.permute(0, 2, 3, 4, 1)           # noqa: E731
+    ref = cl(F.avg_pool3d(cf(x[..., 16:].double()), 2))
+    assert _rel(p.cpu().double(), ref) < 1e-2
+    up = torch.zeros(B, D, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_upsample2_3d(_p(p), _p(up), 32, 0, B, D // 2, H // 2, W // 2, C, _s()))
+    refu = cl(F.interpolate(cf(p.cpu().double()), scale_factor=2, mode="nearest"))
+    assert torch.equal(up[..., :C].cpu().double(), refu)
+    gd = torch.empty(B, D // 2, H // 2, W // 2, C, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_upsample2_3d_bwd(_p(up), 32, 0, _p(gd), B, D // 2, H // 2, W // 2, C, _s()))
+    assert _rel(gd.cpu().double(), 8 * p.cpu().double()) < 1e-2
+    gi = torch.ones(B, D, H, W, 32, dtype=torch.bfloat16, device="cuda")
+    N.check(lib.lbm_nn_avgpool2_3d_bwd(_p(p), _p(gi), 32, 16, B, D, H, W, C, 1, _s()))
+    refg = 1 + 0.125 * cl(F.interpolate(cf(p.cpu().double()), scale_factor=2))
+    assert _rel(gi[..., 16:].cpu().double(), refg) < 1e-2
+    assert torch.all(gi[..., :16].cpu() == 1)
