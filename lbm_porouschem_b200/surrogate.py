@@ -239,32 +239,44 @@ class Conv:
     relu: bool = True
 
 
-# name -> layer; order of the forward pass
-LAYERS = {
-    "e0a": Conv(CIN, 32, 3), "e0b": Conv(32, 32, 3),
-    "e1a": Conv(32, 64, 3), "e1b": Conv(64, 64, 3),
-    "e2a": Conv(64, 128, 3), "e2b": Conv(128, 128, 3),
-    "b3a": Conv(128, 256, 3), "b3b": Conv(256, 256, 3),
-    "r3": Conv(256, 128, 1), "d2a": Conv(256, 128, 3), "d2b": Conv(128, 128, 3),
-    "r2": Conv(128, 64, 1), "d1a": Conv(128, 64, 3), "d1b": Conv(64, 64, 3),
-    "r1": Conv(64, 32, 1), "d0a": Conv(64, 32, 3), "d0b": Conv(32, 32, 3),
-    "out": Conv(32, COUT, 1, relu=False),
-}
+def layers(base: int = 32) -> dict:
+    """name -> layer, in the order of the forward pass; channels base, 2, 4, 8 x base."""
+    c0, c1, c2, c3 = base, 2 * base, 4 * base, 8 * base
+    return {
+        "e0a": Conv(CIN, c0, 3), "e0b": Conv(c0, c0, 3),
+        "e1a": Conv(c0, c1, 3), "e1b": Conv(c1, c1, 3),
+        "e2a": Conv(c1, c2, 3), "e2b": Conv(c2, c2, 3),
+        "b3a": Conv(c2, c3, 3), "b3b": Conv(c3, c3, 3),
+        "r3": Conv(c3, c2, 1), "d2a": Conv(c3, c2, 3), "d2b": Conv(c2, c2, 3),
+        "r2": Conv(c2, c1, 1), "d1a": Conv(c2, c1, 3), "d1b": Conv(c1, c1, 3),
+        "r1": Conv(c1, c0, 1), "d0a": Conv(c1, c0, 3), "d0b": Conv(c0, c0, 3),
+        "out": Conv(c0, COUT, 1, relu=False),
+    }
+
+
+LAYERS = layers(32)        # the 2D network
 
 
 class UNet:
     """U-Net on the lbm_nn kernels.  Forward and backward keep every activation of
-    a batch of B images of S x S (S a multiple of 8)."""
+    a batch of B images of S x S (3D: S x S x S; S a multiple of 8).  dim 2 with 32
+    base channels is the 2D network; dim 3 with 16 the 3D variant (3 x 3 x 3
+    convolutions, 2 x 2 x 2 pooling)."""
 
-    def __init__(self, device="cuda", seed: int = 0):
+    def __init__(self, device="cuda", seed: int = 0, dim: int = 2, base: int = 32):
+        if dim not in (2, 3) or base % 8:
+            raise ValueError("dim must be 2 or 3 and base a multiple of 8")
         self.lib = N.load()
         self.dev = torch.device(device)
+        self.dim, self.base = dim, base
+        self.layers = layers(base)
         gen = torch.Generator().manual_seed(seed)
         self.w, self.b, self.wb = {}, {}, {}
-        for name, L in LAYERS.items():
-            fan_in = L.cin * L.k * L.k
+        for name, L in self.layers.items():
+            taps = L.k ** dim
+            fan_in = L.cin * taps
             std = math.sqrt(2.0 / fan_in) if L.relu else math.sqrt(1.0 / fan_in)
-            w = torch.randn(L.cout, L.k * L.k, L.cin, generator=gen) * std
+            w = torch.randn(L.cout, taps, L.cin, generator=gen) * std
             if name == "e0a":
                 w[:, :, 6:] = 0.0                       # padded input channels
             self.w[name] = w.to(self.dev).contiguous()
@@ -284,28 +296,29 @@ class UNet:
     def _buffers(self, B: int, S: int):
         if self._shape == (B, S):
             return
-        d, bf = self.dev, torch.bfloat16
-        e = lambda s, c: torch.empty(B, s, s, c, dtype=bf, device=d)  # noqa: E731
-        z = lambda s, c: torch.zeros(B, s, s, c, dtype=bf, device=d)  # noqa: E731
+        d, bf, dim = self.dev, torch.bfloat16, self.dim
+        e = lambda s, c: torch.empty(B, *(s,) * dim, c, dtype=bf, device=d)  # noqa: E731
+        z = lambda s, c: torch.zeros(B, *(s,) * dim, c, dtype=bf, device=d)  # noqa: E731
         s0, s1, s2, s3 = S, S // 2, S // 4, S // 8
+        c0, c1, c2, c3 = self.base, 2 * self.base, 4 * self.base, 8 * self.base
         self.a = {
             "x": z(s0, CIN),
-            "e0a": e(s0, 32), "cat0": e(s0, 64), "p1": e(s1, 32),
-            "e1a": e(s1, 64), "cat1": e(s1, 128), "p2": e(s2, 64),
-            "e2a": e(s2, 128), "cat2": e(s2, 256), "p3": e(s3, 128),
-            "b3a": e(s3, 256), "b3b": e(s3, 256), "r3": e(s3, 128),
-            "d2a": e(s2, 128), "d2b": e(s2, 128), "r2": e(s2, 64),
-            "d1a": e(s1, 64), "d1b": e(s1, 64), "r1": e(s1, 32),
-            "d0a": e(s0, 32), "d0b": e(s0, 32),
+            "e0a": e(s0, c0), "cat0": e(s0, c1), "p1": e(s1, c0),
+            "e1a": e(s1, c1), "cat1": e(s1, c2), "p2": e(s2, c1),
+            "e2a": e(s2, c2), "cat2": e(s2, c3), "p3": e(s3, c2),
+            "b3a": e(s3, c3), "b3b": e(s3, c3), "r3": e(s3, c2),
+            "d2a": e(s2, c2), "d2b": e(s2, c2), "r2": e(s2, c1),
+            "d1a": e(s1, c1), "d1b": e(s1, c1), "r1": e(s1, c0),
+            "d0a": e(s0, c0), "d0b": e(s0, c0),
         }
-        self.y = torch.empty(B, S, S, COUT, dtype=torch.float32, device=d)
+        self.y = torch.empty(B, *(S,) * dim, COUT, dtype=torch.float32, device=d)
         # gradients, same layouts
         self.g = {k: torch.empty_like(v) for k, v in self.a.items() if k != "x"}
-        self.gy = torch.empty(B, S, S, COUT, dtype=bf, device=d)
+        self.gy = torch.empty(B, *(S,) * dim, COUT, dtype=bf, device=d)
         self.dw = {k: torch.zeros_like(v) for k, v in self.w.items()}
         self.db = {k: torch.zeros_like(v) for k, v in self.b.items()}
-        self.wt = {k: torch.empty(LAYERS[k].cin, LAYERS[k].k ** 2, LAYERS[k].cout, dtype=bf, device=d)
-                   for k in self.w}
+        L = self.layers
+        self.wt = {k: torch.empty(L[k].cin, L[k].k ** dim, L[k].cout, dtype=bf, device=d) for k in self.w}
         self.partial = torch.empty(1024, dtype=torch.float32, device=d)
         self._shape = (B, S)
 
@@ -319,19 +332,45 @@ class UNet:
     # the input / output views of every layer: (buffer, channel stride, offset)
     def _views(self):
         a = self.a
+        c0, c1, c2, c3 = self.base, 2 * self.base, 4 * self.base, 8 * self.base
         return {
-            "e0a": ((a["x"], CIN, 0), (a["e0a"], 32, 0)), "e0b": ((a["e0a"], 32, 0), (a["cat0"], 64, 32)),
-            "e1a": ((a["p1"], 32, 0), (a["e1a"], 64, 0)), "e1b": ((a["e1a"], 64, 0), (a["cat1"], 128, 64)),
-            "e2a": ((a["p2"], 64, 0), (a["e2a"], 128, 0)), "e2b": ((a["e2a"], 128, 0), (a["cat2"], 256, 128)),
-            "b3a": ((a["p3"], 128, 0), (a["b3a"], 256, 0)), "b3b": ((a["b3a"], 256, 0), (a["b3b"], 256, 0)),
-            "r3": ((a["b3b"], 256, 0), (a["r3"], 128, 0)),
-            "d2a": ((a["cat2"], 256, 0), (a["d2a"], 128, 0)), "d2b": ((a["d2a"], 128, 0), (a["d2b"], 128, 0)),
-            "r2": ((a["d2b"], 128, 0), (a["r2"], 64, 0)),
-            "d1a": ((a["cat1"], 128, 0), (a["d1a"], 64, 0)), "d1b": ((a["d1a"], 64, 0), (a["d1b"], 64, 0)),
-            "r1": ((a["d1b"], 64, 0), (a["r1"], 32, 0)),
-            "d0a": ((a["cat0"], 64, 0), (a["d0a"], 32, 0)), "d0b": ((a["d0a"], 32, 0), (a["d0b"], 32, 0)),
-            "out": ((a["d0b"], 32, 0), (self.y, COUT, 0)),
+            "e0a": ((a["x"], CIN, 0), (a["e0a"], c0, 0)), "e0b": ((a["e0a"], c0, 0), (a["cat0"], c1, c0)),
+            "e1a": ((a["p1"], c0, 0), (a["e1a"], c1, 0)), "e1b": ((a["e1a"], c1, 0), (a["cat1"], c2, c1)),
+            "e2a": ((a["p2"], c1, 0), (a["e2a"], c2, 0)), "e2b": ((a["e2a"], c2, 0), (a["cat2"], c3, c2)),
+            "b3a": ((a["p3"], c2, 0), (a["b3a"], c3, 0)), "b3b": ((a["b3a"], c3, 0), (a["b3b"], c3, 0)),
+            "r3": ((a["b3b"], c3, 0), (a["r3"], c2, 0)),
+            "d2a": ((a["cat2"], c3, 0), (a["d2a"], c2, 0)), "d2b": ((a["d2a"], c2, 0), (a["d2b"], c2, 0)),
+            "r2": ((a["d2b"], c2, 0), (a["r2"], c1, 0)),
+            "d1a": ((a["cat1"], c2, 0), (a["d1a"], c1, 0)), "d1b": ((a["d1a"], c1, 0), (a["d1b"], c1, 0)),
+            "r1": ((a["d1b"], c1, 0), (a["r1"], c0, 0)),
+            "d0a": ((a["cat0"], c1, 0), (a["d0a"], c0, 0)), "d0b": ((a["d0a"], c0, 0), (a["d0b"], c0, 0)),
+            "out": ((a["d0b"], c0, 0), (self.y, COUT, 0)),
         }
+
+    # the library calls, 2D or 3D (spatial sizes of the input: s x s [x s])
+    def _sp(self, s):
+        return (s,) * self.dim
+
+    def _conv_call(self, ib, ics, ico, w, bias, ob_bf, ob_f32, ocs, oco, B, s, cin, cout, k, relu):
+        f = self.lib.lbm_nn_conv if self.dim == 2 else self.lib.lbm_nn_conv3d
+        N.check(f(self._p(ib), ics, ico, self._p(w), self._p(bias), None, self._p(ob_bf), self._p(ob_f32), ocs, oco,
+                  B, *self._sp(s), cin, cout, k, int(relu), 0, self._s()))
+
+    def _pool(self, src, cs, co, dst, B, s, c):
+        f = self.lib.lbm_nn_avgpool2 if self.dim == 2 else self.lib.lbm_nn_avgpool2_3d
+        N.check(f(self._p(src), cs, co, self._p(dst), B, *self._sp(s), c, self._s()))
+
+    def _pool_bwd(self, gout, gin, cs, co, B, s, c):
+        f = self.lib.lbm_nn_avgpool2_bwd if self.dim == 2 else self.lib.lbm_nn_avgpool2_3d_bwd
+        N.check(f(self._p(gout), self._p(gin), cs, co, B, *self._sp(s), c, 1, self._s()))
+
+    def _up(self, src, dst, cs, co, B, s, c):
+        f = self.lib.lbm_nn_upsample2 if self.dim == 2 else self.lib.lbm_nn_upsample2_3d
+        N.check(f(self._p(src), self._p(dst), cs, co, B, *self._sp(s), c, self._s()))
+
+    def _up_bwd(self, gout, cs, co, gin, B, s, c):
+        f = self.lib.lbm_nn_upsample2_bwd if self.dim == 2 else self.lib.lbm_nn_upsample2_3d_bwd
+        N.check(f(self._p(gout), cs, co, self._p(gin), B, *self._sp(s), c, self._s()))
 
     def _gview(self, name):
         """Gradient buffer of a layer's output, same (stride, offset) as the output."""
@@ -347,84 +386,86 @@ class UNet:
 
     # -------------------------------------------------------------- forward
     def _conv(self, name, B, S):
-        L = LAYERS[name]
+        L = self.layers[name]
         (ib, ics, ico), (ob, ocs, oco) = self._views()[name]
         s = self._res(name, B, S)
         is_f32 = ob.dtype == torch.float32
-        N.check(self.lib.lbm_nn_conv(self._p(ib), ics, ico, self._p(self.wb[name]), self._p(self.b[name]), None,
-                                     None if is_f32 else self._p(ob), self._p(ob) if is_f32 else None, ocs, oco,
-                                     B, s, s, L.cin, L.cout, L.k, int(L.relu), 0, self._s()))
+        self._conv_call(ib, ics, ico, self.wb[name], self.b[name], None if is_f32 else ob, ob if is_f32 else None,
+                        ocs, oco, B, s, L.cin, L.cout, L.k, L.relu)
 
     def forward(self, x: torch.Tensor) -> torch.Tensor:
-        """x: (B, S, S, 8) float32 on the device; returns the (B, S, S, 8) FP32 output."""
+        """x: (B, S, S[, S], 8) float32 on the device; returns the FP32 output of the same
+        shape."""
         B, S = x.shape[0], x.shape[1]
-        if S % 8:
-            raise ValueError("S must be a multiple of 8")
+        if S % 8 or x.dim() != self.dim + 2:
+            raise ValueError(f"x must be (B, S{', S' * (self.dim - 1)}, 8) with S a multiple of 8")
         self._buffers(B, S)
-        a, s = self.a, self._s()
-        N.check(self.lib.lbm_nn_to_bf16(self._p(x.contiguous()), self._p(a["x"]), x.numel(), s))
-        lib = self.lib
+        a = self.a
+        c0, c1, c2, c3 = self.base, 2 * self.base, 4 * self.base, 8 * self.base
+        N.check(self.lib.lbm_nn_to_bf16(self._p(x.contiguous()), self._p(a["x"]), x.numel(), self._s()))
         self._conv("e0a", B, S); self._conv("e0b", B, S)
-        N.check(lib.lbm_nn_avgpool2(self._p(a["cat0"]), 64, 32, self._p(a["p1"]), B, S, S, 32, s))
+        self._pool(a["cat0"], c1, c0, a["p1"], B, S, c0)
         self._conv("e1a", B, S); self._conv("e1b", B, S)
-        N.check(lib.lbm_nn_avgpool2(self._p(a["cat1"]), 128, 64, self._p(a["p2"]), B, S // 2, S // 2, 64, s))
+        self._pool(a["cat1"], c2, c1, a["p2"], B, S // 2, c1)
         self._conv("e2a", B, S); self._conv("e2b", B, S)
-        N.check(lib.lbm_nn_avgpool2(self._p(a["cat2"]), 256, 128, self._p(a["p3"]), B, S // 4, S // 4, 128, s))
+        self._pool(a["cat2"], c3, c2, a["p3"], B, S // 4, c2)
         self._conv("b3a", B, S); self._conv("b3b", B, S); self._conv("r3", B, S)
-        N.check(lib.lbm_nn_upsample2(self._p(a["r3"]), self._p(a["cat2"]), 256, 0, B, S // 8, S // 8, 128, s))
+        self._up(a["r3"], a["cat2"], c3, 0, B, S // 8, c2)
         self._conv("d2a", B, S); self._conv("d2b", B, S); self._conv("r2", B, S)
-        N.check(lib.lbm_nn_upsample2(self._p(a["r2"]), self._p(a["cat1"]), 128, 0, B, S // 4, S // 4, 64, s))
+        self._up(a["r2"], a["cat1"], c2, 0, B, S // 4, c1)
         self._conv("d1a", B, S); self._conv("d1b", B, S); self._conv("r1", B, S)
-        N.check(lib.lbm_nn_upsample2(self._p(a["r1"]), self._p(a["cat0"]), 64, 0, B, S // 2, S // 2, 32, s))
+        self._up(a["r1"], a["cat0"], c1, 0, B, S // 2, c0)
         self._conv("d0a", B, S); self._conv("d0b", B, S); self._conv("out", B, S)
         return self.y
 
     # -------------------------------------------------------------- backward
     def _conv_bwd(self, name, B, S, need_dx=True):
         """Gradients of one layer from the gradient of its output (already in its view)."""
-        L = LAYERS[name]
+        L = self.layers[name]
         lib, s = self.lib, self._s()
         (ib, ics, ico), (ob, ocs, oco) = self._views()[name]
         gb, gcs, gco = self._gview(name)
         r = self._res(name, B, S)
-        P = B * r * r
+        P = B * r ** self.dim
         if L.relu:
             N.check(lib.lbm_nn_relu_bwd(self._p(gb), gcs, gco, self._p(ob), ocs, oco, P, L.cout, s))
-        N.check(lib.lbm_nn_conv_wgrad(self._p(ib), ics, ico, self._p(gb), gcs, gco, self._p(self.dw[name]),
-                                      B, r, r, L.cin, L.cout, L.k, s))
+        wg = lib.lbm_nn_conv_wgrad if self.dim == 2 else lib.lbm_nn_conv3d_wgrad
+        N.check(wg(self._p(ib), ics, ico, self._p(gb), gcs, gco, self._p(self.dw[name]),
+                   B, *self._sp(r), L.cin, L.cout, L.k, s))
         N.check(lib.lbm_nn_bias_grad(self._p(gb), gcs, gco, P, L.cout, self._p(self.db[name]), s))
         if not need_dx:
             return
-        N.check(lib.lbm_nn_flip_weights(self._p(self.wb[name]), self._p(self.wt[name]), L.cout, L.k * L.k, L.cin, s))
+        N.check(lib.lbm_nn_flip_weights(self._p(self.wb[name]), self._p(self.wt[name]), L.cout, L.k ** self.dim,
+                                        L.cin, s))
         key = [k for k, v in self.a.items() if v is ib][0]
-        dx = self.g[key]
-        N.check(lib.lbm_nn_conv(self._p(gb), gcs, gco, self._p(self.wt[name]), None, None, self._p(dx), None,
-                                ics, ico, B, r, r, L.cout, L.cin, L.k, 0, 0, s))
+        self._conv_call(gb, gcs, gco, self.wt[name], None, self.g[key], None, ics, ico, B, r, L.cout, L.cin, L.k,
+                        False)
 
     def backward(self, B: int, S: int) -> None:
         """Back-propagate self.gy (gradient of the loss w.r.t. the output)."""
-        lib, s, g = self.lib, self._s(), self.g
+        g = self.g
+        c0, c1, c2, c3 = self.base, 2 * self.base, 4 * self.base, 8 * self.base
         for k in self.dw:
             self.dw[k].zero_()
             self.db[k].zero_()
         for name in ("out", "d0b", "d0a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_upsample2_bwd(self._p(g["cat0"]), 64, 0, self._p(g["r1"]), B, S // 2, S // 2, 32, s))
+        self._up_bwd(g["cat0"], c1, 0, g["r1"], B, S // 2, c0)
         for name in ("r1", "d1b", "d1a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_upsample2_bwd(self._p(g["cat1"]), 128, 0, self._p(g["r2"]), B, S // 4, S // 4, 64, s))
+        self._up_bwd(g["cat1"], c2, 0, g["r2"], B, S // 4, c1)
         for name in ("r2", "d2b", "d2a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_upsample2_bwd(self._p(g["cat2"]), 256, 0, self._p(g["r3"]), B, S // 8, S // 8, 128, s))
+        self._up_bwd(g["cat2"], c3, 0, g["r3"], B, S // 8, c2)
         for name in ("r3", "b3b", "b3a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_avgpool2_bwd(self._p(g["p3"]), self._p(g["cat2"]), 256, 128, B, S // 4, S // 4, 128, 1, s))
+        self._pool_bwd(g["p3"], g["cat2"], c3, c2, B, S // 4, c2)
         for name in ("e2b", "e2a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_avgpool2_bwd(self._p(g["p2"]), self._p(g["cat1"]), 128, 64, B, S // 2, S // 2, 64, 1, s))
+        self._pool_bwd(g["p2"], g["cat1"], c2, c1, B, S // 2, c1)
         for name in ("e1b", "e1a"):
             self._conv_bwd(name, B, S)
-        N.check(lib.lbm_nn_avgpool2_bwd(self._p(g["p1"]), self._p(g["cat0"]), 64, 32, B, S, S, 32, 1, s))
+        self._pool_bwd(g["p1"], g["cat0"], c1, c0, B, S, c0)
         self._conv_bwd("e0b", B, S)
         self._conv_bwd("e0a", B, S, need_dx=False)
 
@@ -465,13 +506,15 @@ class UNet:
 def train(net: UNet, x: np.ndarray, t: np.ndarray, w: np.ndarray, epochs: int = 30, batch: int = 16,
           lr: float = 2e-3, seed: int = 0, log=None, augment: bool = True) -> dict:
     """Adam on the weighted MSE of per-channel normalised targets; cosine learning-rate
-    decay; random periodic shifts along y as augmentation.  Returns the loss history."""
+    decay; random periodic shifts along y (axis 2; 2D or 3D cases) as augmentation.
+    Returns the loss history."""
     rng = np.random.default_rng(seed)
     dev = net.dev
     # per-channel normalisation of the targets (weighted mean and std)
-    wsum = np.maximum(w.sum(axis=(0, 1, 2)), 1e-30)
-    mu = (w * t).sum(axis=(0, 1, 2)) / wsum
-    sd = np.sqrt((w * (t - mu) ** 2).sum(axis=(0, 1, 2)) / wsum)
+    ax = tuple(range(t.ndim - 1))                 # every axis but the channel
+    wsum = np.maximum(w.sum(axis=ax), 1e-30)
+    mu = (w * t).sum(axis=ax) / wsum
+    sd = np.sqrt((w * (t - mu) ** 2).sum(axis=ax) / wsum)
     sd = np.where(sd > 0, sd, 1.0).astype(np.float32)
     net.norm = (mu.astype(np.float32), sd)
     t = ((t - mu) / sd * (w > 0)).astype(np.float32)

@@ -274,3 +274,71 @@ def test_pool3d_upsample3d_and_their_gradients():
     refg = 1 + 0.125 * cl(F.interpolate(cf(p.cpu().double()), scale_factor=2))
     assert _rel(gi[..., 16:].cpu().double(), refg) < 1e-2
     assert torch.all(gi[..., :16].cpu() == 1)
+
+
+def _torch_unet_nd(net, x):
+    """The network in float64 on the CPU with its (bf16) weights, 2D or 3D."""
+    dim = net.dim
+    W = {k: net.wb[k].cpu().double().requires_grad_(True) for k in net.layers}
+    Bb = {k: net.b[k].cpu().double().requires_grad_(True) for k in net.layers}
+    cf = (lambda t: t.permute(0, 3, 1, 2)) if dim == 2 else (lambda t: t.permute(0, 4, 1, 2, 3))
+    cl = (lambda t: t.permute(0, 2, 3, 1)) if dim == 2 else (lambda t: t.permute(0, 2, 3, 4, 1))
+
+    def conv(name, t):
+        L = net.layers[name]
+        y = (_ref_conv if dim == 2 else _ref_conv3d)(t, W[name], L.k, Bb[name])
+        return torch.relu(y) if L.relu else y
+
+    def pool(t):
+        return cl((F.avg_pool2d if dim == 2 else F.avg_pool3d)(cf(t), 2))
+
+    def up(t):
+        return cl(F.interpolate(cf(t), scale_factor=2, mode="nearest"))
+
+    e0 = conv("e0b", conv("e0a", x))
+    e1 = conv("e1b", conv("e1a", pool(e0)))
+    e2 = conv("e2b", conv("e2a", pool(e1)))
+    b3 = conv("b3b", conv("b3a", pool(e2)))
+    d2 = conv("d2b", conv("d2a", torch.cat([up(conv("r3", b3)), e2], -1)))
+    d1 = conv("d1b", conv("d1a", torch.cat([up(conv("r2", d2)), e1], -1)))
+    d0 = conv("d0b", conv("d0a", torch.cat([up(conv("r1", d1)), e0], -1)))
+    return conv("out", d0), W, Bb
+
+
+def test_unet3d_gradients_match_autograd():
+    """The 3D variant (16 base channels): output, loss and gradients against autograd."""
+    from lbm_porouschem_b200.surrogate import UNet
+    net = UNet(seed=5, dim=3, base=16)
+    g = torch.Generator().manual_seed(6)
+    B, S = 2, 16
+    x = torch.randn(B, S, S, S, 8, generator=g)
+    x[..., 6:] = 0
+    t = torch.randn(B, S, S, S, 8, generator=g)
+    wgt = torch.zeros(B, S, S, S, 8)
+    wgt[..., :5] = 1
+    y = net.forward(x.cuda())
+    loss = net.loss_grad(t.cuda(), wgt.cuda())
+    net.backward(B, S)
+    yr, W, Bb = _torch_unet_nd(net, x.to(torch.bfloat16).double())
+    lr = ((yr - t.double()) ** 2 * wgt.double()).sum() / wgt.sum()
+    lr.backward()
+    assert _rel(y.cpu().double(), yr.detach()) < 5e-2
+    assert abs(loss - lr.item()) / lr.item() < 5e-2
+    for name in ("out", "d0a", "r2", "b3b", "e1a", "e0a"):
+        a = net.dw[name].cpu().double().flatten()
+        b = W[name].grad.flatten()
+        assert float(a @ b / (a.norm() * b.norm())) > 0.99, name
+        assert abs(float(a.norm() / b.norm()) - 1) < 0.1, name
+
+
+def test_warm_start_3d_small():
+    """3D sphere packings at 16^3: both starts converge to the same permeability; the step
+    counts are printed (the 32^3 experiment is in the warm-start profile)."""
+    from lbm_porouschem_b200 import surrogate3d as S3
+    r = S3.experiment(S=16, n_train=24, n_test=3, epochs=40, batch=4)
+    print({k: v for k, v in r.items() if k != "cases"})
+    for c in r["cases"]:
+        print(c)
+    assert r["train_cases"] >= 20
+    assert r["loss_last"] < 0.5 * r["loss_first"]
+    assert r["mean"]["k_rel_diff_max"] < 1e-2
