@@ -87,6 +87,15 @@ class ScalarFieldView:
         self.BC = [BC.periodic] * solver._nsides
         self.s_BC = [0.0] * solver._nsides
         self.thermal_diff = 3e-5
+        # THERMAL_DIFF_MODEL.DERIVED with constant conductivity and capacity
+        # (src/LBM/LBM2D/_thermal.py:62-107): D = cond / (rho cm)
+        self.derived = False
+        self.cond: Optional[float] = None
+        self.cm: Optional[float] = None
+        # radiation fields the reference's driver fills (src/LBM/app.py); radiation itself
+        # is not on the CUDA path (set_radiation raises)
+        self.radiation_surface = Field(solver, name + "_radiation_surface")
+        self.emissivity = Field(solver, name + "_emissivity")
 
     def get_physical_value(self, v):
         return v * self.v_scale + self.v_ref
@@ -147,6 +156,7 @@ class _SolverBase:
         self.GetVariableFunc: list[Callable] = []
         self.exportPath = "vtk"
         self.snapshotPath = "snapshot.yaml"
+        self.specieName: list = []          # no species transport on the CUDA path
         self.PVD = PVDWriter(self.exportPath, name)
         # node coordinates of the VTK grid (src/LBM/LBM2D/_core.py:38-40)
         self.x = np.linspace(0, X, self.nx)
@@ -222,6 +232,41 @@ class _SolverBase:
     def set_fluid_Prandtl(self, Pr):
         self.TF.thermal_diff = self.visco / Pr
 
+    # derived diffusivity D = cond / (rho cm) (src/LBM/LBM2D/_io.py:182-248,
+    # _thermal.py:62-107): constant conductivity and capacity only; the fluid density is
+    # taken as rho0 = 1 (the reference divides by the cell's lattice density, ~1), the
+    # solid's from add_rho_solid (uniform over the solid cells)
+    def set_fluid_thermal_diff_derived(self):
+        self.TF.derived = True
+
+    def set_fluid_conductivity(self, value):
+        self.TF.cond = float(value)
+
+    def set_fluid_capacity(self, value):
+        self.TF.cm = float(value)
+
+    def set_solid_thermal_diff_derived(self):
+        self.TS.derived = True
+
+    def set_solid_conductivity(self, value):
+        self.TS.cond = float(value)
+
+    def set_solid_capacity(self, value):
+        self.TS.cm = float(value)
+
+    def _derived_diff(self, view: ScalarFieldView, rho: float) -> float:
+        if view.cond is None or view.cm is None:
+            raise ValueError(f"{view.name}: a derived diffusivity needs set_*_conductivity and set_*_capacity")
+        return view.cond / (rho * view.cm)
+
+    def _solid_density(self) -> float:
+        s = self.solid._host >= 1
+        r = self.rhos._host[s]
+        if r.size == 0 or not np.all(r == r.flat[0]) or r.flat[0] <= 0:
+            raise NotImplementedError("a derived solid diffusivity needs one positive solid density "
+                                      "(add_rho_solid) on every solid cell on the CUDA path")
+        return float(r.flat[0])
+
     def set_BC(self, i, bc):
         """Flow side type (src/LBM/LBM2D/_io.py:385-402)."""
         self.bc[i] = bc
@@ -285,6 +330,10 @@ class _SolverBase:
 
     def set_specie(self, *a, **k):
         raise NotImplementedError("species transport is not on the CUDA path; use set_pyrolysis()")
+
+    def set_radiation(self, model, param):
+        raise NotImplementedError("surface radiation of the solid (src/LBM/LBM2D/_thermal.py:213-220) is not on "
+                                  "the CUDA path")
 
     def add_reaction(self, *a, **k):
         raise NotImplementedError("general reaction networks are not on the CUDA path; use set_pyrolysis()")
@@ -364,8 +413,10 @@ class _SolverBase:
             nu=self._nu_lu(), force=self.body_force, half_force_velocity=self.half_force_velocity,
             thermal=self._thermal_mode(), sides=self._sides())
         if self.TEMPERATURE:
-            cfg.tauT_fluid = self._tau_T(self.TF.thermal_diff)
-            cfg.tauT_solid = self._tau_T(self.TS.thermal_diff)
+            dF = self._derived_diff(self.TF, 1.0) if self.TF.derived else self.TF.thermal_diff
+            dS = self._derived_diff(self.TS, self._solid_density()) if self.TS.derived else self.TS.thermal_diff
+            cfg.tauT_fluid = self._tau_T(dF)
+            cfg.tauT_solid = self._tau_T(dS)
             cfg.T_ref, cfg.T_scale = self.TF.v_ref, self.TF.v_scale
         if self._pyro:
             pz = self._pyro
@@ -521,6 +572,32 @@ class _SolverBase:
         if self._lat is not None:
             self._lat.close()
             self._lat = None
+
+
+def _unsupported(name: str, why: str):
+    def method(self, *a, **k):
+        raise NotImplementedError(f"{name}: {why}")
+    method.__name__ = name
+    method.__doc__ = f"Reference setter (src/LBM/LBM2D/_io.py) that raises here: {why}."
+    return method
+
+
+_TEMP_DEP = "temperature-dependent properties are not on the CUDA path (one constant diffusivity per phase)"
+_SPECIES = "species transport is not on the CUDA path; use set_pyrolysis()"
+for _n, _why in [
+    ("set_fluid_conductivity_poly", _TEMP_DEP), ("set_fluid_conductivity_mixture", _SPECIES),
+    ("set_fluid_capacity_poly", _TEMP_DEP), ("set_fluid_capacity_NASA7", _TEMP_DEP),
+    ("set_fluid_capacity_mixture", _SPECIES),
+    ("set_solid_conductivity_poly", _TEMP_DEP), ("set_solid_conductivity_mixture", _SPECIES),
+    ("set_solid_capacity_poly", _TEMP_DEP), ("set_solid_capacity_NASA7", _TEMP_DEP),
+    ("set_solid_capacity_mixture", _SPECIES),
+    ("set_specie_viscosity", _SPECIES), ("set_specie_viscosity_sutherland", _SPECIES),
+    ("set_specie_diff", _SPECIES), ("set_specie_diff_Schmidt", _SPECIES), ("set_specie_capacity", _SPECIES),
+    ("set_specie_enthalpy", _SPECIES), ("set_specie_NASA7", _SPECIES), ("set_specie_conductivity", _SPECIES),
+    ("set_specie_conductivity_poly", _SPECIES), ("set_specie_BC", _SPECIES), ("set_specie_BC_value", _SPECIES),
+    ("set_species_BC", _SPECIES), ("init_specie", _SPECIES),
+]:
+    setattr(_SolverBase, _n, _unsupported(_n, _why))
 
 
 class LBM2DSolver(_SolverBase):

@@ -157,3 +157,38 @@ def test_solver_steps_like_lattice():
     assert "Max velocity magnitude" in s.log_info()
     s.close()
     lat.close()
+
+
+def test_reference_surface_is_complete():
+    """Every method and attribute the reference's driver touches exists (src/LBM/app.py:
+    101-677); those outside the CUDA path raise NotImplementedError naming themselves."""
+    s = LBM3DSolver(X=8, Y=8, Z=8, dx=1, isThermal=True)
+    for n in ("set_fluid_conductivity_poly", "set_fluid_capacity_NASA7", "set_solid_capacity_mixture",
+              "set_specie_diff", "set_specie_BC", "set_species_BC", "init_specie", "set_radiation"):
+        with pytest.raises(NotImplementedError, match=n if n != "set_radiation" else "radiation"):
+            getattr(s, n)(*([None] * (2 if n in ("set_radiation", "set_fluid_capacity_NASA7") else 1)))
+    assert s.specieName == [] and s.TS.radiation_surface is not None and s.TS.emissivity is not None
+
+
+def test_derived_thermal_diffusivity():
+    """D = cond / (rho cm) with constant conductivity and capacity (src/LBM/LBM2D/_thermal.py:62-107):
+    fluid at rho0 = 1, solid at its (uniform) density."""
+    s = LBM2DSolver(X=0.016, Y=0.008, Z=0, dx=1e-3, dt=1e-4, isThermal=True)
+    s.set_viscosity(2e-5)
+    solid = np.zeros((16, 8, 1))
+    solid[6:10, 2:6] = 1.0
+    s.add_solid(solid)
+    s.add_rho_solid(solid * 500.0)
+    s.set_fluid_thermal_diff_derived()
+    s.set_fluid_conductivity(0.03)
+    s.set_fluid_capacity(1000.0)
+    s.set_solid_thermal_diff_derived()
+    s.set_solid_conductivity(0.5)
+    s.set_solid_capacity(1500.0)
+    cfg = s._config()
+    lu = 1e-4 / 1e-6
+    assert cfg.tauT_fluid == pytest.approx(3 * (0.03 / 1000.0) * lu + 0.5)
+    assert cfg.tauT_solid == pytest.approx(3 * (0.5 / (500.0 * 1500.0)) * lu + 0.5)
+    s.add_rho_solid(solid * np.linspace(0, 1, 16)[:, None, None])     # no longer uniform
+    with pytest.raises(NotImplementedError, match="solid density"):
+        s._config()
