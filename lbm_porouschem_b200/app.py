@@ -4,7 +4,8 @@ Sections read: ``basic`` (dimension, name; ``arch`` is ignored, the lattice alwa
 GPU; ``collision`` / ``precision`` select BGK|MRT and fp32|fp16|fp64), ``spaceControl``
 (geometry, DX), ``timeControl`` (DT, startTime, endTime), ``module``, ``flowProperties``
 (constant viscosity, optional ``force``), ``thermalPropertiesFluid`` / ``thermalPropertiesSolid``
-(normalize.Trange, thermalDiff constant|Prandtl), ``chemicalProperties`` with ``type: pyrolysis``
+(normalize.Trange, thermalDiff constant|Prandtl|derived, constant conductivity and capacity),
+``chemicalProperties`` with ``type: pyrolysis``
 (single-step pyrolysis of reactive solid zones), ``boundaryCondition`` (inlet / outlet / wall /
 periodic flow sides, fixedValue / zeroGradient / periodic temperature), ``geometry`` (sphere,
 cylinder, cone, box voxelised analytically at cell centres), ``initialCondition`` (flow, thermal,
@@ -145,23 +146,41 @@ def build_case(config: dict, logger: logging.Logger):
     if flow.get("force") is not None:
         lb.set_body_force([float(v) for v in flow["force"]])
 
-    for key, setter_range, setter_diff in (("thermalPropertiesFluid", lb.set_fluid_Trange, lb.set_fluid_thermal_diff),
-                                           ("thermalPropertiesSolid", lb.set_solid_Trange, lb.set_solid_thermal_diff)):
+    for key, side in (("thermalPropertiesFluid", "fluid"), ("thermalPropertiesSolid", "solid")):
         tp = config.get(key)
         if not (is_thermal and tp):
             continue
+        setter = lambda name: getattr(lb, f"set_{side}_{name}")     # noqa: E731
         norm = tp.get("normalize")
         if norm:
-            setter_range(norm.get("Trange", [0, 1]))
+            setter("Trange")(norm.get("Trange", [0, 1]))
         td = tp.get("thermalDiff")
         if td:
             ttype = td.get("type", "constant")
             if ttype == "constant":
-                setter_diff(float(td["value"]))
-            elif ttype == "Prandtl" and key == "thermalPropertiesFluid":
+                setter("thermal_diff")(float(td["value"]))
+            elif ttype == "Prandtl" and side == "fluid":
                 lb.set_fluid_Prandtl(float(td["Pr"]))
+            elif ttype == "derived":
+                setter("thermal_diff_derived")()
             else:
                 raise NotImplementedError(f"{key}.thermalDiff.type {ttype!r} is not on the CUDA path")
+        # src/LBM/app.py:143-175: constant values; polynomial / NASA7 / mixture raise in the setters
+        for prop in ("conductivity", "capacity"):
+            pd = tp.get(prop)
+            if not pd:
+                continue
+            ptype = pd.get("type", "constant")
+            if ptype == "constant":
+                setter(prop)(float(pd["value"]))
+            elif ptype == "polynomial":
+                setter(prop + "_poly")(pd.get("data"))
+            elif ptype == "NASA7" and prop == "capacity":
+                setter("capacity_NASA7")(pd.get("Trange"), pd.get("data"))
+            elif ptype == "mixture":
+                setter(prop + "_mixture")()
+            else:
+                raise ValueError(f"{key}.{prop}.type {ptype!r} not valid")
 
     chem = config.get("chemicalProperties")
     pyro_zone = None

@@ -126,3 +126,17 @@ def test_cli_runs_case(tmp_path, monkeypatch):
     d = read_vts(str(tmp_path / "out" / series[-1][1]))
     assert np.isfinite(d["rho"]).all() and d["Tf"].max() > 300.0    # the hot inlet has warmed the fluid
     assert d["velocity"].shape == (d["rho"].size, 3)
+
+
+def test_derived_thermal_properties_from_yaml():
+    """thermalDiff type derived with constant conductivity and capacity (src/LBM/app.py:132-175);
+    polynomial properties stop the run."""
+    cfg = yaml.safe_load(CASE2D)
+    cfg["thermalPropertiesFluid"]["thermalDiff"] = {"type": "derived"}
+    cfg["thermalPropertiesFluid"]["conductivity"] = {"type": "constant", "value": 0.03}
+    cfg["thermalPropertiesFluid"]["capacity"] = {"type": "constant", "value": 1000.0}
+    lb = build_case(cfg, _log())
+    assert lb.TF.derived and lb.TF.cond == 0.03 and lb.TF.cm == 1000.0
+    cfg["thermalPropertiesFluid"]["capacity"] = {"type": "polynomial", "data": [1000, 0, 0, 0, 0]}
+    with pytest.raises(NotImplementedError, match="capacity_poly"):
+        build_case(cfg, _log())
