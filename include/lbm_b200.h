@@ -209,6 +209,13 @@ LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
  * src/LBM/LBM2D/_evolution.py:15). */
 LBM_API int64_t lbm_step_count(const lbm_handle* h);
 
+/* Count n steps (n even) that a replay of a CUDA graph captured around
+ * lbm_step(h, n, flags, stream) took: capturing runs no kernel but moves the
+ * step counter by n, so the first replay brings the state level with the
+ * counter and every later replay is followed by lbm_advance(h, n).  No
+ * reference counterpart (the reference launches two Taichi kernels per step). */
+LBM_API int32_t lbm_advance(lbm_handle* h, int32_t n);
+
 /* Batches: many initialised lattices (same dim, precision, collision, thermal and
  * pyrolysis settings; sizes, geometries and parameters free; each created with
  * bulk_form = 2) stepped together by one persistent launch per kernel, for

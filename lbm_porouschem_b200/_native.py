@@ -42,7 +42,7 @@ EXPORTED = (
     "lbm_abi_version", "lbm_last_error", "lbm_required_bytes", "lbm_create", "lbm_destroy",
     "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_resume", "lbm_step", "lbm_compute_macro",
     "lbm_read_diag",
-    "lbm_step_count", "lbm_diag_noalloc", "lbm_stl_work_bytes", "lbm_voxelise_stl",
+    "lbm_step_count", "lbm_advance", "lbm_diag_noalloc", "lbm_stl_work_bytes", "lbm_voxelise_stl",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
     "lbm_batch_set_blocks",
     "lbm_nn_conv", "lbm_nn_conv_wgrad", "lbm_nn_bias_grad", "lbm_nn_flip_weights", "lbm_nn_avgpool2",
@@ -124,6 +124,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_init_equilibrium.restype = i32
     lib.lbm_resume.argtypes = [vp, i64, vp]
     lib.lbm_resume.restype = i32
+    lib.lbm_advance.argtypes = [vp, i32]
+    lib.lbm_advance.restype = i32
     lib.lbm_stl_work_bytes.argtypes = [i32, i32, i32, i32, C.POINTER(sz)]
     lib.lbm_stl_work_bytes.restype = i32
     lib.lbm_voxelise_stl.argtypes = [vp, i64, i32, i32, i32, i32, C.c_double, vp, sz, vp, vp, vp]

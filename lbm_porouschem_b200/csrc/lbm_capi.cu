@@ -556,6 +556,14 @@ int32_t lbm_batch_set_blocks(lbm_batch* b, int32_t blocks_per_sm) {
   return LBM_OK;
 }
 
+int32_t lbm_advance(lbm_handle* h, int32_t n) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  if (n < 0 || (n & 1)) return fail(LBM_ERR_ARG, "n must be even and >= 0 (a captured sequence keeps the parity)");
+  h->step += n;
+  h->diag_valid = false;
+  return LBM_OK;
+}
+
 int32_t lbm_batch_advance(lbm_batch* b, int32_t n) {
   if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
   if (n < 0 || (n & 1)) return fail(LBM_ERR_ARG, "n must be even and >= 0 (a captured sequence keeps the parity)");

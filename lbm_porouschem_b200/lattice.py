@@ -174,6 +174,31 @@ class Lattice:
                 (N.LBM_STEP_RESIDUAL if residual else 0)
         N.check(self.lib.lbm_step(self._h, int(n), flags, self._s()))
 
+    def capture(self, n: int) -> None:
+        """Record n ordinary steps (n even) as a CUDA graph on the lattice's stream (one
+        is required).  Capturing runs no kernel but moves the step counter by n; the first
+        replay() brings the state level with it, every later replay advances both."""
+        if self.stream is None:
+            raise RuntimeError("capture needs the lattice to own a stream (Lattice(cfg, stream=...))")
+        if n <= 0 or n % 2:
+            raise ValueError("a captured sequence must have an even number of steps")
+        self.stream.synchronize()
+        g = torch.cuda.CUDAGraph()
+        with torch.cuda.graph(g, stream=self.stream):
+            N.check(self.lib.lbm_step(self._h, int(n), 0, self._s()))
+        self.graph, self._graph_steps, self._counted = g, n, True
+
+    def replay(self) -> None:
+        """Run the captured steps once more (capture() first)."""
+        if getattr(self, "graph", None) is None:
+            raise RuntimeError("capture() first")
+        with torch.cuda.stream(self.stream):
+            self.graph.replay()
+        if self._counted:
+            self._counted = False
+        else:
+            N.check(self.lib.lbm_advance(self._h, self._graph_steps))
+
     def compute(self, diag: bool = True, macro: bool = False, residual: bool = False) -> None:
         """Recompute outputs for the current state without advancing it."""
         flags = (N.LBM_STEP_DIAG if diag else 0) | (N.LBM_STEP_MACRO if macro else 0) | \
@@ -300,6 +325,7 @@ class Lattice:
     def close(self) -> None:
         if getattr(self, "buf", None):
             (self.stream or torch.cuda.current_stream()).synchronize()
+        self.graph = None
         if getattr(self, "_h", None) is not None and self._h.value:
             self.lib.lbm_destroy(self._h)
             self._h = ctypes.c_void_p()
