@@ -135,6 +135,11 @@ struct lbm_handle {
   lbm::capi::Launch L;
   bool diag_valid;
   bool initialised;  // lbm_init_equilibrium ran (state and cell lists exist)
+  // list form with active sides: the boundary kernel runs on a second stream beside
+  // the list kernel (created at the first step; null: one stream)
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+  bool side_tried = false;
 };
 
 // A batch of lattices stepped together (batch_kernel.cuh).  Its device tables

@@ -23,9 +23,36 @@ static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st
   step_list<Lt, S, COLL, THERM, MODE><<<L.bulk_blocks, 128, smem, st>>>(p);
 }
 
+// Second stream for the boundary kernel (list form with active sides), made on the
+// device current at the first step; on failure the step stays on one stream.
+inline void ensure_side_stream(lbm_handle* h) {
+  if (h->side_tried) return;
+  h->side_tried = true;
+  if (!(h->L.list && h->L.nfaces > 0)) return;
+  if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
+    cudaGetLastError();
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->side) cudaStreamDestroy(h->side);
+    h->side = nullptr;
+    h->ev_fork = h->ev_join = nullptr;
+  }
+}
+
 template <class Lt, class S, int COLL, int THERM>
 static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const Launch& L = h->L;
+  ensure_side_stream(h);
+  // list form: the boundary kernel is independent of the list kernel (both read the
+  // input half only and write disjoint slots, partial rows apart), so it runs on the
+  // second stream and its blocks take the SMs that the persistent list kernel's blocks
+  // leave as they finish; flip_cells waits for both
+  const bool fork = L.list && L.nfaces > 0 && h->side != nullptr;
+  if (fork) {
+    cudaEventRecord(h->ev_fork, st);
+    cudaStreamWaitEvent(h->side, h->ev_fork, 0);
+  }
   if (L.staged) {
     using LY = StagedLayout<Lt, S, kStagedTile>;
     constexpr size_t smem = (size_t)kStagedStages * LY::STAGE_BYTES;
@@ -47,7 +74,11 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
     p.block_offset = L.bulk_blocks;
     const int4 f01 = make_int4(L.faces[0], L.faces[1], L.faces[2], L.faces[3]);
     const int2 f2 = make_int2(L.faces[4], L.faces[5]);
-    step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, st>>>(p, f01, f2);
+    step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, fork ? h->side : st>>>(p, f01, f2);
+  }
+  if (fork) {
+    cudaEventRecord(h->ev_join, h->side);
+    cudaStreamWaitEvent(st, h->ev_join, 0);
   }
   if constexpr (THERM == 2) {
     // after the boundary kernel: it moves mirrored populations of boundary cells too

@@ -190,6 +190,11 @@ int32_t lbm_create(const lbm_desc* d, lbm_handle** out) {
 }
 
 int32_t lbm_destroy(lbm_handle* h) {
+  if (h) {
+    if (h->ev_fork) cudaEventDestroy(h->ev_fork);
+    if (h->ev_join) cudaEventDestroy(h->ev_join);
+    if (h->side) cudaStreamDestroy(h->side);
+  }
   delete h;
   return LBM_OK;
 }
