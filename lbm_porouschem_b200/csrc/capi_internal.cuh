@@ -105,7 +105,7 @@ inline Launch plan(const lbm_desc& d, int tx) {
   L.list_cap = 2 * (size_t)L.list_base;
   L.list_nbb = (int)((L.N + kListChunk - 1) / kListChunk);
   if (L.list) {
-    const int per_sm = d.precision == LBM_PREC_FP64 ? 2 : 4;  // 128-thread blocks at the register cap
+    const int per_sm = list_blocks_per_sm(d.precision == LBM_PREC_FP64);  // 128-thread blocks at the register cap
     const long chunks = (long)(L.N / 32) + 8;
     L.bulk_blocks = (int)std::max<long>(1, std::min<long>((chunks + 3) / 4, (long)sm_count() * per_sm));
   }

@@ -506,7 +506,7 @@ int32_t lbm_batch_create(lbm_handle* const* hs, int32_t n, void* dev_scratch, si
   b->bc = (int4*)((char*)b->chunks + (chunks.size() * sizeof(int2) + 255) / 256 * 256);
   b->nbc = (int)bc.size();
   b->list_blocks = (int)std::max<long>(1, std::min<long>(((long)chunks.size() + 3) / 4,
-                                                          (long)sm_count() * (hs[0]->d.precision == LBM_PREC_FP64 ? 2 : 4)));
+                                                          (long)sm_count() * list_blocks_per_sm(hs[0]->d.precision == LBM_PREC_FP64)));
   b->flip_blocks = 4;
   // parameters of every lattice at both parities, staged on the host
   std::vector<unsigned char> host((size_t)n * 2 * pb);
@@ -554,7 +554,7 @@ int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream) {
 
 int32_t lbm_batch_set_blocks(lbm_batch* b, int32_t blocks_per_sm) {
   if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
-  const int cap = b->hs[0]->d.precision == LBM_PREC_FP64 ? 2 : 4;  // resident blocks at the register cap
+  const int cap = list_blocks_per_sm(b->hs[0]->d.precision == LBM_PREC_FP64);  // resident blocks at the register cap
   if (blocks_per_sm < 1 || blocks_per_sm > cap)
     return fail(LBM_ERR_ARG, "blocks_per_sm must be 1.." + std::to_string(cap));
   b->list_blocks = (int)std::max<long>(1, std::min<long>(((long)b->nchunks + 3) / 4, (long)sm_count() * blocks_per_sm));

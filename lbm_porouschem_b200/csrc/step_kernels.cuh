@@ -65,12 +65,20 @@ constexpr double kGasConstant = 8.314441; // src/LBM/util/constant.py:17
 
 // Register cap of the FP32/FP16 bulk kernels (FP64 keeps the full budget):
 // 128 registers = 4 blocks of 128 threads (16 warps) per SM.  On B200 at 256^3
-// (D3Q19-MRT + D3Q7 + pyrolysis) 96 and 80 measured no faster.
+// (D3Q19-MRT + D3Q7 + pyrolysis), 96 and 80 registers with 5 and 6 blocks per SM
+// measured slower: FP32 10.9 and 9.2 GLUPS, FP16 15.8 and 15.1, against 12.3 and 18.0.
 #ifndef LBM_BULK_MAXNREG
 #define LBM_BULK_MAXNREG 128
 #endif
 template <class S> struct BulkRegs { static constexpr int v = LBM_BULK_MAXNREG; };
 template <> struct BulkRegs<double> { static constexpr int v = 255; };
+
+// Resident 128-thread list-kernel blocks per SM at the register cap (65,536
+// registers per SM, allocated 8 per thread at a time): 4 at 128, 2 for FP64.
+inline int list_blocks_per_sm(bool fp64) {
+  const int regs = ((fp64 ? BulkRegs<double>::v : BulkRegs<float>::v) + 7) / 8 * 8;
+  return 65536 / (128 * regs);
+}
 
 template <class S>
 struct StepParams {
