@@ -62,6 +62,18 @@ extern "C" {
 #define LBM_BC_PERIODIC 0        /* util/flag.py:89-94 BC */
 #define LBM_BC_ZEROGRADIENT 1
 #define LBM_BC_FIXEDVALUE 2
+/* Velocity type of side 0 (x-) only: the reference's flow-rate inlet BC_FLOW.inlet_flow
+ * (src/LBM/LBM2D/_boundary.py:324-333, _initialize.py:67-73).  side[0].v[0] is the
+ * target flow rate F (sum of rho*u_x over the side's cells, lattice units).  Before
+ * each step, with flow0 = sum of rho*u_x over the side's cells and u1(j) the velocity
+ * of the cell behind side cell j (x = 1), both as the previous step left them, side
+ * cell j takes the velocity (0.01*F/flow0 + 0.99) * u1(j).  As the reference's
+ * init_boundary does, lbm_init_equilibrium gives the columns x = 0 and 1 the velocity
+ * (v0, 0, 0), v0 = F/ny/nz, in place of the u plane's (the reference writes it into
+ * the macro velocity that its first collision reads; here the populations start at
+ * that equilibrium).  The controller's state lives in LBM_FIELD_INLET.  A
+ * proportional controller: its steady flux is F only where u(x = 0) = u(x = 1). */
+#define LBM_BC_FLOWRATE 3
 
 /* mask byte: bit0/bit1 = solid at even/odd step parity, bit2 = reactive solid */
 #define LBM_MASK_SOLID 3u
@@ -133,7 +145,11 @@ typedef struct lbm_diag {
 #define LBM_FIELD_T 7
 #define LBM_FIELD_UPREV 8   /* 3 float32 planes, residual reference */
 #define LBM_FIELD_SCRATCH 9 /* reduction partials, control block, cell lists of the bulk update */
-#define LBM_NUM_FIELDS 10
+#define LBM_FIELD_INLET 10  /* flow-rate inlet state (side 0 of type LBM_BC_FLOWRATE, else 0 bytes):
+                               the step's coefficient F/flow0, then per step parity the
+                               rho*u_x of each side cell and the velocity behind it
+                               (compute precision); part of a checkpoint */
+#define LBM_NUM_FIELDS 11
 
 /* lbm_step flags */
 #define LBM_STEP_DIAG 1      /* reduce diagnostics on the last step */

@@ -26,13 +26,13 @@ LBM_COLL_BGK, LBM_COLL_MRT = 0, 1
 LBM_PREC_FP32, LBM_PREC_FP16, LBM_PREC_FP64 = 0, 1, 2
 LBM_EOS_IDEAL_GAS, LBM_EOS_INCOMPRESSIBLE = 0, 1
 LBM_THERMAL_NONE, LBM_THERMAL_CONJUGATE, LBM_THERMAL_TWOFIELD = 0, 1, 2
-LBM_BC_PERIODIC, LBM_BC_ZEROGRADIENT, LBM_BC_FIXEDVALUE = 0, 1, 2
+LBM_BC_PERIODIC, LBM_BC_ZEROGRADIENT, LBM_BC_FIXEDVALUE, LBM_BC_FLOWRATE = 0, 1, 2, 3
 LBM_MASK_SOLID = 3
 LBM_MASK_REACTIVE = 4
 
 (LBM_FIELD_F, LBM_FIELD_G, LBM_FIELD_MASK, LBM_FIELD_ALPHA, LBM_FIELD_REL, LBM_FIELD_RHO,
- LBM_FIELD_U, LBM_FIELD_T, LBM_FIELD_UPREV, LBM_FIELD_SCRATCH) = range(10)
-LBM_NUM_FIELDS = 10
+ LBM_FIELD_U, LBM_FIELD_T, LBM_FIELD_UPREV, LBM_FIELD_SCRATCH, LBM_FIELD_INLET) = range(11)
+LBM_NUM_FIELDS = 11
 
 LBM_STEP_DIAG = 1
 LBM_STEP_MACRO = 2

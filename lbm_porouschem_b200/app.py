@@ -214,7 +214,11 @@ def build_case(config: dict, logger: logging.Logger):
         elif t == "symmetric":
             lb.set_BC(i, BC_FLOW.symmetric)
         elif t == "inlet_flowrate":
-            raise NotImplementedError("boundaryCondition flow type 'inlet_flowrate' is not on the CUDA path")
+            # src/LBM/app.py:358-364
+            lb.set_BC(i, BC_FLOW.inlet_flow)
+            lb.set_flow_BC_value(i, float(bf["flowrate"]))
+            if bf.get("rho", 1):
+                lb.set_rho_BC_value(i, float(bf.get("rho", 1)))
         elif t not in ("periodic", None):
             raise ValueError(f"boundaryCondition.{_SIDES[i]}.flow.type {t!r} not valid")
         if is_thermal:

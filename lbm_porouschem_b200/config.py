@@ -14,6 +14,7 @@ from dataclasses import dataclass, field
 from . import _native as N
 
 PERIODIC, ZERO_GRADIENT, FIXED_VALUE = N.LBM_BC_PERIODIC, N.LBM_BC_ZEROGRADIENT, N.LBM_BC_FIXEDVALUE
+FLOW_RATE = N.LBM_BC_FLOWRATE   # velocity type of side 0 only (flow-rate inlet)
 
 # d'Humieres et al. (2002) rates for D3Q19: e, eps, q, pi, m (viscous rows use 1/tau)
 MRT_RATES_3D = {1: 1.19, 2: 1.4, 4: 1.2, 6: 1.2, 8: 1.2, 10: 1.4, 12: 1.4, 16: 1.98, 17: 1.98, 18: 1.98}
@@ -50,6 +51,13 @@ class SideBC:
     @staticmethod
     def wall(T_type=PERIODIC, T=0.0) -> "SideBC":
         return SideBC(True, FIXED_VALUE, ZERO_GRADIENT, T_type, (0.0, 0.0, 0.0), 1.0, T)
+
+    @staticmethod
+    def inlet_flowrate(flowrate, T_type=PERIODIC, T=0.0) -> "SideBC":
+        """Flow-rate inlet, side 0 only (the reference's BC_FLOW.inlet_flow,
+        src/LBM/LBM2D/_boundary.py:324-333): the inlet velocity is steered each step
+        so that the sum of rho*u_x over the side's cells approaches ``flowrate``."""
+        return SideBC(True, FLOW_RATE, ZERO_GRADIENT, T_type, (float(flowrate), 0.0, 0.0), 1.0, T)
 
 
 @dataclass

@@ -34,6 +34,10 @@ inline size_t storage_bytes(int prec) { return prec == LBM_PREC_FP16 ? 2 : (prec
 inline size_t compute_bytes(int prec) { return prec == LBM_PREC_FP64 ? 8 : 4; }
 inline int lat_q(int dim) { return dim == 2 ? 9 : 19; }
 inline int lat_qt(int dim) { return dim == 2 ? 5 : 7; }
+// Flow-rate inlet (side 0 of velocity type LBM_BC_FLOWRATE) and the element count of
+// its state in LBM_FIELD_INLET (compute precision).
+inline bool has_flowrate(const lbm_desc& d) { return d.side[0].active && d.side[0].v_type == LBM_BC_FLOWRATE; }
+inline size_t inlet_elems(const lbm_desc& d) { return kInletHead + 2 * 4 * (size_t)d.ny * d.nz; }
 
 struct Launch {
   int tx;             // threads per block along x (bulk kernel)
@@ -254,6 +258,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.u_out = (C*)h->ptr[LBM_FIELD_U];
   p.T_out = (C*)h->ptr[LBM_FIELD_T];
   p.uprev = (float*)h->ptr[LBM_FIELD_UPREV];
+  p.inlet = has_flowrate(d) ? (C*)h->ptr[LBM_FIELD_INLET] : nullptr;
   if (h->L.list && h->ptr[LBM_FIELD_SCRATCH]) {
     p.lhdr = scratch_lhdr(h);
     p.ent_c = scratch_ent_c(h);

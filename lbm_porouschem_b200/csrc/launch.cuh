@@ -44,6 +44,9 @@ template <class Lt, class S, int COLL, int THERM>
 static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const Launch& L = h->L;
   ensure_side_stream(h);
+  // flow-rate inlet: this step's coefficient, before the kernels that read it (a
+  // recompute of the last step reuses the one it had)
+  if (p.inlet && !(p.flags & kStepPeek)) inlet_flow_coef<S><<<1, 1024, 0, st>>>(p);
   // list form: the boundary kernel is independent of the list kernel (both read the
   // input half only and write disjoint slots, partial rows apart), so it runs on the
   // second stream and its blocks take the SMs that the persistent list kernel's blocks

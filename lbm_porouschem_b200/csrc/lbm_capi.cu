@@ -49,8 +49,12 @@ static int validate(const lbm_desc* d) {
     if (!sd.active) continue;
     if (d->dim == 2 && s >= 4) return fail(LBM_ERR_ARG, "z sides cannot be active in 2D");
     const int types[3] = {sd.v_type, sd.rho_type, sd.T_type};
-    for (int t : types)
-      if (t < LBM_BC_PERIODIC || t > LBM_BC_FIXEDVALUE) return fail(LBM_ERR_ARG, "bad side bc type");
+    for (int i = 0; i < 3; ++i) {
+      if (i == 0 && s == 0 && types[i] == LBM_BC_FLOWRATE) continue;
+      if (types[i] < LBM_BC_PERIODIC || types[i] > LBM_BC_FIXEDVALUE)
+        return fail(LBM_ERR_ARG, types[i] == LBM_BC_FLOWRATE ? "the flow-rate type is for the velocity of side 0 only"
+                                                              : "bad side bc type");
+    }
   }
   if ((d->side[0].active && d->side[1].active && d->nx < 4) ||
       (d->side[2].active && d->side[3].active && d->ny < 4) ||
@@ -163,6 +167,7 @@ int32_t lbm_required_bytes(const lbm_desc* d, int32_t field, size_t* bytes) {
     case LBM_FIELD_U: *bytes = 3 * N * cb; break;
     case LBM_FIELD_T: *bytes = d->thermal ? N * cb : 0; break;
     case LBM_FIELD_UPREV: *bytes = 3 * N * 4; break;
+    case LBM_FIELD_INLET: *bytes = has_flowrate(*d) ? inlet_elems(*d) * cb : 0; break;
     case LBM_FIELD_SCRATCH: {
       const Launch L = plan(*d, default_tx(*d));
       *bytes = scratch_bytes(L);
@@ -240,6 +245,8 @@ static int check_bound(lbm_handle* h) {
   if (h->d.thermal && !h->ptr[LBM_FIELD_G]) return fail(LBM_ERR_UNBOUND, "field G is not bound");
   if (h->d.pyro && (!h->ptr[LBM_FIELD_ALPHA] || !h->ptr[LBM_FIELD_REL]))
     return fail(LBM_ERR_UNBOUND, "pyrolysis needs ALPHA and REL bound");
+  if (has_flowrate(h->d) && !h->ptr[LBM_FIELD_INLET])
+    return fail(LBM_ERR_UNBOUND, "a flow-rate inlet needs INLET bound");
   return LBM_OK;
 }
 
@@ -268,6 +275,7 @@ int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector
         h->d.thermal != d0.thermal || h->d.pyro != d0.pyro)
       return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, thermal and pyro");
     if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
+    if (has_flowrate(h->d)) return fail(LBM_ERR_ARG, "batch members cannot have a flow-rate inlet");
     for (int j = 0; j < i; ++j)
       if (hs[j] == h) return fail(LBM_ERR_ARG, "a lattice appears twice in the batch");
   }
@@ -356,7 +364,10 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
     using S = decltype(s);
     // buf = 1 makes fB/gB/relB the buffers that the first step (parity 0) reads
     StepParams<S> p = make_params<S>(h, 1);
-    return dispatch_init<Lt, S>(h, p, rho, u, T, alpha, solid_bit, st);
+    rc = dispatch_init<Lt, S>(h, p, rho, u, T, alpha, solid_bit, st);
+    if (rc == LBM_OK && p.inlet)
+      inlet_seed<<<1, 1024, 0, st>>>(p.inlet, rho, p.nx, p.ny, p.nz, h->d.side[0].v[0]);
+    return rc;
   });
   if (rc) return rc;
   LBM_CUDA_TRY(cudaGetLastError());

@@ -60,6 +60,16 @@ template <> struct Store<__half> {
 };
 
 constexpr int kNumDiag = 10;              // partial slots per block (order of lbm_diag fields)
+
+// Flow-rate inlet state (LBM_FIELD_INLET, compute precision): slot 0 holds the
+// coefficient F/flow0 of the current step; after kInletHead slots come two halves,
+// one per step parity, each of 4 planes over the side's cells j = y + ny*z: rho*u_x
+// of side cell (0,y,z) and the velocity of cell (1,y,z), as the step before left them.
+constexpr int kInletHead = 32;
+template <class C>
+__host__ __device__ __forceinline__ C* inlet_half(C* base, int half, size_t M) {
+  return base + kInletHead + (size_t)half * 4 * M;
+}
 constexpr int kStepPeek = 1 << 8;         // internal flag: recompute outputs, leave the state untouched
 constexpr double kGasConstant = 8.314441; // src/LBM/util/constant.py:17
 
@@ -113,6 +123,7 @@ struct StepParams {
   C* u_out;
   C* T_out;
   float* uprev;
+  C* inlet;        // flow-rate inlet state (LBM_FIELD_INLET), null without one
   int* err;        // set to 1 when a bounded wait gives up
   // cell lists (step_list<>): entry cell index / neighbour-solid bits, the entry
   // of each cell (-1: none) and the list header (kLh* slots)
@@ -922,6 +933,45 @@ __global__ void __launch_bounds__(256) flip_cells(const __grid_constant__ StepPa
   if (diag) block_reduce_store(acc, p.partials + (size_t)(p.block_offset + blockIdx.x), (size_t)p.partial_rows);
 }
 
+// ------------------------------------------------------ flow-rate inlet
+// Coefficient F/flow0 of this step (src/LBM/LBM2D/_boundary.py:324-329): flow0 sums
+// rho*u_x over the side cells as the previous step left them (half p.par).  One block;
+// FP64 sum in a fixed order.
+template <class S>
+__global__ void __launch_bounds__(1024) inlet_flow_coef(const __grid_constant__ StepParams<S> p) {
+  using C = typename Store<S>::C;
+  const size_t M = (size_t)p.ny * p.nz;
+  const C* m = inlet_half(p.inlet, p.par, M);
+  double acc = 0.0;
+  for (size_t j = threadIdx.x; j < M; j += blockDim.x) acc += (double)m[j];
+  for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+  __shared__ double part[32];
+  if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    acc = threadIdx.x < (blockDim.x >> 5) ? part[threadIdx.x] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_down_sync(0xffffffffu, acc, o);
+    if (threadIdx.x == 0) p.inlet[0] = (C)(p.sides[0].v[0] / acc);
+  }
+}
+
+// Controller start (src/LBM/LBM2D/_initialize.py:67-73): both reads of the first
+// step see the uniform inlet velocity v0 = F/ny/nz, with the initial density of the
+// side cells.  Half 0 (the first step's parity).  One block.
+template <class C>
+__global__ void __launch_bounds__(1024) inlet_seed(C* inlet, const float* rho, int nx, int ny, int nz, double F) {
+  const size_t M = (size_t)ny * nz;
+  const C v0 = (C)(F / ny / nz);
+  C* h = inlet_half(inlet, 0, M);
+  for (size_t j = threadIdx.x; j < M; j += blockDim.x) {
+    h[j] = (C)rho[(size_t)nx * j] * v0;
+    h[M + j] = v0;
+    h[2 * M + j] = (C)0;
+    h[3 * M + j] = (C)0;
+  }
+  if (threadIdx.x == 0) inlet[0] = (C)1;
+}
+
 // --------------------------------------------------------- boundary kernel
 template <class L, class S>
 struct MState {
@@ -984,6 +1034,15 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
     // _boundary.py:54-65 (flow), _scalarField.py:83-92 (scalar)
     if (sd.v_type == LBM_BC_FIXEDVALUE) { s.ux = (C)sd.v[0]; s.uy = (C)sd.v[1]; s.uz = (C)sd.v[2]; }
     else if (sd.v_type == LBM_BC_ZEROGRADIENT) { s.ux = in.ux; s.uy = in.uy; s.uz = in.uz; }
+    else if (sd.v_type == LBM_BC_FLOWRATE) {
+      // side 0 only: (a*F/flow0 + 1 - a) * u(1,y,z) of the previous step, a = 0.01
+      // (src/LBM/LBM2D/_boundary.py:330-332)
+      const size_t M = (size_t)p.ny * p.nz, j = (size_t)y + (size_t)p.ny * z;
+      const C* w = inlet_half(p.inlet, p.par, M) + M;
+      const C a = (C)0.01;
+      const C gain = a * p.inlet[0] + (C)1 - a;
+      s.ux = gain * w[j]; s.uy = gain * w[M + j]; s.uz = gain * w[2 * M + j];
+    }
     if (sd.rho_type == LBM_BC_FIXEDVALUE) s.rho = (C)sd.rho;
     else if (sd.rho_type == LBM_BC_ZEROGRADIENT) s.rho = in.rho;
     const C usb = s.ux * s.ux + s.uy * s.uy + s.uz * s.uz;
@@ -1044,6 +1103,24 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   if (!valid) return;
   const int c = x + p.nx * (y + p.ny * z);
   MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z, THERMAL);
+  if (p.inlet && x <= 1 && !(p.flags & kStepPeek)) {
+    // flow-rate inlet: record what the next step's controller reads (final values)
+    const size_t M = (size_t)p.ny * p.nz, j = (size_t)y + (size_t)p.ny * z;
+    C* o = inlet_half(p.inlet, p.par ^ 1, M);
+    if (x == 0) {
+      o[j] = s.rho * s.ux;
+      // cell (1,y,z) behind it: its post-stream state when no side owns it
+      const bool owned = ((p.active & 2) && p.nx == 2) || ((p.active & 4) && y == 0) ||
+                         ((p.active & 8) && y == p.ny - 1) || ((p.active & 16) && z == 0) ||
+                         ((p.active & 32) && z == p.nz - 1);
+      if (!owned) {
+        const MState<L, S> b = bc_state<L, S, THERMAL, PYRO, -1>(p, 1, y, z, false);
+        o[M + j] = b.ux; o[2 * M + j] = b.uy; o[3 * M + j] = b.uz;
+      }
+    } else {
+      o[M + j] = s.ux; o[2 * M + j] = s.uy; o[3 * M + j] = s.uz;
+    }
+  }
   if (diag) {
     diag_flow(p, acc, c, s.rho, s.ux, s.uy, s.uz);
     if (THERMAL) diag_thermal(p, acc, c, s.T);
@@ -1099,7 +1176,14 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
   // neighbours' bit `solid_bit` keeps its value while the bytes are normalised
   const uint32_t nbits = K::neighbour_bits(p, nb, solid_bit);
   const C rho = (C)rho_in[c];
-  const C ux = (C)u_in[c], uy = (C)u_in[p.N + c], uz = (C)u_in[2 * p.N + c];
+  C ux = (C)u_in[c], uy = (C)u_in[p.N + c], uz = (C)u_in[2 * p.N + c];
+  if (p.inlet && x <= 1) {
+    // flow-rate inlet: the columns x = 0 and 1 start at the inlet velocity v0 = F/ny/nz,
+    // which the reference writes into their macro velocity for its first collision
+    // (src/LBM/LBM2D/_initialize.py:69-74); without it the first profile is zero
+    ux = (C)(p.sides[0].v[0] / p.ny / p.nz);
+    uy = uz = (C)0;
+  }
   if (!solid) {
     C F[Q];
     K::feq_all(p, rho, ux, uy, uz, F);

@@ -263,13 +263,15 @@ class Lattice:
                 out[name] = self._view(fid, cd).cpu().numpy()
         if N.LBM_FIELD_UPREV in self.buf:
             out["uprev"] = self._view(N.LBM_FIELD_UPREV, torch.float32).cpu().numpy()
+        if N.LBM_FIELD_INLET in self.buf:
+            out["inlet"] = self._view(N.LBM_FIELD_INLET, cd).cpu().numpy()
         return out
 
     def save_checkpoint(self, path) -> str:
         """Write the state to ``path`` (numpy .npz, uncompressed): the halves of the flow and
         temperature populations and the gas-release plane that the next step reads, the
-        mask, reactive fraction, residual reference and macro planes, in their device
-        precision, with the step count and the configuration.  ``Lattice.load_checkpoint``
+        mask, reactive fraction, residual reference, macro planes and flow-rate inlet
+        state, in their device precision, with the step count and the configuration.  ``Lattice.load_checkpoint``
         continues from it with the same fields, bit for bit.  (The reference has no
         restart; its export_snapshot is a reserved no-op, src/LBM/LBM2D/_io.py:589-598.)"""
         if not self.nsteps and self._init_fields is None:
@@ -319,6 +321,8 @@ class Lattice:
                     put(self._view(fid, cd), name)
             if N.LBM_FIELD_UPREV in self.buf:
                 put(self._view(N.LBM_FIELD_UPREV, torch.float32), "uprev")
+            if N.LBM_FIELD_INLET in self.buf:
+                put(self._view(N.LBM_FIELD_INLET, cd), "inlet")
             N.check(self.lib.lbm_resume(self._h, int(step), self._s()))
         self._init_fields = {}
 

@@ -24,7 +24,7 @@ from typing import Callable, Optional
 
 import numpy as np
 
-from .config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
+from .config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
 from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, SOURCE_TERM, VISCOSITY_MODEL
 from .vtk import PVDWriter, write_vts
 
@@ -278,8 +278,6 @@ class _SolverBase:
             self.bc_v[i], self.bc_rho[i] = BC.zeroGradient, BC.zeroGradient
         if bc == BC_FLOW.wall:
             self.v_BC[i] = (0.0, 0.0, 0.0)
-        if bc == BC_FLOW.inlet_flow:
-            raise NotImplementedError("flow-rate inlets (updateBC_kernel) are not on the CUDA path")
 
     def set_BCs(self, bcs):
         for i, b in enumerate(bcs):
@@ -302,6 +300,11 @@ class _SolverBase:
 
     def set_flow_BC_value(self, i, f):
         self.flow_BC[i] = float(f)
+        self._push_sides()
+
+    def set_flow_BCs_value(self, fs):
+        for i, f in enumerate(fs):
+            self.set_flow_BC_value(i, f)
 
     def set_TF_BC(self, i, bc):
         self.TF.set_BC(i, bc)
@@ -401,7 +404,18 @@ class _SolverBase:
                 active = self.ref_quirk_nee_on_periodic or (vt, rt, Tt) != (PERIODIC, PERIODIC, PERIODIC)
             else:
                 raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path (NEE only)")
-            sides[i] = SideBC(active, vt, rt, Tt, self.v_BC[i], self.rho_BC[i], self.TF.s_BC[i])
+            v = self.v_BC[i]
+            if self.bc[i] == BC_FLOW.inlet_flow and vt == FIXED_VALUE:
+                # the reference sets an inlet profile for side 0 only
+                # (src/LBM/LBM2D/_initialize.py:67-73, LBM3D/_initialize.py:78-85); the
+                # 2D solver steers it each step (LBM2D/_boundary.py:324-333), the 3D one
+                # keeps v0 = F/ny/nz (LBM3D/_boundary.py:12-14 only runs user callbacks)
+                v = (0.0, 0.0, 0.0)
+                if i == 0 and self.DIM == 2:
+                    vt, v = FLOW_RATE, (self.flow_BC[0], 0.0, 0.0)
+                elif i == 0:
+                    v = (self.flow_BC[0] / self.ny / self.nz, 0.0, 0.0)
+            sides[i] = SideBC(active, vt, rt, Tt, v, self.rho_BC[i], self.TF.s_BC[i])
         return sides
 
     def _config(self) -> LatticeConfig:

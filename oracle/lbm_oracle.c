@@ -54,7 +54,8 @@ static const int E19[19][3] = {{0,0,0},{1,0,0},{-1,0,0},{0,1,0},{0,-1,0},{0,0,1}
 static const int OPP19[19] = {0,2,1,4,3,6,5,10,9,8,7,14,13,12,11,18,17,16,15};
 
 /* ------------------------------------------------------------------ config */
-enum { ORC_BC_PERIODIC = 0, ORC_BC_ZEROGRAD = 1, ORC_BC_FIXED = 2 };
+enum { ORC_BC_PERIODIC = 0, ORC_BC_ZEROGRAD = 1, ORC_BC_FIXED = 2,
+       ORC_BC_FLOWRATE = 3 /* velocity of side 0 only: BC_FLOW.inlet_flow, v[0] = flow rate */ };
 
 typedef struct orc_side {
     int active;      /* 1: NEE applied on this side (reference BC_MODEL.NEE) */
@@ -105,6 +106,10 @@ typedef struct orc {
     REAL *f, *F, *g, *G;
     REAL *rho, *u, *T, *dS, *alpha, *rel;
     uint8_t *mask, *mask_next;
+    /* flow-rate inlet on side 0, per side cell j = y + ny*z: what the reference's
+     * updateBC_kernel reads (rho*u_x at x = 0, u at x = 1, 3 per cell) and the
+     * inlet velocity profile it writes (v_bc_profile[0], 3 per cell) */
+    REAL *inl_m, *inl_w, *inl_prof;
 } orc;
 
 /* ------------------------------------------------------------ MRT basis */
@@ -281,13 +286,18 @@ orc* orc_create(const orc_cfg* cfg) {
     o->rel = (REAL*)calloc(N, sizeof(REAL));
     o->mask = (uint8_t*)calloc(N, 1);
     o->mask_next = (uint8_t*)calloc(N, 1);
+    long M = (long)o->c.ny * o->c.nz;
+    o->inl_m = (REAL*)calloc(M, sizeof(REAL));
+    o->inl_w = (REAL*)calloc(3*M, sizeof(REAL));
+    o->inl_prof = (REAL*)calloc(3*M, sizeof(REAL));
     return o;
 }
 
 void orc_destroy(orc* o) {
     if (!o) return;
     free(o->f); free(o->F); free(o->g); free(o->G); free(o->rho); free(o->u); free(o->T);
-    free(o->dS); free(o->alpha); free(o->rel); free(o->mask); free(o->mask_next); free(o);
+    free(o->dS); free(o->alpha); free(o->rel); free(o->mask); free(o->mask_next);
+    free(o->inl_m); free(o->inl_w); free(o->inl_prof); free(o);
 }
 
 int orc_Q(const orc* o) { return o->Q; }
@@ -299,10 +309,13 @@ double orc_M(const orc* o, int r, int k) { return o->M[r][k]; }
 void orc_init(orc* o, const double* rho, const double* u, const double* T,
               const uint8_t* mask, const double* alpha) {
     long N = o->N;
+    int fr = o->c.side[0].active && o->c.side[0].v_type == ORC_BC_FLOWRATE;
+    REAL v0 = fr ? (REAL)(o->c.side[0].v[0] / o->c.ny / o->c.nz) : 0;
     for (long c = 0; c < N; ++c) {
         o->mask[c] = mask[c] & (ORC_SOLID | ORC_REACTIVE);
         o->rho[c] = (REAL)rho[c];
         for (int d = 0; d < 3; ++d) o->u[c*3 + d] = (REAL)u[d*N + c];
+        if (fr && c % o->c.nx <= 1) { o->u[c*3] = v0; o->u[c*3+1] = 0; o->u[c*3+2] = 0; }
         o->T[c] = T ? (REAL)T[c] : 0;
         o->alpha[c] = alpha ? (REAL)alpha[c] : 0;
         o->dS[c] = 0;
@@ -317,6 +330,17 @@ void orc_init(orc* o, const double* rho, const double* u, const double* T,
             REAL v = is_solid(o->mask, c) ? o->wt[k]*o->T[c] : geq_fluid(o, k, o->T[c], &o->u[c*3]);
             o->g[c*o->QT + k] = v;
             o->G[c*o->QT + k] = v;
+        }
+    }
+    /* init_boundary (src/LBM/LBM2D/_initialize.py:67-74): the columns x = 0 and 1 start
+     * at the inlet velocity v0 = F/ny/nz and the first controller update reads it.  The
+     * reference writes v0 into the macro velocity only (its first collision reads it)
+     * and keeps the populations of the initial fields; here the populations start at
+     * equilibrium with v0 too. */
+    if (fr) {
+        for (long j = 0; j < (long)o->c.ny * o->c.nz; ++j) {
+            o->inl_m[j] = o->rho[(long)o->c.nx * j] * v0;
+            o->inl_w[3*j] = v0; o->inl_w[3*j+1] = 0; o->inl_w[3*j+2] = 0;
         }
     }
 }
@@ -446,11 +470,12 @@ static void macro(orc* o) {
 /* Non-equilibrium extrapolation on one boundary cell b with inner neighbour i.
  * Flow: src/LBM/LBM2D/_boundary.py:54-101 (3D: LBM3D/_boundary.py:71-142).
  * Scalar: src/LBM/LBM2D/_scalarField.py:83-122. */
-static void nee_cell(orc* o, const orc_side* s, long b, long i) {
+static void nee_cell(orc* o, const orc_side* s, long b, long i, const REAL* prof) {
     int Q = o->Q, QT = o->QT;
     REAL* ub = &o->u[b*3];
     const REAL* ui = &o->u[i*3];
     if (s->v_type == ORC_BC_FIXED) for (int d = 0; d < 3; ++d) ub[d] = (REAL)s->v[d];
+    else if (s->v_type == ORC_BC_FLOWRATE) for (int d = 0; d < 3; ++d) ub[d] = prof[d];
     else if (s->v_type == ORC_BC_ZEROGRAD) for (int d = 0; d < 3; ++d) ub[d] = ui[d];
     if (s->rho_type == ORC_BC_FIXED) o->rho[b] = (REAL)s->rho;
     else if (s->rho_type == ORC_BC_ZEROGRAD) o->rho[b] = o->rho[i];
@@ -472,26 +497,52 @@ static void nee(orc* o) {
     int nx = o->c.nx, ny = o->c.ny, nz = o->c.nz;
     const orc_side* S = o->c.side;
     for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) {
-        if (S[0].active) nee_cell(o, &S[0], cidx(o, 0, y, z), cidx(o, 1, y, z));
-        if (S[1].active) nee_cell(o, &S[1], cidx(o, nx-1, y, z), cidx(o, nx-2, y, z));
+        if (S[0].active) nee_cell(o, &S[0], cidx(o, 0, y, z), cidx(o, 1, y, z), &o->inl_prof[3*(y + (long)ny*z)]);
+        if (S[1].active) nee_cell(o, &S[1], cidx(o, nx-1, y, z), cidx(o, nx-2, y, z), NULL);
     }
     for (int z = 0; z < nz; ++z) for (int x = 0; x < nx; ++x) {
-        if (S[2].active) nee_cell(o, &S[2], cidx(o, x, 0, z), cidx(o, x, 1, z));
-        if (S[3].active) nee_cell(o, &S[3], cidx(o, x, ny-1, z), cidx(o, x, ny-2, z));
+        if (S[2].active) nee_cell(o, &S[2], cidx(o, x, 0, z), cidx(o, x, 1, z), NULL);
+        if (S[3].active) nee_cell(o, &S[3], cidx(o, x, ny-1, z), cidx(o, x, ny-2, z), NULL);
     }
     if (o->c.dim == 3)
         for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
-            if (S[4].active) nee_cell(o, &S[4], cidx(o, x, y, 0), cidx(o, x, y, 1));
-            if (S[5].active) nee_cell(o, &S[5], cidx(o, x, y, nz-1), cidx(o, x, y, nz-2));
+            if (S[4].active) nee_cell(o, &S[4], cidx(o, x, y, 0), cidx(o, x, y, 1), NULL);
+            if (S[5].active) nee_cell(o, &S[5], cidx(o, x, y, nz-1), cidx(o, x, y, nz-2), NULL);
         }
 }
 
-/* step: src/LBM/LBM2D/_evolution.py:12-25 */
+/* Flow-rate inlet, updateBC_kernel (src/LBM/LBM2D/_boundary.py:324-333), run before
+ * the step: flow0 = sum of rho*u_x over the side-0 cells, coef = F/flow0, and the
+ * profile of side cell j is (a*coef + 1 - a) * u(1,j), a = 0.01, from the fields
+ * the previous step left (inl_m, inl_w; flow0 summed in double). */
+static void flowrate_update(orc* o) {
+    long M = (long)o->c.ny * o->c.nz;
+    double flow0 = 0;
+    for (long j = 0; j < M; ++j) flow0 += (double)o->inl_m[j];
+    REAL coef = (REAL)(o->c.side[0].v[0] / flow0);
+    REAL a = (REAL)0.01;
+    REAL gain = a*coef + (REAL)1 - a;
+    for (long j = 0; j < 3*M; ++j) o->inl_prof[j] = gain*o->inl_w[j];
+}
+
+/* What the next update reads: rho*u_x at x = 0 and u at x = 1 after macro and NEE. */
+static void flowrate_record(orc* o) {
+    for (int z = 0; z < o->c.nz; ++z) for (int y = 0; y < o->c.ny; ++y) {
+        long j = y + (long)o->c.ny*z, b = cidx(o, 0, y, z), i = cidx(o, 1, y, z);
+        o->inl_m[j] = o->rho[b]*o->u[b*3];
+        for (int d = 0; d < 3; ++d) o->inl_w[3*j + d] = o->u[i*3 + d];
+    }
+}
+
+/* step: src/LBM/LBM2D/_evolution.py:12-25 (updateBC, then step_kernel) */
 void orc_step(orc* o, int n) {
+    int fr = o->c.side[0].active && o->c.side[0].v_type == ORC_BC_FLOWRATE;
     for (int i = 0; i < n; ++i) {
+        if (fr) flowrate_update(o);
         collide_stream(o);
         macro(o);
         nee(o);
+        if (fr) flowrate_record(o);
     }
 }
 

@@ -6,7 +6,7 @@ import pytest
 import yaml
 
 from lbm_porouschem_b200.app import _centres, build_case, voxelise
-from lbm_porouschem_b200.config import FIXED_VALUE, ZERO_GRADIENT
+from lbm_porouschem_b200.config import FIXED_VALUE, FLOW_RATE, ZERO_GRADIENT
 
 CASE2D = """
 basic:
@@ -98,6 +98,16 @@ def test_build_case_from_yaml():
     assert sd[1].rho_type == FIXED_VALUE and sd[1].T_type == ZERO_GRADIENT
     assert sd[2].active and sd[3].active
     assert np.all(lb.TF.S.to_numpy() == 0.0)                         # 300 K normalised
+
+
+def test_flowrate_inlet_from_yaml():
+    """`inlet_flowrate` (src/LBM/app.py:358-364): the 2D left side becomes the steered
+    flow-rate inlet with its target flux; rho is extrapolated."""
+    cfg = yaml.safe_load(CASE2D)
+    cfg["boundaryCondition"]["left"]["flow"] = {"type": "inlet_flowrate", "flowrate": 0.05}
+    sd = build_case(cfg, _log())._config().sides
+    assert sd[0].active and sd[0].v_type == FLOW_RATE and sd[0].v == (0.05, 0.0, 0.0)
+    assert sd[0].rho_type == ZERO_GRADIENT and sd[0].T_type == FIXED_VALUE
 
 
 def test_unsupported_options_stop_the_run():

@@ -181,3 +181,59 @@ def test_two_field_interface_is_adiabatic(oracle_mod, dim):
     assert abs(tot["two_field"][0] - solid.sum()) < 1e-9
     assert abs(tot["two_field"][1]) < 1e-9
     assert tot["conjugate"][1] > 0.1 * solid.sum()
+
+
+def _flowrate_channel(dim, F, coll="bgk"):
+    sides = [SideBC() for _ in range(6)]
+    sides[0] = SideBC.inlet_flowrate(F)
+    sides[1] = SideBC.outlet(1.0)
+    sides[2], sides[3] = SideBC.wall(), SideBC.wall()
+    return LatticeConfig(dim=dim, nx=24, ny=10, nz=4 if dim == 3 else 1, collision=coll, nu=0.1, sides=sides)
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_flowrate_inlet_follows_the_reference_controller(oracle_mod, dim):
+    """The flow-rate inlet law of src/LBM/LBM2D/_boundary.py:324-333, restated here in
+    numpy from the fields of the previous step: flow0 = sum rho*u_x at x = 0,
+    coef = F/flow0, u(0,j) = (0.01*coef + 1 - 0.01) * u(1,j) on every side cell that no
+    other side overrides; the columns x = 0, 1 start at v0 = F/ny/nz
+    (_initialize.py:67-74)."""
+    F = 0.12
+    cfg = _flowrate_channel(dim, F)
+    o = oracle_mod.Oracle(cfg, real="f64")
+    o.init(np.zeros(cfg.shape[:dim], dtype=bool), rho=1.0, u=(0.0, 0.0, 0.0))
+    f = o.fields()
+    v0 = F / cfg.ny / cfg.nz
+    assert np.all(f["u"][0][:2] == v0) and np.all(f["u"][1][:2] == 0)
+    inner = slice(1, cfg.ny - 1)                       # y = 0, ny-1 belong to the walls
+    for _ in range(40):
+        rho0, ux0 = f["rho"][0].reshape(-1), f["u"][0][0].reshape(-1)
+        flow0 = 0.0
+        for a, b in zip(rho0, ux0):                   # the oracle's summation order (j = y + ny*z)
+            flow0 += a * b
+        gain = 0.01 * (F / flow0) + 1 - 0.01
+        want = gain * f["u"][:, 1]
+        o.step(1)
+        f = o.fields()
+        assert np.allclose(f["u"][:, 0][:, inner], want[:, inner], rtol=1e-13, atol=1e-17)
+        assert np.all(f["u"][:, 0][:, [0, -1]] == 0)   # wall corners
+
+
+def test_flowrate_inlet_steady_state(oracle_mod):
+    """After the flow develops the controller holds a steady inlet flux: the law's fixed
+    point u(0,j) = g u(1,j), with one gain g = 0.01 F/flux + 0.99 over the side.  The
+    law is proportional, so the steady flux is F only where u(0) = u(1); on this short
+    walled channel it settles near 0.42 F."""
+    F = 0.12
+    cfg = _flowrate_channel(2, F)
+    o = oracle_mod.Oracle(cfg, real="f64")
+    o.init(np.zeros(cfg.shape[:2], dtype=bool), rho=1.0, u=(0.0, 0.0, 0.0))
+    o.step(3000)
+    a = o.fields()
+    o.step(200)
+    b = o.fields()
+    flux = [float((f["rho"][0, :, 0] * f["u"][0, 0, :, 0]).sum()) for f in (a, b)]
+    assert abs(flux[1] - flux[0]) < 1e-9 * F
+    g = 0.01 * F / flux[1] + 0.99
+    assert np.allclose(b["u"][0, 0, 1:-1, 0], g * b["u"][0, 1, 1:-1, 0], rtol=1e-10)
+    assert 0 < flux[1] < F

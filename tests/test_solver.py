@@ -4,7 +4,7 @@ import numpy as np
 import pytest
 
 from lbm_porouschem_b200 import LatticeConfig, SideBC
-from lbm_porouschem_b200.config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT
+from lbm_porouschem_b200.config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT
 from lbm_porouschem_b200.flag import BC, BC_FLOW, BC_MODEL
 from lbm_porouschem_b200.solver import LBM2DSolver, LBM3DSolver
 
@@ -95,12 +95,31 @@ def test_unsupported_features_raise():
         s.set_viscosity_sutherland(1.0, 1.0)
     with pytest.raises(NotImplementedError):
         s.load_cantera("gri30.yaml")
-    with pytest.raises(NotImplementedError):
-        s.set_BC(0, BC_FLOW.inlet_flow)
     s.boundary_condition_model = BC_MODEL.NEBB
     s.set_BC(0, BC_FLOW.outlet)
     with pytest.raises(NotImplementedError):
         s._config()
+
+
+def test_flowrate_inlet_mapping():
+    """BC_FLOW.inlet_flow: side 0 steered each step in 2D (LBM_BC_FLOWRATE, target in
+    v[0]), the uniform v0 = F/ny/nz in 3D, zero velocity on any other side (the
+    reference sets an inlet profile for side 0 only)."""
+    s = LBM2DSolver(X=16, Y=8, Z=0)
+    s.set_BC(0, BC_FLOW.inlet_flow)
+    s.set_flow_BC_value(0, 0.4)
+    s.set_BC(1, BC_FLOW.outlet)
+    s.set_rho_BC_value(1, 1.0)
+    sd = s._config().sides
+    assert sd[0].active and sd[0].v_type == FLOW_RATE and sd[0].rho_type == ZERO_GRADIENT
+    assert sd[0].v == (0.4, 0.0, 0.0)
+    s3 = LBM3DSolver(X=8, Y=4, Z=5)
+    for i in (0, 1):
+        s3.set_BC(i, BC_FLOW.inlet_flow)
+        s3.set_flow_BC_value(i, 0.4)
+    sd = s3._config().sides
+    assert sd[0].v_type == FIXED_VALUE and sd[0].v == pytest.approx((0.4 / 4 / 5, 0.0, 0.0))
+    assert sd[1].v_type == FIXED_VALUE and sd[1].v == (0.0, 0.0, 0.0)
 
 
 def test_init_field_forms(tmp_path):
