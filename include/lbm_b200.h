@@ -82,7 +82,11 @@ extern "C" {
 /* One domain side: 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+  (reference side order,
  * src/LBM/LBM3D/_core.py:72).  active = 1 applies non-equilibrium
  * extrapolation (BC_MODEL.NEE, src/LBM/LBM2D/_boundary.py:17-101) on that
- * side; 0 leaves it periodic. */
+ * side; 2 the equilibrium scheme (BC_MODEL.ES, src/LBM/LBM2D/_boundary.py:229-315,
+ * LBM3D/_boundary.py:145-274: the side cell's flow populations are feq(rho_b, u_b)
+ * alone, its temperature is extrapolated as under NEE); 0 leaves it periodic. */
+#define LBM_SIDE_NEE 1
+#define LBM_SIDE_ES 2
 typedef struct lbm_side_desc {
   int32_t active;
   int32_t v_type;   /* LBM_BC_*, velocity  (set_BC mapping src/LBM/LBM2D/_io.py:385-402) */

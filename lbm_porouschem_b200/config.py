@@ -26,7 +26,9 @@ GAS_CONSTANT = 8.314441  # src/LBM/util/constant.py:17
 
 @dataclass
 class SideBC:
-    """One domain side.  ``active`` False keeps the side periodic."""
+    """One domain side.  ``active`` False keeps the side periodic; ``model`` is the
+    boundary scheme of an active side: "nee" (non-equilibrium extrapolation) or "es"
+    (equilibrium populations of the side's state), the reference's BC_MODEL."""
     active: bool = False
     v_type: int = PERIODIC
     rho_type: int = PERIODIC
@@ -34,6 +36,15 @@ class SideBC:
     v: tuple = (0.0, 0.0, 0.0)
     rho: float = 1.0
     T: float = 0.0
+    model: str = "nee"
+
+    def code(self) -> int:
+        """lbm_side_desc.active: 0 periodic, 1 NEE, 2 ES."""
+        if not self.active:
+            return 0
+        if self.model not in ("nee", "es"):
+            raise ValueError(f"side model {self.model!r}: 'nee' or 'es'")
+        return 2 if self.model == "es" else 1
 
     @staticmethod
     def inlet(v, T_type=PERIODIC, T=0.0) -> "SideBC":
@@ -168,7 +179,7 @@ class LatticeConfig:
 
 def fill_sides(arr, sides) -> None:
     for i, s in enumerate(sides):
-        arr[i].active = int(bool(s.active))
+        arr[i].active = s.code()
         arr[i].v_type, arr[i].rho_type, arr[i].T_type = int(s.v_type), int(s.rho_type), int(s.T_type)
         for k in range(3):
             arr[i].v[k] = float(s.v[k])

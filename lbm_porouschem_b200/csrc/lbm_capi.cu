@@ -46,6 +46,7 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");
   for (int s = 0; s < 6; ++s) {
     const lbm_side_desc& sd = d->side[s];
+    if (sd.active < 0 || sd.active > LBM_SIDE_ES) return fail(LBM_ERR_ARG, "side active must be 0, 1 (NEE) or 2 (ES)");
     if (!sd.active) continue;
     if (d->dim == 2 && s >= 4) return fail(LBM_ERR_ARG, "z sides cannot be active in 2D");
     const int types[3] = {sd.v_type, sd.rho_type, sd.T_type};

@@ -1047,15 +1047,27 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
     else if (sd.rho_type == LBM_BC_ZEROGRADIENT) s.rho = in.rho;
     const C usb = s.ux * s.ux + s.uy * s.uy + s.uz * s.uz;
     const C usi = in.ux * in.ux + in.uy * in.uy + in.uz * in.uz;
-    s.F[0] = K::feq_rest(p, s.rho, usb) + (in.F[0] - K::feq_rest(p, in.rho, usi));
-    static_for<num_pairs<L>()>([&](auto pp) {
-      constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
-      C evb, odb, evi, odi;
-      K::template feq_pair<k>(p, s.rho, s.ux, s.uy, s.uz, usb, evb, odb);
-      K::template feq_pair<k>(p, in.rho, in.ux, in.uy, in.uz, usi, evi, odi);
-      s.F[k] = (evb + odb) + (in.F[k] - (evi + odi));
-      s.F[o] = (evb - odb) + (in.F[o] - (evi - odi));
-    });
+    if (sd.active == LBM_SIDE_ES) {
+      // equilibrium scheme (src/LBM/LBM2D/_boundary.py:269-315): feq of the side's state
+      s.F[0] = K::feq_rest(p, s.rho, usb);
+      static_for<num_pairs<L>()>([&](auto pp) {
+        constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+        C evb, odb;
+        K::template feq_pair<k>(p, s.rho, s.ux, s.uy, s.uz, usb, evb, odb);
+        s.F[k] = evb + odb;
+        s.F[o] = evb - odb;
+      });
+    } else {
+      s.F[0] = K::feq_rest(p, s.rho, usb) + (in.F[0] - K::feq_rest(p, in.rho, usi));
+      static_for<num_pairs<L>()>([&](auto pp) {
+        constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
+        C evb, odb, evi, odi;
+        K::template feq_pair<k>(p, s.rho, s.ux, s.uy, s.uz, usb, evb, odb);
+        K::template feq_pair<k>(p, in.rho, in.ux, in.uy, in.uz, usi, evi, odi);
+        s.F[k] = (evb + odb) + (in.F[k] - (evi + odi));
+        s.F[o] = (evb - odb) + (in.F[o] - (evi - odi));
+      });
+    }
     if (THERMAL && needT) {
       if (sd.T_type == LBM_BC_FIXEDVALUE) s.T = (C)sd.T;
       else if (sd.T_type == LBM_BC_ZEROGRADIENT) s.T = in.T;

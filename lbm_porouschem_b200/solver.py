@@ -400,10 +400,10 @@ class _SolverBase:
                 Tt = PERIODIC
             if self.boundary_condition_model == BC_MODEL.NONE:
                 active = False
-            elif self.boundary_condition_model == BC_MODEL.NEE:
+            elif self.boundary_condition_model in (BC_MODEL.NEE, BC_MODEL.ES):
                 active = self.ref_quirk_nee_on_periodic or (vt, rt, Tt) != (PERIODIC, PERIODIC, PERIODIC)
             else:
-                raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path (NEE only)")
+                raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path (NEE and ES only)")
             v = self.v_BC[i]
             if self.bc[i] == BC_FLOW.inlet_flow and vt == FIXED_VALUE:
                 # the reference sets an inlet profile for side 0 only
@@ -415,7 +415,8 @@ class _SolverBase:
                     vt, v = FLOW_RATE, (self.flow_BC[0], 0.0, 0.0)
                 elif i == 0:
                     v = (self.flow_BC[0] / self.ny / self.nz, 0.0, 0.0)
-            sides[i] = SideBC(active, vt, rt, Tt, v, self.rho_BC[i], self.TF.s_BC[i])
+            model = "es" if self.boundary_condition_model == BC_MODEL.ES else "nee"
+            sides[i] = SideBC(active, vt, rt, Tt, v, self.rho_BC[i], self.TF.s_BC[i], model)
         return sides
 
     def _config(self) -> LatticeConfig:

@@ -58,7 +58,7 @@ enum { ORC_BC_PERIODIC = 0, ORC_BC_ZEROGRAD = 1, ORC_BC_FIXED = 2,
        ORC_BC_FLOWRATE = 3 /* velocity of side 0 only: BC_FLOW.inlet_flow, v[0] = flow rate */ };
 
 typedef struct orc_side {
-    int active;      /* 1: NEE applied on this side (reference BC_MODEL.NEE) */
+    int active;      /* 1: NEE on this side (reference BC_MODEL.NEE), 2: ES (BC_MODEL.ES) */
     int v_type;      /* ORC_BC_* for velocity  (LBM2D/_io.py:385-402 set_BC mapping) */
     int rho_type;    /* ORC_BC_* for density */
     int T_type;      /* ORC_BC_* for the temperature distribution */
@@ -480,7 +480,9 @@ static void nee_cell(orc* o, const orc_side* s, long b, long i, const REAL* prof
     if (s->rho_type == ORC_BC_FIXED) o->rho[b] = (REAL)s->rho;
     else if (s->rho_type == ORC_BC_ZEROGRAD) o->rho[b] = o->rho[i];
     for (int k = 0; k < Q; ++k)
-        o->f[b*Q + k] = feq(o, k, o->rho[b], ub) + (o->f[i*Q + k] - feq(o, k, o->rho[i], ui));
+        o->f[b*Q + k] = s->active == 2   /* ES, src/LBM/LBM2D/_boundary.py:269-315 */
+            ? feq(o, k, o->rho[b], ub)
+            : feq(o, k, o->rho[b], ub) + (o->f[i*Q + k] - feq(o, k, o->rho[i], ui));
     if (o->c.thermal >= 1) {
         if (s->T_type == ORC_BC_FIXED) o->T[b] = (REAL)s->T;
         else if (s->T_type == ORC_BC_ZEROGRAD) o->T[b] = o->T[i];

@@ -115,7 +115,7 @@ class Oracle:
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):
-            c.side[i].active = int(bool(s.active))
+            c.side[i].active = s.code()
             c.side[i].v_type, c.side[i].rho_type, c.side[i].T_type = int(s.v_type), int(s.rho_type), int(s.T_type)
             for k in range(3):
                 c.side[i].v[k] = float(s.v[k])

@@ -272,11 +272,13 @@ def test_two_field_thermal_fp64(oracle_mod, dim):
     assert np.allclose(g["T"].reshape(shape)[solid], 0.5, atol=1e-12)
 
 
+@pytest.mark.parametrize("model", ["nee", "es"])
 @pytest.mark.parametrize("dim", [2, 3])
-def test_nee_every_side_mixed_types_fp64(oracle_mod, dim):
+def test_nee_every_side_mixed_types_fp64(oracle_mod, dim, model):
     """Every side active, with v, rho and T each fixed, extrapolated or kept (PERIODIC
     type: the side cell's own post-stream value) on some side; corner cells take two or
-    three NEE passes.  FP64 kernels vs the FP64 oracle, conjugate heat with pyrolysis."""
+    three passes.  NEE and the equilibrium scheme (ES).  FP64 kernels vs the FP64
+    oracle, conjugate heat with pyrolysis."""
     from lbm_porouschem_b200.config import FIXED_VALUE, PERIODIC, ZERO_GRADIENT, SideBC
     rng = np.random.default_rng(31 + dim)
     shape = (36, 28) if dim == 2 else (20, 17, 14)
@@ -290,6 +292,8 @@ def test_nee_every_side_mixed_types_fp64(oracle_mod, dim):
              SideBC(True, PERIODIC, FIXED_VALUE, ZERO_GRADIENT, rho=1.001)]
     sides += ([SideBC.wall(ZERO_GRADIENT), SideBC(True, ZERO_GRADIENT, PERIODIC, FIXED_VALUE, T=0.2)]
               if dim == 3 else [SideBC(), SideBC()])
+    for sd in sides:
+        sd.model = model
     cfg = LatticeConfig(dim=dim, nx=shape[0], ny=shape[1], nz=(1 if dim == 2 else shape[2]), collision="mrt",
                         nu=0.05, thermal="conjugate", pyro=True, pyro_A=1.2e11, heat_norm=0.02, gas_coef=0.05,
                         precision="fp64", sides=sides)

@@ -237,3 +237,38 @@ def test_flowrate_inlet_steady_state(oracle_mod):
     g = 0.01 * F / flux[1] + 0.99
     assert np.allclose(b["u"][0, 0, 1:-1, 0], g * b["u"][0, 1, 1:-1, 0], rtol=1e-10)
     assert 0 < flux[1] < F
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_es_side_cells_hold_equilibrium(oracle_mod, dim):
+    """BC_MODEL.ES (src/LBM/LBM2D/_boundary.py:269-315): after a step every side cell's
+    populations are feq of its own (rho, u), with u the fixed inlet velocity and rho the
+    fixed outlet density; the reference's feq9/feq19 (_evolution.py:213-225)."""
+    sides = [SideBC.inlet((0.03, 0.0, 0.0)), SideBC.outlet(1.01), SideBC.wall(), SideBC.wall(),
+             SideBC(), SideBC()]
+    for sd in sides:
+        sd.model = "es"
+    cfg = LatticeConfig(dim=dim, nx=16, ny=10, nz=4 if dim == 3 else 1, nu=0.1, sides=sides)
+    o = oracle_mod.Oracle(cfg, real="f64")
+    o.init(np.zeros(cfg.shape[:dim], dtype=bool), rho=1.0, u=(0.0, 0.0, 0.0))
+    o.step(25)
+    fl = o.fields()
+    f, _ = o.dist()
+    Q = f.shape[0]
+    f = np.stack([fk.reshape(cfg.shape, order="F") for fk in f])
+    e, w = np.array(_E[dim], dtype=float), _W[dim]
+    for x in (0, cfg.nx - 1):
+        rho = fl["rho"][x]
+        u = fl["u"][:, x]
+        eu = np.tensordot(e, u, axes=(1, 0))
+        uu = (u * u).sum(0)
+        feq = w.reshape((Q,) + (1,) * rho.ndim) * rho * (1 + 3 * eu + 4.5 * eu ** 2 - 1.5 * uu)
+        assert np.allclose(f[:, x][:, 1:-1], feq[:, 1:-1], rtol=0, atol=1e-15)
+    assert np.allclose(fl["u"][0][0][1:-1], 0.03) and np.allclose(fl["rho"][-1][1:-1], 1.01)
+
+
+_E = {2: [(0, 0, 0), (1, 0, 0), (0, 1, 0), (-1, 0, 0), (0, -1, 0), (1, 1, 0), (-1, 1, 0), (-1, -1, 0), (1, -1, 0)],
+      3: [(0, 0, 0), (1, 0, 0), (-1, 0, 0), (0, 1, 0), (0, -1, 0), (0, 0, 1), (0, 0, -1), (1, 1, 0), (-1, 1, 0),
+          (1, -1, 0), (-1, -1, 0), (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1), (0, 1, 1), (0, -1, 1),
+          (0, 1, -1), (0, -1, -1)]}
+_W = {2: np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4), 3: np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)}

@@ -99,6 +99,9 @@ def test_unsupported_features_raise():
     s.set_BC(0, BC_FLOW.outlet)
     with pytest.raises(NotImplementedError):
         s._config()
+    s.boundary_condition_model = BC_MODEL.ES            # the equilibrium scheme is on the path
+    sd = s._config().sides
+    assert sd[0].active and sd[0].model == "es" and sd[0].code() == 2 and sd[2].code() == 0
 
 
 def test_flowrate_inlet_mapping():
