@@ -52,6 +52,8 @@ extern "C" {
 #define LBM_PREC_FP32 0
 #define LBM_PREC_FP16 1 /* FP16 storage of f - w*rho0 and g - wt*T0, FP32 arithmetic */
 #define LBM_PREC_FP64 2
+#define LBM_VISC_CONSTANT 0      /* nu (util/flag.py VISCOSITY_MODEL.CONSTANT) */
+#define LBM_VISC_SUTHERLAND 1    /* per cell from its temperature; needs the temperature field */
 #define LBM_EOS_IDEAL_GAS 0      /* util/flag.py:64-67 FLUID_STATE_EQUATION */
 #define LBM_EOS_INCOMPRESSIBLE 1
 #define LBM_THERMAL_NONE 0
@@ -121,6 +123,11 @@ typedef struct lbm_desc {
   double mrt_s[19];       /* MRT rates per moment; viscous moments use 1/tau(rho) */
   double rho0, T0;        /* FP16 storage shift references */
   lbm_side_desc side[6];
+  int32_t viscosity;      /* LBM_VISC_* */
+  int32_t reserved0;      /* 0 */
+  double suth_A, suth_Ts; /* LBM_VISC_SUTHERLAND: lattice viscosity suth_A T^1.5/(T + suth_Ts) of the
+                             cell's temperature T in kelvin (T_ref + T_scale*T); suth_A = As*dt/dx^2
+                             of set_viscosity_sutherland(As, Ts) (src/LBM/LBM2D/_evolution.py:228-235) */
 } lbm_desc;
 
 /* Diagnostics (FP64 accumulation).  No reference counterpart except umax,

@@ -27,6 +27,7 @@ LBM_PREC_FP32, LBM_PREC_FP16, LBM_PREC_FP64 = 0, 1, 2
 LBM_EOS_IDEAL_GAS, LBM_EOS_INCOMPRESSIBLE = 0, 1
 LBM_THERMAL_NONE, LBM_THERMAL_CONJUGATE, LBM_THERMAL_TWOFIELD = 0, 1, 2
 LBM_BC_PERIODIC, LBM_BC_ZEROGRADIENT, LBM_BC_FIXEDVALUE, LBM_BC_FLOWRATE = 0, 1, 2, 3
+LBM_VISC_CONSTANT, LBM_VISC_SUTHERLAND = 0, 1
 LBM_MASK_SOLID = 3
 LBM_MASK_REACTIVE = 4
 
@@ -73,6 +74,7 @@ class lbm_desc(C.Structure):
         ("T_scale", C.c_double), ("dt_phys", C.c_double), ("heat_norm", C.c_double),
         ("gas_coef", C.c_double), ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19),
         ("rho0", C.c_double), ("T0", C.c_double), ("side", lbm_side_desc * 6),
+        ("viscosity", C.c_int32), ("reserved0", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
     ]
 
 

@@ -140,9 +140,12 @@ def build_case(config: dict, logger: logging.Logger):
     visc = flow.get("viscosity")
     if visc is not None:
         vtype = visc.get("type", "constant") if isinstance(visc, dict) else "constant"
-        if vtype != "constant":
+        if vtype == "sutherland":
+            lb.set_viscosity_sutherland(float(visc["As"]), float(visc["Ts"]))    # src/LBM/app.py:117-120
+        elif vtype != "constant":
             raise NotImplementedError(f"flowProperties.viscosity.type {vtype!r} is not on the CUDA path")
-        lb.set_viscosity(float(_scalar(visc)))
+        else:
+            lb.set_viscosity(float(_scalar(visc)))
     if flow.get("force") is not None:
         lb.set_body_force([float(v) for v in flow["force"]])
 

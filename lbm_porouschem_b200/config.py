@@ -102,6 +102,9 @@ class LatticeConfig:
     T0: float = 0.0
     sides: list = field(default_factory=lambda: [SideBC() for _ in range(6)])
     bulk_form: str = "auto"         # "auto" (cell lists from 65536 cells) | "tile" | "list"
+    viscosity: str = "constant"     # "constant" (nu) | "sutherland" (per cell from T; thermal only)
+    suth_A: float = 0.0             # Sutherland: nu = suth_A TK^1.5 / (TK + suth_Ts), TK = T_ref + T_scale T
+    suth_Ts: float = 0.0            #   (suth_A = As dt/dx^2 in lattice units, suth_Ts in K)
 
     @property
     def shape(self) -> tuple:
@@ -174,6 +177,8 @@ class LatticeConfig:
             d.mrt_s[r] = v
         d.rho0, d.T0 = self.rho0, self.T0
         fill_sides(d.side, self.sides)
+        d.viscosity = {"constant": N.LBM_VISC_CONSTANT, "sutherland": N.LBM_VISC_SUTHERLAND}[self.viscosity]
+        d.suth_A, d.suth_Ts = self.suth_A, self.suth_Ts
         return d
 
 

@@ -245,6 +245,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.pyA = (C)d.pyro_A; p.pyb = (C)d.pyro_b; p.pyEaR = (C)(d.pyro_Ea / kGasConstant); p.pyTmin = (C)d.pyro_Tmin;
   p.Tref = (C)d.T_ref; p.Tscale = (C)d.T_scale; p.dtp = (C)d.dt_phys;
   p.heat_norm = (C)d.heat_norm; p.gas_coef = (C)d.gas_coef; p.alpha_flip = (C)d.alpha_flip;
+  p.suthA = (C)d.suth_A; p.suthTs = (C)d.suth_Ts;
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

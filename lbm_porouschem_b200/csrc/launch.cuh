@@ -7,6 +7,13 @@
 namespace lbm {
 namespace capi {
 
+// Collision code of the kernels: LBM_COLL_*, plus kCollSutherland with the Sutherland
+// viscosity (thermal modes only: THERM 1-3)
+constexpr int kSB = kCollSutherland + LBM_COLL_BGK, kSM = kCollSutherland + LBM_COLL_MRT;
+inline int collision_code(const lbm_desc& d) {
+  return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0);
+}
+
 template <class Lt, class S, int COLL, int THERM, int MODE>
 static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st) {
   constexpr size_t smem = list_smem_bytes<Lt, S>(128);
@@ -92,12 +99,13 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
 
 template <class Lt, class S>
 int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
-  const int coll = h->d.collision;
+  const int coll = collision_code(h->d);
   const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_step<Lt, S, C_, T_>(h, p, st); return LBM_OK; }
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
+  LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -119,12 +127,13 @@ static void launch_batch(lbm_batch* b, cudaStream_t st) {
 template <class Lt, class S>
 int dispatch_batch(lbm_batch* b, cudaStream_t st) {
   const lbm_desc& d = b->hs[0]->d;
-  const int coll = d.collision;
+  const int coll = collision_code(d);
   const int therm = d.thermal ? (d.pyro ? 2 : (d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_batch<Lt, S, C_, T_>(b, st); return LBM_OK; }
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
+  LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -132,7 +141,7 @@ int dispatch_batch(lbm_batch* b, cudaStream_t st) {
 template <class Lt, class S>
 int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
                   const float* alpha, int solid_bit, cudaStream_t st) {
-  const int coll = h->d.collision;
+  const int coll = collision_code(h->d);
   const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
   const int bs = 256;
   const unsigned nb = (unsigned)((h->N + bs - 1) / bs);
@@ -143,6 +152,7 @@ int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float*
   }
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
+  LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }

@@ -42,6 +42,10 @@ static int validate(const lbm_desc* d) {
   if (d->pyro && d->thermal != LBM_THERMAL_CONJUGATE)
     return fail(LBM_ERR_ARG, "pyrolysis needs the conjugate thermal field (heat reaches a reacting cell through it)");
   if (!(d->nu > 0)) return fail(LBM_ERR_ARG, "nu must be > 0");
+  if (d->viscosity != LBM_VISC_CONSTANT && d->viscosity != LBM_VISC_SUTHERLAND)
+    return fail(LBM_ERR_ARG, "unknown viscosity model");
+  if (d->viscosity == LBM_VISC_SUTHERLAND && (d->thermal == LBM_THERMAL_NONE || !(d->suth_A > 0)))
+    return fail(LBM_ERR_ARG, "Sutherland viscosity needs the temperature field and suth_A > 0");
   if (d->thermal && !(d->tauT_fluid > 0.5 && d->tauT_solid > 0.5))
     return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");
   for (int s = 0; s < 6; ++s) {
@@ -273,8 +277,8 @@ int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector
     if (!h->L.list)
       return fail(LBM_ERR_ARG, "batch member " + std::to_string(i) + " does not use cell lists (set bulk_form = 2)");
     if (h->d.dim != d0.dim || h->d.precision != d0.precision || h->d.collision != d0.collision ||
-        h->d.thermal != d0.thermal || h->d.pyro != d0.pyro)
-      return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, thermal and pyro");
+        h->d.thermal != d0.thermal || h->d.pyro != d0.pyro || h->d.viscosity != d0.viscosity)
+      return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, viscosity, thermal and pyro");
     if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
     if (has_flowrate(h->d)) return fail(LBM_ERR_ARG, "batch members cannot have a flow-rate inlet");
     for (int j = 0; j < i; ++j)

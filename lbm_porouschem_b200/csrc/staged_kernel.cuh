@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(TILE, (std::is_same<S, double>::value ? 1 : 4)
         K::moments(p, F, rho, ux, uy, uz);
         if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
         if (!peek) {
-          K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
+          K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T);
           K::store_flow(p, nb, c, nbits, F);
         }
       } else if constexpr (PYRO) {

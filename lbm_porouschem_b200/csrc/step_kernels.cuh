@@ -60,6 +60,9 @@ template <> struct Store<__half> {
 };
 
 constexpr int kNumDiag = 10;              // partial slots per block (order of lbm_diag fields)
+// Internal collision codes: LBM_COLL_BGK / LBM_COLL_MRT, plus kCollSutherland when the
+// viscosity follows the cell's temperature (LBM_VISC_SUTHERLAND)
+constexpr int kCollSutherland = 2;
 
 // Flow-rate inlet state (LBM_FIELD_INLET, compute precision): slot 0 holds the
 // coefficient F/flow0 of the current step; after kInletHead slots come two halves,
@@ -112,6 +115,7 @@ struct StepParams {
   C itauT_f, itauT_s;
   C rho0, T0;
   C pyA, pyb, pyEaR, pyTmin, Tref, Tscale, dtp, heat_norm, gas_coef, alpha_flip;  // pyEaR = Ea/R
+  C suthA, suthTs;  // Sutherland viscosity (collision codes kCollSutherland + BGK/MRT)
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -314,12 +318,18 @@ struct Kern {
   // Flow collision (BGK: _evolution.py:33; MRT: new) plus Guo forcing; writes
   // the post-collision populations over F.  Works on opposite-direction pairs.
   template <int COLL>
-  __device__ __forceinline__ static void collide_flow(const P& p, C F[Q], C rho, C ux, C uy, C uz) {
-    const C tau = (C)3 * (p.eos == 0 ? p.nu / rho : p.nu) + (C)0.5;
+  __device__ __forceinline__ static void collide_flow(const P& p, C F[Q], C rho, C ux, C uy, C uz, C T = (C)0) {
+    C nu = p.nu;
+    if constexpr (COLL >= kCollSutherland) {
+      // Sutherland, src/LBM/LBM2D/_evolution.py:232-234, at the cell's temperature in kelvin
+      const C TK = T * p.Tscale + p.Tref;
+      nu = p.suthA * TK * sqrt(TK) / (TK + p.suthTs);
+    }
+    const C tau = (C)3 * (p.eos == 0 ? nu / rho : nu) + (C)0.5;
     const C itau = (C)1 / tau;
     const C usq = ux * ux + uy * uy + uz * uz;
     const C fe0 = feq_rest(p, rho, usq);
-    if constexpr (COLL == LBM_COLL_BGK) {
+    if constexpr ((COLL & 1) == LBM_COLL_BGK) {
       F[0] = F[0] - itau * (F[0] - fe0);
       static_for<NP>([&](auto pp) {
         constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
@@ -699,7 +709,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
     src.template flow<PYRO>(p, nb, c, nbits, F);
     K::moments(p, F, rho, ux, uy, uz);
     if (!peek) {
-      K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
+      K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T);
       K::store_flow(p, nb, c, nbits, F);
     }
     if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);  // after the store: fewer live registers
@@ -892,19 +902,23 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
       }
     });
   }
+  // temperature first: the collision's viscosity may depend on it (the pull reads the
+  // input half, which the flow store below does not touch)
+  C G[QT > 0 ? QT : 1];
+  C T = 0;
+  if constexpr (THERMAL) {
+    K::pull_thermal(p, nb, c, G);
+    static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
+  }
   {
     C F[Q];
     K::feq_all(p, rb, ux, uy, uz, F);
-    K::template collide_flow<COLL>(p, F, rb, ux, uy, uz);
+    K::template collide_flow<COLL>(p, F, rb, ux, uy, uz, T);
     const uint32_t nbn = K::neighbour_bits(p, nb, np);
     K::store_flow(p, nb, c, nbn, F);
     if (p.lhdr) list_turn_fluid<L>(p, c, nb, nbn);
   }
   if constexpr (THERMAL) {
-    C G[QT];
-    K::pull_thermal(p, nb, c, G);
-    C T = 0;
-    static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
     K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
@@ -1140,7 +1154,7 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   if (!(p.flags & kStepPeek)) {
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
     const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
-    K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz);
+    K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz, s.T);
     K::store_flow(p, nb, c, nbits, s.F);
     if constexpr (THERMAL) {
       K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
@@ -1199,7 +1213,7 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
   if (!solid) {
     C F[Q];
     K::feq_all(p, rho, ux, uy, uz, F);
-    K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
+    K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T_in ? (C)T_in[c] : (C)0);
     K::store_flow(p, nb, (int)c, nbits, F);
   }
   if constexpr (THERMAL) {

@@ -136,6 +136,7 @@ class _SolverBase:
         self.RADIATION = bool(isRadiation and isThermal)
         self.viscosity_model = VISCOSITY_MODEL.NONE
         self.visco = 2e-5
+        self.sutherland_coef = [1.6e-6, 170.0]   # src/LBM/LBM2D/_core.py:27
         self.source_term_model = SOURCE_TERM.NONE
         self.force_term_model = FORCE_TERM.NONE
         self.boundary_condition_model = BC_MODEL.NEE
@@ -212,7 +213,9 @@ class _SolverBase:
         self.viscosity_model = VISCOSITY_MODEL.CONSTANT
 
     def set_viscosity_sutherland(self, As, Ts):
-        raise NotImplementedError("Sutherland viscosity is not on the CUDA path (constant viscosity only)")
+        """src/LBM/LBM2D/_io.py:144-147: mu = As T^1.5/(T + Ts) at the fluid temperature."""
+        self.sutherland_coef = [float(As), float(Ts)]
+        self.viscosity_model = VISCOSITY_MODEL.SUTHERLAND
 
     def set_viscosity_mixture(self):
         raise NotImplementedError("mixture viscosity needs species transport, which is not on the CUDA path")
@@ -420,7 +423,7 @@ class _SolverBase:
         return sides
 
     def _config(self) -> LatticeConfig:
-        if self.viscosity_model not in (VISCOSITY_MODEL.CONSTANT, VISCOSITY_MODEL.NONE):
+        if self.viscosity_model not in (VISCOSITY_MODEL.CONSTANT, VISCOSITY_MODEL.NONE, VISCOSITY_MODEL.SUTHERLAND):
             raise NotImplementedError(f"{self.viscosity_model} is not on the CUDA path")
         cfg = LatticeConfig(
             dim=self.DIM, nx=self.nx, ny=self.ny, nz=self.nz, collision=self.collision, precision=self.precision,
@@ -433,6 +436,14 @@ class _SolverBase:
             cfg.tauT_fluid = self._tau_T(dF)
             cfg.tauT_solid = self._tau_T(dS)
             cfg.T_ref, cfg.T_scale = self.TF.v_ref, self.TF.v_scale
+        if self.viscosity_model == VISCOSITY_MODEL.SUTHERLAND:
+            # src/LBM/LBM2D/_evolution.py:232-234 at GetTF (:304-307): the fluid
+            # temperature, or 273.15 K without the temperature field
+            As, Ts = self.sutherland_coef
+            if self.TEMPERATURE:
+                cfg.viscosity, cfg.suth_A, cfg.suth_Ts = "sutherland", As * self.dt / self.dx ** 2, Ts
+            else:
+                cfg.nu = As * 273.15 ** 1.5 / (273.15 + Ts) * self.dt / self.dx ** 2
         if self._pyro:
             pz = self._pyro
             cfg.pyro = True

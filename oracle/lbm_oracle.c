@@ -85,6 +85,8 @@ typedef struct orc_cfg {
     double alpha_flip;       /* reactive fraction below which a solid cell turns fluid */
     double mrt_s[19];        /* MRT relaxation rates per moment (viscous ones overwritten by 1/tau) */
     orc_side side[6];        /* 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+ */
+    int visc_model;          /* 0 constant nu, 1 Sutherland: nu = suth_A T^1.5/(T + suth_Ts), T in K */
+    double suth_A, suth_Ts;  /* suth_A = As*dt/dx^2 (LBM2D/_evolution.py:228-235) */
 } orc_cfg;
 
 /* mask bits */
@@ -189,9 +191,14 @@ static inline REAL geq_fluid(const orc* o, int k, REAL T, const REAL* u) {
     REAL uv = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
     return o->wt[k]*T*((REAL)1.0 + o->ta*eu + o->tb*eu*eu - o->tc*uv);
 }
-/* tau: src/LBM/LBM2D/_evolution.py:241-249 (IDEAL_GAS divides viscosity by rho) */
-static inline REAL tau_flow(const orc* o, REAL rho) {
+/* tau: src/LBM/LBM2D/_evolution.py:228-249 (viscosity(i): constant or Sutherland at the
+ * fluid temperature GetTF(i) = T_ref + T_scale*T, :304-307; IDEAL_GAS divides by rho) */
+static inline REAL tau_flow(const orc* o, REAL rho, REAL T) {
     REAL nu = (REAL)o->c.nu;
+    if (o->c.visc_model == 1) {
+        REAL TK = T*(REAL)o->c.T_scale + (REAL)o->c.T_ref;
+        nu = (REAL)o->c.suth_A*(REAL)pow(TK, 1.5)/(TK + (REAL)o->c.suth_Ts);
+    }
     if (o->c.eos == 0) nu = nu / rho;
     return (REAL)3*nu + (REAL)0.5;
 }
@@ -211,9 +218,9 @@ static inline REAL guo(const orc* o, int k, REAL rho, const REAL* u, REAL tau) {
 }
 
 /* Post-collision flow populations of a fluid cell (BGK: _evolution.py:33; MRT new). */
-static void collide_flow(const orc* o, const REAL* fin, REAL rho, const REAL* u, REAL* fout) {
+static void collide_flow(const orc* o, const REAL* fin, REAL rho, const REAL* u, REAL T, REAL* fout) {
     int Q = o->Q;
-    REAL tau = tau_flow(o, rho);
+    REAL tau = tau_flow(o, rho, T);
     REAL fe[19];
     for (int k = 0; k < Q; ++k) fe[k] = feq(o, k, rho, u);
     if (o->c.collision == 0) {
@@ -356,7 +363,7 @@ static void collide_stream(orc* o) {
         REAL fo[19], go[7];
         int solid = is_solid(o->mask, c);
         if (!solid) {
-            collide_flow(o, &o->f[c*Q], o->rho[c], &o->u[c*3], fo);
+            collide_flow(o, &o->f[c*Q], o->rho[c], &o->u[c*3], o->T[c], fo);
             for (int k = 0; k < Q; ++k) {
                 long ip = nbr(o, c, k, +1);
                 if (!is_solid(o->mask, ip)) o->F[ip*Q + k] = fo[k];      /* :69-70 */

@@ -39,6 +39,7 @@ class orc_cfg(C.Structure):
         ("pyro_Ea", C.c_double), ("pyro_Tmin", C.c_double), ("T_ref", C.c_double), ("T_scale", C.c_double),
         ("dt_phys", C.c_double), ("heat_norm", C.c_double), ("gas_coef", C.c_double),
         ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19), ("side", orc_side * 6),
+        ("visc_model", C.c_int), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
     ]
 
 
@@ -112,6 +113,8 @@ class Oracle:
         c.pyro_A, c.pyro_b, c.pyro_Ea, c.pyro_Tmin = cfg.pyro_A, cfg.pyro_b, cfg.pyro_Ea, cfg.pyro_Tmin
         c.T_ref, c.T_scale, c.dt_phys = cfg.T_ref, cfg.T_scale, cfg.dt_phys
         c.heat_norm, c.gas_coef, c.alpha_flip = cfg.heat_norm, cfg.gas_coef, cfg.alpha_flip
+        c.visc_model = 1 if cfg.viscosity == "sutherland" else 0
+        c.suth_A, c.suth_Ts = cfg.suth_A, cfg.suth_Ts
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):

@@ -110,6 +110,15 @@ def test_flowrate_inlet_from_yaml():
     assert sd[0].rho_type == ZERO_GRADIENT and sd[0].T_type == FIXED_VALUE
 
 
+def test_sutherland_viscosity_from_yaml():
+    """flowProperties.viscosity {type: sutherland, As, Ts} (src/LBM/app.py:117-120)."""
+    cfg = yaml.safe_load(CASE2D)
+    cfg["flowProperties"]["viscosity"] = {"type": "sutherland", "As": 1.5e-6, "Ts": 110.4}
+    c = build_case(cfg, _log())._config()
+    assert c.viscosity == "sutherland" and c.suth_Ts == 110.4
+    assert c.suth_A == pytest.approx(1.5e-6 * 1e-4 / 1e-6)
+
+
 def test_unsupported_options_stop_the_run():
     cfg = yaml.safe_load(CASE2D)
     cfg["chemicalProperties"] = {"type": "cantera", "canteraFile": "mech.yaml"}

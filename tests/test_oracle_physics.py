@@ -272,3 +272,31 @@ _E = {2: [(0, 0, 0), (1, 0, 0), (0, 1, 0), (-1, 0, 0), (0, -1, 0), (1, 1, 0), (-
           (1, -1, 0), (-1, -1, 0), (1, 0, 1), (-1, 0, 1), (1, 0, -1), (-1, 0, -1), (0, 1, 1), (0, -1, 1),
           (0, 1, -1), (0, -1, -1)]}
 _W = {2: np.array([4 / 9] + [1 / 9] * 4 + [1 / 36] * 4), 3: np.array([1 / 3] + [1 / 18] * 6 + [1 / 36] * 12)}
+
+
+@pytest.mark.parametrize("coll", ["bgk", "mrt"])
+def test_sutherland_at_uniform_temperature_equals_constant_viscosity(oracle_mod, coll):
+    """Sutherland viscosity (src/LBM/LBM2D/_evolution.py:232-234) at a uniform temperature
+    is the constant viscosity suth_A TK^1.5/(TK + Ts).  The flow moves the temperature by
+    ~1e-5 (compressibility, solid interfaces), so the runs agree to 1e-4 of the velocity
+    scale; a wrong law or unit mapping differs at order one."""
+    shape = (20, 14)
+    solid = packing(shape, 1.5, 2.5, 0.8, seed=4)
+    base = LatticeConfig(dim=2, nx=20, ny=14, collision=coll, nu=0.1, thermal="conjugate",
+                         force=(2e-5, 0.0, 0.0), T_ref=300.0, T_scale=500.0)
+    TK = 300.0 + 500.0 * 0.6
+    A, Ts = 0.004, 170.0
+    suth = base.replace(viscosity="sutherland", suth_A=A, suth_Ts=Ts)
+    const = base.replace(nu=A * TK ** 1.5 / (TK + Ts))
+    out = []
+    for cfg in (suth, const):
+        o = oracle_mod.Oracle(cfg, real="f64")
+        o.init(solid, rho=1.0, u=(0.0, 0.0, 0.0), T=0.6)
+        o.step(150)
+        out.append(o.fields())
+    fl = ~out[0]["solid"]
+    umax = np.abs(out[0]["u"][:, fl]).max()
+    assert umax > 1e-5
+    assert np.abs(out[0]["T"] - 0.6).max() < 1e-4
+    assert np.abs(out[0]["u"] - out[1]["u"]).max() < 1e-4 * umax
+    assert np.abs(out[0]["rho"] - out[1]["rho"]).max() < 1e-8

@@ -92,8 +92,6 @@ def test_prandtl_and_pyrolysis_mapping():
 def test_unsupported_features_raise():
     s = LBM2DSolver(X=8, Y=8, Z=0)
     with pytest.raises(NotImplementedError):
-        s.set_viscosity_sutherland(1.0, 1.0)
-    with pytest.raises(NotImplementedError):
         s.load_cantera("gri30.yaml")
     s.boundary_condition_model = BC_MODEL.NEBB
     s.set_BC(0, BC_FLOW.outlet)
@@ -123,6 +121,24 @@ def test_flowrate_inlet_mapping():
     sd = s3._config().sides
     assert sd[0].v_type == FIXED_VALUE and sd[0].v == pytest.approx((0.4 / 4 / 5, 0.0, 0.0))
     assert sd[1].v_type == FIXED_VALUE and sd[1].v == (0.0, 0.0, 0.0)
+
+
+def test_sutherland_viscosity_mapping():
+    """set_viscosity_sutherland (src/LBM/LBM2D/_io.py:144-147): with the temperature field
+    the lattice takes As dt/dx^2 and Ts; without it the reference evaluates the law at
+    273.15 K (GetTF, _evolution.py:304-307), a constant viscosity."""
+    s = _channel2d()
+    s.set_viscosity_sutherland(1.6e-6, 170.0)
+    c = s._config()
+    assert c.viscosity == "sutherland" and c.suth_Ts == 170.0
+    assert c.suth_A == pytest.approx(1.6e-6 * 1e-4 / 1e-6)
+    d = c.to_desc()
+    assert d.viscosity == 1 and d.suth_A == pytest.approx(1.6e-4)
+    s2 = LBM2DSolver(X=8, Y=8, Z=0, dx=1e-3, dt=1e-4)
+    s2.set_viscosity_sutherland(1.6e-6, 170.0)
+    c2 = s2._config()
+    assert c2.viscosity == "constant"
+    assert c2.nu == pytest.approx(1.6e-6 * 273.15 ** 1.5 / (273.15 + 170.0) * 1e-4 / 1e-6)
 
 
 def test_init_field_forms(tmp_path):
