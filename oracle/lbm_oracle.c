@@ -5,14 +5,16 @@
  * tests, the smoke entry and the bench's CPU-baseline leg call it.  Nothing in
  * the product links or executes it.
  *
- * PARITY UNPINNED: the reference (Python + Taichi 1.7.4) cannot run in this
- * environment (Taichi is not installed and there is no network) and its own
- * tests pin no lattice numbers.  This restatement follows the reference's code
- * line by line where the reference defines the behaviour, and defines the new
- * behaviour (body force, conjugate heat, pyrolysis with cell flip, MRT,
- * reductions) where the reference has none.  It is pinned instead by analytic
- * known answers (Poiseuille, mass conservation, equilibrium fixed point, the
- * single-cell Arrhenius ODE) in tests/test_oracle_*.py.
+ * PARITY PINNED against the reference's own code: tests/golden/ref_*.npz hold outputs
+ * of the unmodified reference solver modules (src/LBM/LBM2D, src/LBM/LBM3D) run on
+ * small lattices through a sequential NumPy stand-in for Taichi (the reference's Taichi
+ * 1.7.4 is not installable here), in float64; tests/test_oracle_vs_reference.py checks
+ * this file's FP64 build against them to 1e-12 (it agrees bit for bit) on periodic, NEE,
+ * ES and NEE-on-periodic sides, 2D and 3D, flow and two-field temperature.  Where the
+ * reference has no behaviour (body force, conjugate heat, pyrolysis with cell flip, MRT,
+ * reductions) this file defines it, pinned by analytic known answers (Poiseuille, mass
+ * conservation, equilibrium fixed point, the single-cell Arrhenius ODE) in
+ * tests/test_oracle_physics.py.
  *
  * Structure mirrors the reference's push scheme:
  *   step():  collision_source_streaming (push, halfway bounce-back)
@@ -87,6 +89,10 @@ typedef struct orc_cfg {
     orc_side side[6];        /* 0 x-, 1 x+, 2 y-, 3 y+, 4 z-, 5 z+ */
     int visc_model;          /* 0 constant nu, 1 Sutherland: nu = suth_A T^1.5/(T + suth_Ts), T in K */
     double suth_A, suth_Ts;  /* suth_A = As*dt/dx^2 (LBM2D/_evolution.py:228-235) */
+    int ref_quirk_frozen_solid_T; /* two fields only: the reference's macro skips pure-solid
+                              * cells (LBM2D/_evolution.py:119), so their TS.S never changes and
+                              * TS.g keeps its own post-collision values instead of the streamed
+                              * ones (collision :96-100 writes TS.g in place).  1 reproduces that. */
 } orc_cfg;
 
 /* mask bits */
@@ -387,6 +393,8 @@ static void collide_stream(orc* o) {
                 if (o->c.thermal == 2 && k > 0 && is_solid(o->mask, ip) != solid) o->G[c*QT + o->opp[k]] = go[k];
                 else o->G[ip*QT + k] = go[k];
             }
+            if (solid && o->c.thermal == 2 && o->c.ref_quirk_frozen_solid_T)
+                for (int k = 0; k < QT; ++k) o->g[c*QT + k] = go[k];   /* TS.g[i][k] = g, :96-100 */
         }
     }
     /* pyrolysis gas release: a reacting solid cell pushes rel*w_k into each fluid
@@ -425,7 +433,7 @@ static void macro(orc* o) {
             o->rho[c] = r;
             for (int d = 0; d < 3; ++d) o->u[c*3 + d] = j[d];
         }
-        if (o->c.thermal >= 1) {
+        if (o->c.thermal >= 1 && !(o->c.thermal == 2 && o->c.ref_quirk_frozen_solid_T && is_solid(o->mask, c))) {
             REAL Tc = 0;
             for (int k = 0; k < QT; ++k) { Tc += o->G[c*QT + k]; o->g[c*QT + k] = o->G[c*QT + k]; }
             o->T[c] = Tc;

@@ -3,10 +3,10 @@
 TEST INFRASTRUCTURE ONLY: imported by ``tests/``, ``__graft_entry__.smoke()``
 and the CPU-baseline leg of ``bench.py``.  Never part of the product path.
 
-PARITY UNPINNED: the reference cannot run here (Taichi 1.7.4 is absent and
-there is no network) and ships no golden vectors for the lattice update, so
-this restatement is pinned by analytic known answers instead
-(tests/test_oracle_physics.py).
+PARITY PINNED: ``tests/test_oracle_vs_reference.py`` checks the FP64 build against
+golden outputs of the reference's own solver modules (``tests/golden/ref_*.npz``, made by
+``tests/golden/make_reference_fixtures.py``); behaviour the reference lacks is pinned by
+analytic known answers (``tests/test_oracle_physics.py``).
 
 ``build_oracle()`` compiles ``lbm_oracle.c`` twice (FP32 and FP64) with
 ``gcc -O3 -fopenmp`` into ``oracle/_build/``.
@@ -40,6 +40,7 @@ class orc_cfg(C.Structure):
         ("dt_phys", C.c_double), ("heat_norm", C.c_double), ("gas_coef", C.c_double),
         ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19), ("side", orc_side * 6),
         ("visc_model", C.c_int), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
+        ("ref_quirk_frozen_solid_T", C.c_int),
     ]
 
 
@@ -94,7 +95,11 @@ class Oracle:
     ``real`` is "f32" or "f64" (the arithmetic precision of the restatement).
     Arrays in and out use the reference's (nx, ny, nz) layout."""
 
-    def __init__(self, cfg, real: str = "f64", threads: int | None = None):
+    def __init__(self, cfg, real: str = "f64", threads: int | None = None,
+                 ref_quirk_frozen_solid_T: bool = False):
+        """``ref_quirk_frozen_solid_T`` (two-field temperature only) reproduces the reference's
+        pure-solid cells, whose temperature ``macro`` never refreshes
+        (src/LBM/LBM2D/_evolution.py:119); the default diffuses heat through the solid."""
         self.cfg = cfg
         self.lib = _load(real)
         if threads:
@@ -115,6 +120,7 @@ class Oracle:
         c.heat_norm, c.gas_coef, c.alpha_flip = cfg.heat_norm, cfg.gas_coef, cfg.alpha_flip
         c.visc_model = 1 if cfg.viscosity == "sutherland" else 0
         c.suth_A, c.suth_Ts = cfg.suth_A, cfg.suth_Ts
+        c.ref_quirk_frozen_solid_T = int(ref_quirk_frozen_solid_T)
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):

@@ -1,0 +1,278 @@
+"""Generate golden fixtures by running LBM_porousChem's own solver code on small lattices.
+
+TEST INFRASTRUCTURE ONLY (run by hand in a checkout that has the reference next to it; the
+fixtures it writes are committed and the tests read only those):
+
+    python tests/golden/make_reference_fixtures.py /path/to/LBM_porousChem
+
+The reference is Python + Taichi 1.7.4, and Taichi is not installable here, so the script
+puts ``tests/golden/standin`` (a sequential NumPy stand-in for the Taichi subset the solver
+uses, plus empty ``pyevtk``/``pyvista``/``ruamel.yaml`` modules its I/O file imports) ahead
+of ``<reference>/src`` on ``sys.path`` and drives the **unmodified** ``LBM.LBM2D.LBM2DSolver``
+/ ``LBM.LBM3D.LBM3DSolver`` through their own setters, exactly as ``src/LBM/app.py:101-677``
+does: constructor, ``set_viscosity``, ``set_BC``..., ``init_field``/``init_field3``/
+``add_solid``, ``init_simulation()``, then ``step()`` N times.  Real type: float64.
+
+Each case also records the ``LatticeConfig`` that describes the same run to this package
+(``meta``), with the mapping rules written next to it:
+
+* ``set_viscosity(mu)`` with dx = dt = 1 -> ``nu = mu`` (``LBM2D/_evolution.py:227-249``);
+  IDEAL_GAS, so tau = 3 nu/rho + 1/2 in both.
+* thermal diffusivity D -> ``tauT = 3 D + 1/2`` (2D) / ``4 D + 1/2`` (3D),
+  ``_scalarField.py:56-58``; the fixture computes tauT with the same expression.
+* ``BC_FLOW.inlet`` / ``outlet`` / ``wall`` -> ``SideBC.inlet`` / ``outlet`` / ``wall``
+  (``LBM2D/_io.py:385-402``); under ``BC_MODEL.NEE`` every side is extrapolated, so sides the
+  case leaves periodic are active with PERIODIC types (``ref_quirk_nee_on_periodic``).
+* 3D side 4 (z = 0) "zero-gradient" density assigns the cell to itself
+  (``LBM3D/_boundary.py:128``), i.e. keeps the cell's own density: PERIODIC density type.
+* two-field temperature on a binary mask: fluid cells carry ``TF``, solid cells ``TS``;
+  ``macro`` skips solid cells, so ``TS`` there is never refreshed from the streamed
+  populations (``LBM2D/_evolution.py:119``): ``ref_quirk_frozen_solid_T``.
+
+Every input is float32-representable (``init_field`` of a constant goes through float32,
+``LBM2D/_io.py:49-51``, and the CUDA path takes float32 initial fields).
+"""
+from __future__ import annotations
+
+import json
+import os
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+ROOT = HERE.parent.parent
+sys.path.insert(0, str(ROOT))
+
+from lbm_porouschem_b200.config import (FIXED_VALUE, PERIODIC, ZERO_GRADIENT,  # noqa: E402
+                                        LatticeConfig, SideBC)
+
+
+def _import_reference(ref_root: str):
+    sys.path.insert(0, str(HERE / "standin"))
+    sys.path.insert(1, os.path.join(ref_root, "src"))
+    from LBM.LBM2D import LBM2DSolver
+    from LBM.LBM3D import LBM3DSolver
+    from LBM.util import flag
+    return LBM2DSolver, LBM3DSolver, flag
+
+
+# --------------------------------------------------------------------------- inputs
+def _disks(shape, n, rmin, rmax, margin_x, seed):
+    """Binary mask of ``n`` seeded disks (circles in 2D, spheres in 3D) kept ``margin_x`` cells
+    away from the x sides (those are the active sides of the channel cases)."""
+    rng = np.random.default_rng(seed)
+    grids = np.meshgrid(*[np.arange(s) for s in shape], indexing="ij")
+    m = np.zeros(shape, dtype=bool)
+    for _ in range(n):
+        r = rng.uniform(rmin, rmax)
+        c = [rng.uniform(margin_x + r, shape[0] - 1 - margin_x - r)]
+        c += [rng.uniform(0, s) for s in shape[1:]]
+        d2 = sum((g - cc) ** 2 for g, cc in zip(grids, c))
+        m |= d2 <= r * r
+    return m
+
+
+def _smooth_field(shape, seed, amp):
+    """float32-representable smooth random perturbation."""
+    rng = np.random.default_rng(seed)
+    grids = np.meshgrid(*[np.arange(s) for s in shape], indexing="ij")
+    out = np.zeros(shape)
+    for _ in range(3):
+        k = [rng.integers(1, 3) * 2 * np.pi / s for s in shape]
+        ph = rng.uniform(0, 2 * np.pi)
+        out += np.cos(sum(kk * g for kk, g in zip(k, grids)) + ph)
+    return (amp * out / 3).astype(np.float32).astype(np.float64)
+
+
+# --------------------------------------------------------------------------- cases
+def _common_inputs(shape, seed, solid, u_amp=0.02, rho_amp=0.002, T0=None):
+    nd = len(shape)
+    rho = (1.0 + _smooth_field(shape, seed, rho_amp)).astype(np.float32).astype(np.float64)
+    u = np.stack([_smooth_field(shape, seed + 1 + d, u_amp) if d < nd else np.zeros(shape)
+                  for d in range(3)])
+    u[:, solid] = 0.0
+    T = np.zeros(shape) if T0 is None else T0
+    return rho, u, T
+
+
+def case_periodic2d():
+    shape = (16, 12, 1)
+    solid = _disks(shape[:2], 3, 1.5, 2.5, 0, 1)[..., None]
+    rho, u, T = _common_inputs(shape, 11, solid)
+    cfg = LatticeConfig(dim=2, nx=16, ny=12, nz=1, collision="bgk", precision="fp64", nu=0.1)
+    return dict(name="ref_periodic2d", cfg=cfg, bc_model="NONE", solid=solid, rho=rho, u=u, T=T,
+                steps=60, thermal=None, sides=None)
+
+
+def _channel_sides(flag, dim, u_in, rho_out, thermal):
+    """inlet at x = 0, outlet at x = nx-1, walls on the other sides (2D: y; 3D: y and z)."""
+    T_in = 1.0
+    ref = {0: ("inlet", (u_in, 0.0, 0.0), None), 1: ("outlet", None, rho_out)}
+    for s in range(2, 2 * dim):
+        ref[s] = ("wall", None, None)
+    tbc = {0: ("fixed", T_in), 1: ("zero", None)}
+    for s in range(2, 2 * dim):
+        tbc[s] = ("zero", None)
+    Tt = lambda s: (FIXED_VALUE if tbc[s][0] == "fixed" else ZERO_GRADIENT) if thermal else PERIODIC
+    sides = [SideBC() for _ in range(6)]
+    sides[0] = SideBC.inlet((u_in, 0.0, 0.0), Tt(0), T_in)
+    sides[1] = SideBC.outlet(rho_out, Tt(1), 0.0)
+    for s in range(2, 2 * dim):
+        sides[s] = SideBC.wall(Tt(s), 0.0)
+    if dim == 3:
+        sides[4].rho_type = PERIODIC   # LBM3D/_boundary.py:128 self-assignment
+    return ref, tbc, sides
+
+
+def case_channel2d_thermal():
+    nx, ny = 20, 12
+    shape = (nx, ny, 1)
+    solid = np.zeros(shape, dtype=bool)
+    solid[:, 2:ny - 2, 0] = _disks((nx, ny - 4), 3, 1.5, 2.2, 3, 2)
+    T0 = (_smooth_field(shape, 23, 0.2) + 0.3).astype(np.float32).astype(np.float64)
+    rho, u, T = _common_inputs(shape, 21, solid, T0=T0)
+    Df, Ds = 1.0 / 30.0, 0.1
+    cfg = LatticeConfig(dim=2, nx=nx, ny=ny, nz=1, collision="bgk", precision="fp64", nu=0.1,
+                        thermal="two_field", tauT_fluid=3 * Df + .5, tauT_solid=3 * Ds + .5)
+    return dict(name="ref_channel2d_thermal", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u,
+                T=T, steps=60, thermal=(Df, Ds), channel=(0.03, 1.0))
+
+
+def case_channel2d_es():
+    d = case_channel2d_thermal()
+    d["name"] = "ref_channel2d_es"
+    d["bc_model"] = "ES"
+    d["steps"] = 40
+    return d
+
+
+def case_nee_periodic2d():
+    """NEE model with the y sides left periodic: the reference extrapolates them anyway."""
+    nx, ny = 18, 10
+    shape = (nx, ny, 1)
+    solid = np.zeros(shape, dtype=bool)
+    solid[:, 2:ny - 2, 0] = _disks((nx, ny - 4), 2, 1.5, 2.0, 3, 5)
+    rho, u, T = _common_inputs(shape, 31, solid)
+    cfg = LatticeConfig(dim=2, nx=nx, ny=ny, nz=1, collision="bgk", precision="fp64", nu=0.12)
+    return dict(name="ref_nee_periodic2d", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T,
+                steps=50, thermal=None, channel=(0.02, 1.0), periodic_y=True)
+
+
+def case_periodic3d():
+    shape = (10, 8, 8)
+    solid = _disks(shape, 2, 1.5, 2.2, 0, 7)
+    rho, u, T = _common_inputs(shape, 41, solid)
+    cfg = LatticeConfig(dim=3, nx=10, ny=8, nz=8, collision="bgk", precision="fp64", nu=0.1)
+    return dict(name="ref_periodic3d", cfg=cfg, bc_model="NONE", solid=solid, rho=rho, u=u, T=T,
+                steps=24, thermal=None)
+
+
+def case_channel3d_thermal():
+    nx, ny, nz = 12, 8, 8
+    shape = (nx, ny, nz)
+    solid = np.zeros(shape, dtype=bool)
+    solid[:, 2:ny - 2, 2:nz - 2] = _disks((nx, ny - 4, nz - 4), 2, 1.2, 1.8, 3, 8)
+    T0 = (_smooth_field(shape, 53, 0.2) + 0.3).astype(np.float32).astype(np.float64)
+    rho, u, T = _common_inputs(shape, 51, solid, T0=T0)
+    Df, Ds = 0.025, 0.1
+    cfg = LatticeConfig(dim=3, nx=nx, ny=ny, nz=nz, collision="bgk", precision="fp64", nu=0.1,
+                        thermal="two_field", tauT_fluid=4 * Df + .5, tauT_solid=4 * Ds + .5)
+    return dict(name="ref_channel3d_thermal", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u,
+                T=T, steps=20, thermal=(Df, Ds), channel=(0.03, 1.0))
+
+
+CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
+         case_periodic3d, case_channel3d_thermal]
+
+
+# --------------------------------------------------------------------------- driver
+def run_reference(case, Solver2D, Solver3D, flag):
+    cfg = case["cfg"]
+    dim = cfg.dim
+    nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
+    thermal = case.get("thermal")
+    Solver = Solver2D if dim == 2 else Solver3D
+    lb = Solver(nx, ny, nz, 1, 1, case["name"], thermal is not None, False, False, False)
+    lb.source_term_model = flag.SOURCE_TERM.MICRO       # app.py:103-104
+    lb.force_term_model = flag.FORCE_TERM.GUO
+    lb.set_viscosity(cfg.nu)
+    lb.boundary_condition_model = getattr(flag.BC_MODEL, case["bc_model"])
+    sides = [SideBC() for _ in range(6)]
+    if "channel" in case:
+        u_in, rho_out = case["channel"]
+        ref, tbc, sides = _channel_sides(flag, dim, u_in, rho_out, thermal is not None)
+        if case.get("periodic_y"):
+            ref = {s: v for s, v in ref.items() if s < 2}
+            for s in (2, 3):
+                sides[s] = SideBC(True, PERIODIC, PERIODIC, PERIODIC)
+        for s, (kind, v, r) in ref.items():
+            lb.set_BC(s, getattr(flag.BC_FLOW, kind))
+            if v is not None:
+                lb.set_v_BC_value(s, list(v))
+            if r is not None:
+                lb.set_rho_BC_value(s, r)
+        if thermal is not None:
+            for s, (kind, val) in tbc.items():
+                bc = flag.BC.fixedValue if kind == "fixed" else flag.BC.zeroGradient
+                lb.set_TF_BC(s, bc)
+                lb.set_TS_BC(s, bc)
+                if val is not None:
+                    lb.set_TF_BC_value(s, val)
+                    lb.set_TS_BC_value(s, val)
+    if case["bc_model"] == "NEE":
+        for s in range(2 * dim):
+            if not sides[s].active:
+                sides[s] = SideBC(True, PERIODIC, PERIODIC, PERIODIC)
+    if case["bc_model"] == "ES":
+        for s in range(2 * dim):
+            sides[s].model = "es"
+    cfg.sides = sides
+    if thermal is not None:
+        Df, Ds = thermal
+        lb.set_fluid_thermal_diff(Df)
+        lb.set_solid_thermal_diff(Ds)
+        lb.init_field(lb.TF.S, case["T"].copy())
+        lb.init_field(lb.TS.S, case["T"].copy())
+    lb.init_field(lb.rho, case["rho"].copy())
+    lb.init_field3(lb.v, case["u"][0].copy(), case["u"][1].copy(), case["u"][2].copy())
+    lb.add_solid(case["solid"].astype(np.float64))
+    lb.init_simulation()
+    t0 = time.time()
+    for _ in range(case["steps"]):
+        lb.step()
+    out = dict(rho=lb.rho.to_numpy(), u=np.moveaxis(lb.v.to_numpy(), -1, 0),
+               f=np.moveaxis(lb.f.to_numpy(), -1, 0))
+    if thermal is not None:
+        tf, ts = lb.TF.S.to_numpy(), lb.TS.S.to_numpy()
+        out["T"] = np.where(case["solid"], ts, tf)
+        out["g"] = np.moveaxis(np.where(case["solid"][..., None], lb.TS.g.to_numpy(), lb.TF.g.to_numpy()), -1, 0)
+    return out, time.time() - t0
+
+
+def main(argv):
+    if len(argv) < 2:
+        print(__doc__)
+        return 2
+    Solver2D, Solver3D, flag = _import_reference(argv[1])
+    only = set(argv[2:])
+    for mk in CASES:
+        case = mk()
+        if only and case["name"] not in only:
+            continue
+        out, dt = run_reference(case, Solver2D, Solver3D, flag)
+        meta = dict(cfg=case["cfg"].to_dict(), steps=case["steps"], bc_model=case["bc_model"],
+                    ref_quirk_frozen_solid_T=case["cfg"].thermal == "two_field",
+                    generator="tests/golden/make_reference_fixtures.py")
+        path = HERE / f"{case['name']}.npz"
+        np.savez_compressed(path, meta=json.dumps(meta), solid=case["solid"], rho0=case["rho"],
+                            u0=case["u"], T0=case["T"], **{k + "_ref": v for k, v in out.items()})
+        print(f"{case['name']}: {case['steps']} steps in {dt:.1f} s -> {path.name} "
+              f"({path.stat().st_size} B)")
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main(sys.argv))

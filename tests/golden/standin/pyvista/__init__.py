@@ -1,0 +1,1 @@
+"""Empty stand-in so the reference's I/O module imports (test infrastructure only)."""
