@@ -109,7 +109,9 @@ typedef struct lbm_desc {
   int32_t thermal;      /* LBM_THERMAL_* */
   int32_t pyro;         /* 1: Arrhenius pyrolysis with solid->fluid flip (needs the conjugate field) */
   int32_t half_force_velocity; /* 1: u includes F/2 (reference: 0) */
-  int32_t bulk_form;    /* 0: cell lists from 65536 cells, else tile; 1: tile; 2: cell lists */
+  int32_t bulk_form;    /* 0: cell lists from 65536 cells, else tile; 1: tile; 2: cell lists;
+                           3: dense TMA-staged tiles (3D; nx % 32, ny % 4, nz % 2 == 0;
+                           no two-field temperature) */
   double nu;            /* lattice viscosity visco*dt/dx^2 (_evolution.py:227-249) */
   double force[3];      /* body acceleration in lattice units (Guo forcing) */
   double tauT_fluid;    /* thermal relaxation time in fluid cells */
@@ -235,6 +237,18 @@ LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
 /* Lattice steps taken since lbm_init_equilibrium (tLattice counter,
  * src/LBM/LBM2D/_evolution.py:15). */
 LBM_API int64_t lbm_step_count(const lbm_handle* h);
+
+/* Bulk form the handle runs (1 tile, 2 cell lists, 3 dense TMA-staged tiles), decided
+ * by lbm_create from bulk_form, LBM_BULK and the lattice size.  No reference
+ * counterpart (Taichi picks its own loop schedule). */
+LBM_API int32_t lbm_bulk_form(const lbm_handle* h);
+
+/* Failure detection (no reference counterpart: Taichi kernels have no error status).
+ * The dense bulk form waits on an mbarrier for each staged tile; a wait gives up after
+ * `tries` tries of about a microsecond each (default 4194304, i.e. seconds), records
+ * the timeout for lbm_read_diag (LBM_ERR_TIMEOUT: the state is invalid), lets the copies
+ * it issued land and ends the block.  0 gives up at the first wait: a test of that path. */
+LBM_API int32_t lbm_set_wait_limit(lbm_handle* h, uint32_t tries);
 
 /* Count n steps (n even) that a replay of a CUDA graph captured around
  * lbm_step(h, n, flags, stream) took: capturing runs no kernel but moves the

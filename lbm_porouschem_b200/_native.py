@@ -43,7 +43,7 @@ EXPORTED = (
     "lbm_abi_version", "lbm_last_error", "lbm_required_bytes", "lbm_create", "lbm_destroy",
     "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_resume", "lbm_step", "lbm_compute_macro",
     "lbm_read_diag",
-    "lbm_step_count", "lbm_advance", "lbm_diag_noalloc", "lbm_stl_work_bytes", "lbm_voxelise_stl",
+    "lbm_step_count", "lbm_bulk_form", "lbm_set_wait_limit", "lbm_advance", "lbm_diag_noalloc", "lbm_stl_work_bytes", "lbm_voxelise_stl",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
     "lbm_batch_set_blocks",
     "lbm_nn_conv", "lbm_nn_conv_wgrad", "lbm_nn_bias_grad", "lbm_nn_flip_weights", "lbm_nn_avgpool2",
@@ -140,6 +140,10 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_read_diag.restype = i32
     lib.lbm_step_count.argtypes = [vp]
     lib.lbm_step_count.restype = i64
+    lib.lbm_bulk_form.argtypes = [vp]
+    lib.lbm_bulk_form.restype = i32
+    lib.lbm_set_wait_limit.argtypes = [vp, C.c_uint32]
+    lib.lbm_set_wait_limit.restype = i32
     lib.lbm_diag_noalloc.argtypes = [vp, C.POINTER(lbm_diag), vp]
     lib.lbm_diag_noalloc.restype = i32
     lib.lbm_batch_required_bytes.argtypes = [C.POINTER(vp), i32, vp, C.POINTER(sz)]

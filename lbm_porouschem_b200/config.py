@@ -101,7 +101,7 @@ class LatticeConfig:
     rho0: float = 1.0
     T0: float = 0.0
     sides: list = field(default_factory=lambda: [SideBC() for _ in range(6)])
-    bulk_form: str = "auto"         # "auto" (cell lists from 65536 cells) | "tile" | "list"
+    bulk_form: str = "auto"         # "auto" (cell lists from 65536 cells) | "tile" | "list" | "dense" (3D)
     viscosity: str = "constant"     # "constant" (nu) | "sutherland" (per cell from T; thermal only)
     suth_A: float = 0.0             # Sutherland: nu = suth_A TK^1.5 / (TK + suth_Ts), TK = T_ref + T_scale T
     suth_Ts: float = 0.0            #   (suth_A = As dt/dx^2 in lattice units, suth_Ts in K)
@@ -165,7 +165,7 @@ class LatticeConfig:
                      "two_field": N.LBM_THERMAL_TWOFIELD}[self.thermal]
         d.pyro = int(self.pyro)
         d.half_force_velocity = int(self.half_force_velocity)
-        d.bulk_form = {"auto": 0, "tile": 1, "list": 2}[self.bulk_form]
+        d.bulk_form = {"auto": 0, "tile": 1, "list": 2, "dense": 3}[self.bulk_form]
         d.nu = self.nu
         for i in range(3):
             d.force[i] = float(self.force[i])

@@ -1,9 +1,11 @@
 // capi_internal.cuh -- handle layout and launch templates shared by the C-ABI
 // translation unit and the per-(lattice, precision) instantiation units.
 #pragma once
+#include <cudaTypedefs.h>
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <mutex>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
@@ -12,8 +14,8 @@
 #include <vector>
 
 #include "batch_kernel.cuh"
+#include "dense_kernel.cuh"
 #include "list_kernel.cuh"
-#include "staged_kernel.cuh"
 #include "step_kernels.cuh"
 
 namespace lbm {
@@ -48,8 +50,9 @@ struct Launch {
   dim3 bc_grid;
   int bulk_blocks, bc_blocks;
   int flip_blocks;    // grid of flip_cells (pyrolysis only), 256 threads each
-  bool staged;        // bulk update by step_bulk_staged (persistent grid of bulk_blocks)
   bool list;          // bulk update by step_list (persistent grid of bulk_blocks x 128)
+  bool dense;         // bulk update by step_dense (persistent grid of bulk_blocks x kDThreads)
+  int dense_smem;     // its dynamic shared memory (two stages)
   size_t N;
   int list_base;      // first entry of the solid list (capacity of the fluid list)
   size_t list_cap;    // entries in both lists
@@ -66,6 +69,20 @@ inline int sm_count() {
     return 148;
   }
   return n;
+}
+
+// Shared memory of one stage of step_dense for this lattice's storage and physics.
+template <class S>
+inline int dense_stage_bytes_t(const lbm_desc& d) {
+  const bool th = d.thermal != LBM_THERMAL_NONE, py = d.pyro != 0;
+  if (th && py) return DenseLayout<Lattice<3>, S, true, true>::STAGE;
+  if (th) return DenseLayout<Lattice<3>, S, true, false>::STAGE;
+  return DenseLayout<Lattice<3>, S, false, false>::STAGE;
+}
+inline int dense_stage_bytes(const lbm_desc& d) {
+  return d.precision == LBM_PREC_FP16 ? dense_stage_bytes_t<__half>(d)
+                                      : (d.precision == LBM_PREC_FP64 ? dense_stage_bytes_t<double>(d)
+                                                                       : dense_stage_bytes_t<float>(d));
 }
 
 inline Launch plan(const lbm_desc& d, int tx) {
@@ -87,15 +104,6 @@ inline Launch plan(const lbm_desc& d, int tx) {
   L.bc_grid = dim3((maxcells + L.bc_threads - 1) / L.bc_threads, L.nfaces > 0 ? L.nfaces : 1, 1);
   L.bc_blocks = L.nfaces > 0 ? (int)(L.bc_grid.x * L.bc_grid.y) : 0;
   L.flip_blocks = d.pyro ? 2 * 148 : 0;
-  // staged bulk kernel (rows split into kStagedTile tiles, persistent grid): opt-in
-  // with LBM_STAGED=1; on B200 it measured slower than step_bulk (barrier-bound)
-  const char* e = getenv("LBM_STAGED");
-  L.staged = d.nx % kStagedTile == 0 && e && e[0] == '1';
-  if (L.staged) {
-    const long ntiles = (long)(d.nx / kStagedTile) * d.ny * d.nz;
-    const int per_sm = d.precision == LBM_PREC_FP64 ? 1 : 4;
-    L.bulk_blocks = (int)std::min<long>(ntiles, (long)sm_count() * per_sm);
-  }
   // cell-list bulk kernel from 65536 cells up (below, its start-up round trips
   // outweigh what it saves); LBM_BULK=tile / list forces either form
   const char* b = getenv("LBM_BULK");
@@ -103,8 +111,9 @@ inline Launch plan(const lbm_desc& d, int tx) {
   // the descriptor's bulk_form wins over LBM_BULK
   const bool force_tile = d.bulk_form == 1 || (d.bulk_form == 0 && b && std::strcmp(b, "tile") == 0);
   const bool force_list = d.bulk_form == 2 || (d.bulk_form == 0 && b && std::strcmp(b, "list") == 0);
-  if (force_list) L.staged = false;
-  L.list = !L.staged && !force_tile && (force_list || L.N >= 65536);
+  const bool force_dense = d.bulk_form == 3 || (d.bulk_form == 0 && b && std::strcmp(b, "dense") == 0);
+  L.list = !force_tile && !force_dense && (force_list || L.N >= 65536);
+  L.dense = force_dense;
   L.list_base = (int)((L.N + 64 + 31) / 32 * 32);
   L.list_cap = 2 * (size_t)L.list_base;
   L.list_nbb = (int)((L.N + kListChunk - 1) / kListChunk);
@@ -113,7 +122,21 @@ inline Launch plan(const lbm_desc& d, int tx) {
     const long chunks = (long)(L.N / 32) + 8;
     L.bulk_blocks = (int)std::max<long>(1, std::min<long>((chunks + 3) / 4, (long)sm_count() * per_sm));
   }
+  if (L.dense) {
+    const long ntiles = (long)(d.nx / kDTX) * (d.ny / kDTY) * (d.nz / kDTZ);
+    const int per_sm = d.precision == LBM_PREC_FP64 ? DenseCTAs<double>::v : DenseCTAs<float>::v;
+    L.bulk_blocks = (int)std::max<long>(1, std::min<long>(ntiles, (long)sm_count() * per_sm));
+    L.dense_smem = 2 * dense_stage_bytes(d);
+  }
   return L;
+}
+
+// Why the dense form cannot run this lattice (nullptr: it can).
+inline const char* dense_unsupported(const lbm_desc& d) {
+  if (d.dim != 3) return "the dense bulk form is 3D only";
+  if (d.nx % kDTX || d.ny % kDTY || d.nz % kDTZ) return "the dense bulk form needs nx % 32 == 0, ny % 4 == 0, nz % 2 == 0";
+  if (d.thermal == LBM_THERMAL_TWOFIELD) return "the dense bulk form runs the conjugate temperature field only";
+  return nullptr;
 }
 
 // Threads per block along x for the bulk kernel.  LBM_BLOCK_X (32..256, a
@@ -144,6 +167,11 @@ struct lbm_handle {
   cudaStream_t side = nullptr;
   cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   bool side_tried = false;
+  // dense form: tensor maps over the bound F / G / MASK buffers (rebuilt when a buffer
+  // is rebound) and the bound of its mbarrier waits
+  lbm::DenseMaps maps{};
+  const void* maps_for[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  uint32_t wait_spins = lbm::kDefaultWaitSpins;
 };
 
 // A batch of lattices stepped together (batch_kernel.cuh).  Its device tables
@@ -177,11 +205,12 @@ inline size_t list_offset(const Launch& L) {
   return ((scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16 + 255) / 256 * 256;
 }
 inline size_t list_bytes(const Launch& L) {
+  if (L.dense) return (size_t)kLhSlots * 4 + 2 * L.N * 4;  // header | flip lists [2][N]
   if (!L.list) return 0;
   return (size_t)kLhSlots * 4 + (size_t)4 * L.list_nbb * 4 + 2 * L.list_cap * 4 + L.N * 4 + 2 * L.N * 4;
 }
 inline size_t scratch_bytes(const Launch& L) {
-  if (L.list) return list_offset(L) + list_bytes(L);
+  if (L.list || L.dense) return list_offset(L) + list_bytes(L);
   return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16;
 }
 inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
@@ -201,7 +230,9 @@ inline int* scratch_lblk(lbm_handle* h) { return scratch_lhdr(h) + kLhSlots; }
 inline uint32_t* scratch_ent_c(lbm_handle* h) { return (uint32_t*)(scratch_lblk(h) + 4 * (size_t)h->L.list_nbb); }
 inline uint32_t* scratch_ent_b(lbm_handle* h) { return scratch_ent_c(h) + h->L.list_cap; }
 inline int* scratch_pos(lbm_handle* h) { return (int*)(scratch_ent_b(h) + h->L.list_cap); }
-inline int* scratch_flips(lbm_handle* h) { return scratch_pos(h) + h->N; }
+inline int* scratch_flips(lbm_handle* h) {
+  return h->L.dense ? scratch_lhdr(h) + kLhSlots : scratch_pos(h) + h->N;
+}
 // Two-stage deterministic reduction of the block partials into scratch_final().
 inline void launch_reduce(lbm_handle* h, cudaStream_t st) {
   reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), partial_rows(h->L), scratch_stage1(h));
@@ -267,7 +298,98 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
     p.pos = scratch_pos(h);
     p.flips = scratch_flips(h);
   }
+  if (h->L.dense && h->ptr[LBM_FIELD_SCRATCH]) {  // flip lists only
+    p.lhdr = scratch_lhdr(h);
+    p.flips = scratch_flips(h);
+  }
+  p.wait_spins = h->wait_spins;
   return p;
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link to libcuda).
+inline PFN_cuTensorMapEncodeTiled_v12000 tmap_encoder() {
+  static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
+  static std::once_flag once;
+  std::call_once(once, [] {
+    void* f = nullptr;
+    cudaDriverEntryPointQueryResult q{};
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &f, cudaEnableDefault, &q) == cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      fn = reinterpret_cast<PFN_cuTensorMapEncodeTiled_v12000>(f);
+    else
+      cudaGetLastError();
+  });
+  return fn;
+}
+
+// Tensor maps of the dense form over the bound buffers (kept until a buffer is rebound).
+// Populations: 4-D (x, y, z, plane) with planes = 2 Q (both halves), one flow map per box
+// shape (bx, kDTY [+1], kDTZ [+1], 1); mask: 3-D bytes, box (64, kDTY + 2, kDTZ + 2); gas
+// release: 4-D (x, y, z, half) of the compute type, box (bx, kDTY + 2, kDTZ + 2, 1);
+// reactive fraction: 3-D, box (32, kDTY, kDTZ).  Out-of-bounds box parts read zeros.
+template <class S>
+int encode_dense_maps(lbm_handle* h) {
+  if (h->maps_for[0] == h->ptr[LBM_FIELD_F] && h->maps_for[1] == h->ptr[LBM_FIELD_G] &&
+      h->maps_for[2] == h->ptr[LBM_FIELD_MASK] && h->maps_for[3] == h->ptr[LBM_FIELD_REL] &&
+      h->maps_for[4] == h->ptr[LBM_FIELD_ALPHA])
+    return LBM_OK;
+  PFN_cuTensorMapEncodeTiled_v12000 enc = tmap_encoder();
+  if (!enc) return fail(LBM_ERR_CUDA, "cuTensorMapEncodeTiled is not available from the driver");
+  const lbm_desc& d = h->d;
+  const cuuint64_t nx = (cuuint64_t)d.nx, ny = (cuuint64_t)d.ny, nz = (cuuint64_t)d.nz, es = sizeof(S);
+  const CUtensorMapDataType dt = sizeof(S) == 2 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT16
+                                                : (sizeof(S) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64
+                                                                  : CU_TENSOR_MAP_DATA_TYPE_FLOAT32);
+  using LY = DenseLayout<Lattice<3>, S, true, true>;
+  using C = typename Store<S>::C;
+  const CUtensorMapDataType dtc = sizeof(C) == 8 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT64 : CU_TENSOR_MAP_DATA_TYPE_FLOAT32;
+  auto map4 = [&](CUtensorMap* m, CUtensorMapDataType t, cuuint64_t e, void* base, int planes, int bx, int by,
+                  int bz) -> CUresult {
+    const cuuint64_t dims[4] = {nx, ny, nz, (cuuint64_t)planes};
+    const cuuint64_t strides[3] = {nx * e, nx * ny * e, nx * ny * nz * e};
+    const cuuint32_t box[4] = {(cuuint32_t)bx, (cuuint32_t)by, (cuuint32_t)bz, 1};
+    const cuuint32_t estr[4] = {1, 1, 1, 1};
+    return enc(m, t, 4, base, dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+               CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  };
+  CUresult r = CUDA_SUCCESS;
+  for (int i = 0; i < 8 && r == CUDA_SUCCESS; ++i)  // f[wide << 2 | ey << 1 | ez]
+    r = map4(&h->maps.f[i], dt, es, h->ptr[LBM_FIELD_F], 2 * 19, (i & 4) ? LY::BXW : LY::BXN,
+             kDTY + ((i >> 1) & 1), kDTZ + (i & 1));
+  if (r == CUDA_SUCCESS && h->ptr[LBM_FIELD_G]) {
+    r = map4(&h->maps.g_wide, dt, es, h->ptr[LBM_FIELD_G], 2 * 7, LY::BXW, kDTY, kDTZ);
+    if (r == CUDA_SUCCESS) r = map4(&h->maps.g_narrow, dt, es, h->ptr[LBM_FIELD_G], 2 * 7, LY::BXN, kDTY, kDTZ);
+  }
+  if (r == CUDA_SUCCESS && d.pyro && h->ptr[LBM_FIELD_REL] && h->ptr[LBM_FIELD_ALPHA]) {
+    r = map4(&h->maps.rel, dtc, sizeof(C), h->ptr[LBM_FIELD_REL], 2, LY::RX, LY::MY, LY::MZ);
+    if (r == CUDA_SUCCESS) {
+      const cuuint64_t dims[3] = {nx, ny, nz};
+      const cuuint64_t strides[2] = {nx * sizeof(C), nx * ny * sizeof(C)};
+      const cuuint32_t box[3] = {(cuuint32_t)kDTX, (cuuint32_t)kDTY, (cuuint32_t)kDTZ};
+      const cuuint32_t estr[3] = {1, 1, 1};
+      r = enc(&h->maps.alpha, dtc, 3, h->ptr[LBM_FIELD_ALPHA], dims, strides, box, estr, CU_TENSOR_MAP_INTERLEAVE_NONE,
+              CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    }
+  }
+  if (r == CUDA_SUCCESS) {
+    const cuuint64_t dims[3] = {nx, ny, nz};
+    const cuuint64_t strides[2] = {nx, nx * ny};
+    const cuuint32_t box[3] = {(cuuint32_t)LY::MX, (cuuint32_t)LY::MY, (cuuint32_t)LY::MZ};
+    const cuuint32_t estr[3] = {1, 1, 1};
+    r = enc(&h->maps.mask, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, h->ptr[LBM_FIELD_MASK], dims, strides, box, estr,
+            CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+            CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+  }
+  if (r != CUDA_SUCCESS) {
+    for (auto& q : h->maps_for) q = nullptr;
+    return fail(LBM_ERR_CUDA, "cuTensorMapEncodeTiled failed with CUresult " + std::to_string((int)r));
+  }
+  h->maps_for[0] = h->ptr[LBM_FIELD_F];
+  h->maps_for[1] = h->ptr[LBM_FIELD_G];
+  h->maps_for[2] = h->ptr[LBM_FIELD_MASK];
+  h->maps_for[3] = h->ptr[LBM_FIELD_REL];
+  h->maps_for[4] = h->ptr[LBM_FIELD_ALPHA];
+  return LBM_OK;
 }
 
 // Launch one step (bulk + boundary) for handle h; defined per (lattice, storage)

@@ -2,6 +2,8 @@
 // by the inst_*.cu translation units (split so that the kernels compile in
 // parallel).
 #pragma once
+#include <atomic>
+
 #include "capi_internal.cuh"
 
 namespace lbm {
@@ -14,18 +16,28 @@ inline int collision_code(const lbm_desc& d) {
   return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0);
 }
 
+// Dynamic shared memory above the 48 KB default is a per-device attribute of a kernel:
+// opt in once per device ordinal (one bit per device in `done`, which each call site keeps
+// per kernel instantiation), again after a failure; the launch that follows then reports
+// the error through cudaGetLastError.
+template <class K>
+inline void opt_in_smem(std::atomic<unsigned long long>& done, K* kernel, int bytes) {
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return;
+  const unsigned long long bit = dev < 64 ? 1ull << dev : 0ull;
+  if (bit && (done.load(std::memory_order_acquire) & bit)) return;
+  if (cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes) == cudaSuccess && bit)
+    done.fetch_or(bit, std::memory_order_acq_rel);
+}
+
 template <class Lt, class S, int COLL, int THERM, int MODE>
 static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st) {
   constexpr size_t smem = list_smem_bytes<Lt, S>(128);
   if (smem > 0) {
     // opt in above the 48 KB default: with the static reduction buffer the total can
     // pass it even when the stages alone do not
-    static bool attr_set = false;  // one attribute call per process and instantiation
-    if (!attr_set) {
-      cudaFuncSetAttribute(step_list<Lt, S, COLL, THERM, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                           (int)smem);
-      attr_set = true;
-    }
+    static std::atomic<unsigned long long> done{0};
+    opt_in_smem(done, step_list<Lt, S, COLL, THERM, MODE>, (int)smem);
   }
   step_list<Lt, S, COLL, THERM, MODE><<<L.bulk_blocks, 128, smem, st>>>(p);
 }
@@ -35,7 +47,7 @@ static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st
 inline void ensure_side_stream(lbm_handle* h) {
   if (h->side_tried) return;
   h->side_tried = true;
-  if (!(h->L.list && h->L.nfaces > 0)) return;
+  if (!((h->L.list || h->L.dense) && h->L.nfaces > 0)) return;
   if (cudaStreamCreateWithFlags(&h->side, cudaStreamNonBlocking) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
       cudaEventCreateWithFlags(&h->ev_join, cudaEventDisableTiming) != cudaSuccess) {
@@ -44,6 +56,15 @@ inline void ensure_side_stream(lbm_handle* h) {
     if (h->side) cudaStreamDestroy(h->side);
     h->side = nullptr;
     h->ev_fork = h->ev_join = nullptr;
+  }
+}
+
+template <class Lt, class S, int COLL, int THERM, int MODE>
+static void launch_dense(lbm_handle* h, const StepParams<S>& p, cudaStream_t st) {
+  if constexpr (Lt::DIM == 3 && THERM != 3) {
+    static std::atomic<unsigned long long> done{0};
+    opt_in_smem(done, step_dense<Lt, S, COLL, THERM, MODE>, h->L.dense_smem);
+    step_dense<Lt, S, COLL, THERM, MODE><<<h->L.bulk_blocks, kDThreads, h->L.dense_smem, st>>>(p, h->maps);
   }
 }
 
@@ -58,21 +79,15 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   // input half only and write disjoint slots, partial rows apart), so it runs on the
   // second stream and its blocks take the SMs that the persistent list kernel's blocks
   // leave as they finish; flip_cells waits for both
-  const bool fork = L.list && L.nfaces > 0 && h->side != nullptr;
+  const bool fork = (L.list || L.dense) && L.nfaces > 0 && h->side != nullptr;
   if (fork) {
     cudaEventRecord(h->ev_fork, st);
     cudaStreamWaitEvent(h->side, h->ev_fork, 0);
   }
-  if (L.staged) {
-    using LY = StagedLayout<Lt, S, kStagedTile>;
-    constexpr size_t smem = (size_t)kStagedStages * LY::STAGE_BYTES;
-    static bool attr_set = false;  // one attribute call per process and instantiation
-    if (!attr_set) {
-      cudaFuncSetAttribute(step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages>,
-                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      attr_set = true;
-    }
-    step_bulk_staged<Lt, S, COLL, THERM, kStagedTile, kStagedStages><<<L.bulk_blocks, kStagedTile, smem, st>>>(p);
+  if (L.dense) {
+    if (p.flags & kStepPeek) launch_dense<Lt, S, COLL, THERM, 2>(h, p, st);
+    else if (p.flags) launch_dense<Lt, S, COLL, THERM, 1>(h, p, st);
+    else launch_dense<Lt, S, COLL, THERM, 0>(h, p, st);
   } else if (L.list) {
     if (p.flags & kStepPeek) launch_list<Lt, S, COLL, THERM, 2>(L, p, st);
     else if (p.flags) launch_list<Lt, S, COLL, THERM, 1>(L, p, st);
@@ -81,7 +96,7 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
     step_bulk<Lt, S, COLL, THERM><<<L.grid, L.block, 0, st>>>(p);
   }
   if (L.nfaces > 0) {
-    p.block_offset = L.bulk_blocks;
+    p.block_offset = L.bulk_blocks;  // one partial row per bulk block, then the boundary blocks
     const int4 f01 = make_int4(L.faces[0], L.faces[1], L.faces[2], L.faces[3]);
     const int2 f2 = make_int2(L.faces[4], L.faces[5]);
     step_boundary<Lt, S, COLL, THERM><<<L.bc_grid, L.bc_threads, 0, fork ? h->side : st>>>(p, f01, f2);
@@ -91,7 +106,8 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
     cudaStreamWaitEvent(st, h->ev_join, 0);
   }
   if constexpr (THERM == 2) {
-    // after the boundary kernel: it moves mirrored populations of boundary cells too
+    // after the boundary kernel: the flipped cells' new populations go in after every
+    // other store of the pass
     p.block_offset = L.bulk_blocks + L.bc_blocks;
     flip_cells<Lt, S, COLL, THERM><<<L.flip_blocks, 256, 0, st>>>(p);
   }
@@ -101,6 +117,12 @@ template <class Lt, class S>
 int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const int coll = collision_code(h->d);
   const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
+  if (h->L.dense) {
+    const char* why = dense_unsupported(h->d);
+    if (why) return fail(LBM_ERR_ARG, why);
+    const int rc = encode_dense_maps<S>(h);
+    if (rc) return rc;
+  }
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_step<Lt, S, C_, T_>(h, p, st); return LBM_OK; }
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)

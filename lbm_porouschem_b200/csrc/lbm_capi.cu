@@ -34,7 +34,11 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "unknown collision");
   if (d->precision < LBM_PREC_FP32 || d->precision > LBM_PREC_FP64)
     return fail(LBM_ERR_ARG, "unknown precision");
-  if (d->bulk_form < 0 || d->bulk_form > 2) return fail(LBM_ERR_ARG, "bulk_form must be 0, 1 or 2");
+  if (d->bulk_form < 0 || d->bulk_form > 3) return fail(LBM_ERR_ARG, "bulk_form must be 0, 1, 2 or 3");
+  if (d->bulk_form == 3) {
+    const char* why = dense_unsupported(*d);
+    if (why) return fail(LBM_ERR_ARG, why);
+  }
   if (d->eos != LBM_EOS_IDEAL_GAS && d->eos != LBM_EOS_INCOMPRESSIBLE)
     return fail(LBM_ERR_ARG, "unknown eos");
   if (d->thermal != LBM_THERMAL_NONE && d->thermal != LBM_THERMAL_CONJUGATE && d->thermal != LBM_THERMAL_TWOFIELD)
@@ -146,6 +150,10 @@ static int build_lists_t(lbm_handle* h, cudaStream_t st) {
   return LBM_OK;
 }
 static int build_lists(lbm_handle* h, cudaStream_t st) {
+  if (h->L.dense) {  // flip lists only: both empty
+    LBM_CUDA_TRY(cudaMemsetAsync(scratch_lhdr(h), 0, kLhSlots * sizeof(int), st));
+    return LBM_OK;
+  }
   if (!h->L.list) return LBM_OK;
   return h->d.dim == 2 ? build_lists_t<Lattice<2>>(h, st) : build_lists_t<Lattice<3>>(h, st);
 }
@@ -227,6 +235,17 @@ int32_t lbm_bind(lbm_handle* h, int32_t field, void* ptr, size_t bytes) {
 }
 
 int64_t lbm_step_count(const lbm_handle* h) { return h ? h->step : -1; }
+
+int32_t lbm_set_wait_limit(lbm_handle* h, uint32_t tries) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  h->wait_spins = tries;
+  return LBM_OK;
+}
+
+int32_t lbm_bulk_form(const lbm_handle* h) {
+  if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
+  return h->L.dense ? 3 : (h->L.list ? 2 : 1);
+}
 
 }  // extern "C"
 

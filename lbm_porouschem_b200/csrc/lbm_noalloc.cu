@@ -29,16 +29,20 @@ constexpr size_t kDiagDoubles = kFinalOff + kNumDiag;
 // (kDiagDoubles * 8 bytes, about 2.6 MB, plus the side records).
 static __device__ __align__(256) double g_noalloc_diag[kDiagDoubles];
 static __device__ __align__(256) lbm_side_desc g_noalloc_sides[6];
+// Kernel error flags of a call whose lattice has no SCRATCH buffer bound (tile form):
+// bit 0 a bounded wait gave up, bit 1 the fluid cell list overflowed.
+static __device__ __align__(256) int g_noalloc_err[1];
 
-// Device addresses of the two arrays, looked up once per device with that
+// Device addresses of the three arrays, looked up once per device with that
 // device current (in host code the array names are host-side stand-ins, not
 // device addresses).
 constexpr int kMaxDevices = 64;
 std::mutex g_mu;
 double* g_diag_dev[kMaxDevices] = {};
 lbm_side_desc* g_sides_dev[kMaxDevices] = {};
+int* g_err_dev[kMaxDevices] = {};
 
-int device_arrays(double** diag, lbm_side_desc** sides) {
+int device_arrays(double** diag, lbm_side_desc** sides, int** err) {
   int dev = -1;
   LBM_CUDA_TRY(cudaGetDevice(&dev));
   if (dev < 0 || dev >= kMaxDevices) return fail(LBM_ERR_ARG, "device ordinal out of range");
@@ -46,13 +50,17 @@ int device_arrays(double** diag, lbm_side_desc** sides) {
   if (!g_diag_dev[dev]) {
     void* pd = nullptr;
     void* ps = nullptr;
+    void* pe = nullptr;
     LBM_CUDA_TRY(cudaGetSymbolAddress(&pd, g_noalloc_diag));
     LBM_CUDA_TRY(cudaGetSymbolAddress(&ps, g_noalloc_sides));
+    LBM_CUDA_TRY(cudaGetSymbolAddress(&pe, g_noalloc_err));
     g_diag_dev[dev] = (double*)pd;
     g_sides_dev[dev] = (lbm_side_desc*)ps;
+    g_err_dev[dev] = (int*)pe;
   }
   *diag = g_diag_dev[dev];
   *sides = g_sides_dev[dev];
+  *err = g_err_dev[dev];
   return LBM_OK;
 }
 
@@ -85,10 +93,16 @@ extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) 
     return fail(LBM_ERR_UNBOUND, "lbm_diag_noalloc needs SCRATCH bound: it holds the cell lists of the lattice");
   double* diag = nullptr;
   lbm_side_desc* sides = nullptr;
-  int rc = device_arrays(&diag, &sides);
+  int* static_err = nullptr;
+  int rc = device_arrays(&diag, &sides, &static_err);
   if (rc) return rc;
   cudaStream_t st = (cudaStream_t)stream;
   LBM_CUDA_TRY(cudaMemcpyAsync(sides, h->d.side, sizeof(h->d.side), cudaMemcpyHostToDevice, st));
+  // Error flags: with SCRATCH bound they are the lattice's own, which also hold what the
+  // earlier steps recorded (a state they invalidated stays invalid); without it, this
+  // call's flags go to the static word, cleared first.
+  int* err = h->ptr[LBM_FIELD_SCRATCH] ? scratch_err(h) : static_err;
+  if (err == static_err) LBM_CUDA_TRY(cudaMemsetAsync(static_err, 0, sizeof(int), st));
   const int buf = (int)((h->step - 1) & 1);
   rc = with_types_na(h, [&](auto lat, auto s) -> int {
     using Lt = decltype(lat);
@@ -97,6 +111,7 @@ extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) 
     p.partials = diag;
     p.partial_rows = rows;
     p.sides = sides;
+    p.err = err;
     p.flags = LBM_STEP_DIAG | kStepPeek;
     return dispatch_step<Lt, S>(h, p, st);
   });
@@ -106,8 +121,13 @@ extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) 
   reduce_diag_stage2<<<1, 256, 0, st>>>(diag + kStage1Off, kStage1Blocks, diag + kFinalOff);
   LBM_CUDA_TRY(cudaGetLastError());
   double v[kNumDiag];
+  int flags = 0;
   LBM_CUDA_TRY(cudaMemcpyAsync(v, diag + kFinalOff, sizeof(v), cudaMemcpyDeviceToHost, st));
+  LBM_CUDA_TRY(cudaMemcpyAsync(&flags, err, sizeof(int), cudaMemcpyDeviceToHost, st));
   LBM_CUDA_TRY(cudaStreamSynchronize(st));
+  // the same mapping as lbm_read_diag
+  if (flags & 1) return fail(LBM_ERR_TIMEOUT, "a staged-load wait in the step kernel timed out; the state is invalid");
+  if (flags & 2) return fail(LBM_ERR_CUDA, "the fluid cell list overflowed; the state is invalid");
   out->mass = v[0]; out->energy = v[1]; out->solid_alpha = v[2]; out->umax = v[3];
   out->Tmin = v[4]; out->Tmax = v[5]; out->nonfinite = v[6]; out->nfluid = v[7];
   out->res_num = v[8]; out->res_den = v[9];

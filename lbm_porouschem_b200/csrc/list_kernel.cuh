@@ -230,7 +230,9 @@ template <class L, class S> struct ListStaged { static constexpr bool value = L:
 // stage sits at base[k * stride] (stride = threads per block, so that the
 // threads of a warp read consecutive words).  Per stage and thread: f[Q] | g[QT] |
 // rel[Q] (gas release of the solid neighbour c - e_k, zero where that neighbour
-// is fluid) | alpha (reactive fraction of a solid cell).
+// is fluid) | alpha (reactive fraction of a solid cell).  The copies take the
+// bounce-back slots (the cell's own slot of the opposite direction) where the link
+// needs them, so the staged values are the post-stream populations themselves.
 template <class L, class S>
 struct StagedPull {
   using C = typename Store<S>::C;
@@ -248,7 +250,9 @@ struct StagedPull {
       F[k] = v;
     });
   }
-  __device__ __forceinline__ void thermal(const StepParams<S>&, const Nbhd&, int, C G[L::QT]) const {
+  // the copies already resolved the adiabatic links of the two-field mode
+  template <bool ADIA, bool RT>
+  __device__ __forceinline__ void thermal(const StepParams<S>&, const Nbhd&, int, uint32_t, bool, C G[L::QT]) const {
     static_for<L::QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       G[k] = (C)sf[(kG + k) * stride];
@@ -349,16 +353,20 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ St
         const int c = (int)ec;
         const Nbhd nb = nbhd(c, base < (fl ? fg : sg));
         S* sf = stage0 + st * stage_elems;
+        // neighbour-solid bits of the pass being run: the entry's, or for a peek pass
+        // (which recomputes the last pass before flip_cells<> updated the entries) the
+        // mask's at that parity
+        const uint32_t bits = peek ? Kern<L, S>::neighbour_bits(p, nb, p.par) : (eb & ~(kEntReactive | kEntDead));
         if (fl) {
           static_for<Q>([&](auto kk) {
             constexpr int k = decltype(kk)::value;
             const int src = k == 0 ? c : nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-            const S* g = p.fA + (size_t)k * p.N + src;
+            const bool bb = k > 0 && ((bits >> L::opp(k)) & 1);
+            const S* g = bb ? p.fA + (size_t)L::opp(k) * p.N + c : p.fA + (size_t)k * p.N + src;
             if constexpr (sizeof(S) == 8) cp_async8(sf + k * stride, g); else cp_async4(sf + k * stride, g);
             if constexpr (PYRO && k > 0) {
-              // gas released by a solid neighbour c - e_k (bit opp(k) of the entry; a
-              // peek pass takes its bits from the mask, so it copies every value)
-              const unsigned nbytes = (peek || ((eb >> L::opp(k)) & 1)) ? (unsigned)sizeof(S) : 0u;
+              // gas released by a solid neighbour c - e_k (zero where it is fluid)
+              const unsigned nbytes = bb ? (unsigned)sizeof(S) : 0u;
               const S* r = (const S*)p.relA + src;
               if constexpr (sizeof(S) == 8) cp_async8_zfill(sf + (SP::kR + k) * stride, r, nbytes);
               else cp_async4_zfill(sf + (SP::kR + k) * stride, r, nbytes);
@@ -372,10 +380,12 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ St
         }
         if constexpr (THERMAL) {
           S* sgp = sf + SP::kG * stride;
+          const bool adia = THERM == 3 || p.adiabatic;  // two-field: links across phases bounce
           static_for<QT>([&](auto kk) {
             constexpr int k = decltype(kk)::value;
             const int src = k == 0 ? c : nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-            const S* g = p.gA + (size_t)k * p.N + src;
+            const bool bb = k > 0 && adia && ((bits >> L::opp(k)) & 1) != (uint32_t)!fl;
+            const S* g = bb ? p.gA + (size_t)L::opp(k) * p.N + c : p.gA + (size_t)k * p.N + src;
             if constexpr (sizeof(S) == 8) cp_async8(sgp + k * stride, g); else cp_async4(sgp + k * stride, g);
           });
         }
@@ -424,7 +434,7 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ St
         const SP src{stage0 + st * stage_elems, stride};
         solid_next = cell_update<L, S, COLL, THERM>(p, cacc, diag, peek, c, nb, nbits, solid, reactive, mk, src);
       } else {
-        // the ordinary step takes store_thermal<>'s run-time form (fewer spills)
+        // the ordinary step takes pull_thermal<>'s run-time form (fewer spills)
         solid_next = cell_update<L, S, COLL, THERM, GlobalPull<L, S>, MODE == 0>(p, cacc, diag, peek, c, nb, nbits,
                                                                                  solid, reactive, mk);
       }

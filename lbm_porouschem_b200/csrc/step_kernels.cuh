@@ -19,12 +19,14 @@
 //   alpha[c]       reactive fraction (compute precision; solid cells, in place)
 //   rel[buf][c]    gas release per unit lattice weight (reacting solid cells)
 //
-// Bounce-back by mirror stores.  Solid cells carry no flow populations.  When
-// fluid cell c collides and its neighbour c+e_k is solid, the outgoing
-// population f*_k(c) is stored in the solid neighbour's slot f[opp k][c+e_k]:
-// that is exactly the slot cell c pulls direction opp(k) from on the next
-// step, so every pull is an unconditional load f[k][c-e_k] and the halfway
-// bounce-back needs no mask test before the loads are issued.
+// Bounce-back by own slots.  Every cell stores its post-collision populations in its
+// own slots f[k][c]; solid cells carry no flow populations (their flow slots are never
+// read).  A fluid cell pulls direction k from f[k][c-e_k]; when c-e_k is solid, the
+// halfway bounce-back value is the cell's own post-collision population of direction
+// opp(k) from the last pass, f[opp k][c].  So every pull is one load whose address
+// depends on one link bit, every store goes to the cell's own slots, and a warp's
+// stores of a row cover whole sectors when its solid lanes store too (the dense
+// kernel stores zeros there).
 #pragma once
 #include <cuda_fp16.h>
 #include <math.h>
@@ -119,7 +121,7 @@ struct StepParams {
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
-  int adiabatic;   // two-field temperature (store_thermal<>'s run-time form)
+  int adiabatic;   // two-field temperature (pull_thermal<>'s run-time form)
   double* partials;    // SoA: partials[i * partial_rows + block]
   int partial_rows;
   int block_offset;
@@ -128,7 +130,8 @@ struct StepParams {
   C* T_out;
   float* uprev;
   C* inlet;        // flow-rate inlet state (LBM_FIELD_INLET), null without one
-  int* err;        // set to 1 when a bounded wait gives up
+  int* err;        // bit 0: a bounded wait gave up; bit 1: the fluid list overflowed
+  unsigned wait_spins;  // tries of a bounded mbarrier wait (dense kernel) before it gives up
   // cell lists (step_list<>): entry cell index / neighbour-solid bits, the entry
   // of each cell (-1: none) and the list header (kLh* slots)
   uint32_t* ent_c;
@@ -219,9 +222,11 @@ struct Kern {
     return b;
   }
 
-  // Post-stream flow populations of fluid cell c: unconditional pulls (mirror
-  // slots hold the bounced populations) plus the gas released by reacting
-  // solid neighbours (pull direction k comes from c - e_k = c + e_opp(k)).
+  // Post-stream flow populations of fluid cell c.  Pull direction k comes from
+  // c - e_k = c + e_opp(k) (bit opp(k) of nbits set if that cell is solid): the
+  // neighbour's slot f[k][c-e_k], or at a solid neighbour the halfway bounce-back,
+  // c's own slot f[opp k][c] (same FP16 shift: w(k) = w(opp k)), plus the gas a
+  // reacting solid neighbour released along that link.
   template <bool PYRO>
   __device__ __forceinline__ static void pull_flow(const P& p, const Nbhd& nb, int c, uint32_t nbits, C F[Q]) {
     static_for<Q>([&](auto kk) {
@@ -230,21 +235,39 @@ struct Kern {
         F[0] = Store<S>::ld(p.fA, c, fshift<L, S, 0>(p));
       } else {
         const int src = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-        C v = Store<S>::ld(p.fA, (size_t)k * p.N + src, fshift<L, S, k>(p));
+        const bool bb = (nbits >> L::opp(k)) & 1;
+        const size_t idx = bb ? (size_t)L::opp(k) * p.N + c : (size_t)k * p.N + src;
+        C v = Store<S>::ld(p.fA, idx, fshift<L, S, k>(p));
         if constexpr (PYRO) {
-          if ((nbits >> L::opp(k)) & 1) v += p.relA[src] * (C)L::w(k);
+          if (bb) v += p.relA[src] * (C)L::w(k);
         }
         F[k] = v;
       }
     });
   }
 
-  // Post-stream temperature populations (conjugate mode streams through solids).
-  __device__ __forceinline__ static void pull_thermal(const P& p, const Nbhd& nb, int c, C G[QT]) {
+  // Post-stream temperature populations.  Conjugate mode streams through solids.  In
+  // the two-field mode (the reference's TF / TS, which never exchange heat across a
+  // binary mask, src/LBM/LBM2D/_evolution.py:67-95) a link to a cell of the other phase
+  // is adiabatic: the population bounces back, i.e. comes from c's own slot of the
+  // opposite direction.  ADIA selects that at compile time, RT tests p.adiabatic at run
+  // time instead (the ordinary step of the list kernel; fewer registers there).
+  // nbits: bit j set if c + e_j is solid; solid: c itself.
+  template <bool ADIA = false, bool RT = false>
+  __device__ __forceinline__ static void pull_thermal(const P& p, const Nbhd& nb, int c, uint32_t nbits,
+                                                      bool solid, C G[QT]) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      const int src = (k == 0) ? c : nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-      G[k] = Store<S>::ld(p.gA, (size_t)k * p.N + src, gshift<L, S, k>(p));
+      if constexpr (k == 0) {
+        G[0] = Store<S>::ld(p.gA, c, gshift<L, S, 0>(p));
+      } else {
+        size_t idx = (size_t)k * p.N + nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
+        if constexpr (ADIA || RT) {
+          if ((ADIA || p.adiabatic) && ((nbits >> L::opp(k)) & 1) != (uint32_t)solid)
+            idx = (size_t)L::opp(k) * p.N + c;
+        }
+        G[k] = Store<S>::ld(p.gA, idx, gshift<L, S, k>(p));
+      }
     });
   }
 
@@ -444,44 +467,19 @@ struct Kern {
     });
   }
 
-  // Store post-collision flow populations; a population headed for a solid
-  // neighbour (bit k of sbits) goes to the neighbour's mirror slot opp(k).
-  __device__ __forceinline__ static void store_flow(const P& p, const Nbhd& nb, int c, uint32_t sbits,
-                                                    const C F[Q]) {
+  // Store post-collision flow populations in the cell's own slots.
+  __device__ __forceinline__ static void store_flow(const P& p, int c, const C F[Q]) {
     static_for<Q>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      if constexpr (k == 0) {
-        Store<S>::st(p.fB, c, F[0], fshift<L, S, 0>(p));
-      } else {
-        const size_t idx = ((sbits >> k) & 1)
-                               ? (size_t)L::opp(k) * p.N + nb.at(L::ex(k), L::ey(k), L::ez(k))
-                               : (size_t)k * p.N + c;
-        Store<S>::st(p.fB, idx, F[k], fshift<L, S, k>(p));
-      }
+      Store<S>::st(p.fB, (size_t)k * p.N + c, F[k], fshift<L, S, k>(p));
     });
   }
-  // Post-collision temperature populations of cell c.  Two-field mode (the
-  // reference's TF / TS, which never exchange heat across a binary mask): a link
-  // to a cell of the other phase is adiabatic, so c stores its population in the
-  // slot the neighbour would have filled, f[opp k][c+e_k], which c pulls back next
-  // step; the neighbour does the same into f[k][c].  Every slot is still written
-  // once and every pull stays unconditional.  nbits: bit k set if c + e_k is solid.
-  // ADIA (the two-field kernels) selects the adiabatic links at compile time; RT
-  // tests p.adiabatic at run time instead.  The run-time form is what the ordinary
-  // step of the list kernel uses: with it that loop is register-allocated with fewer
-  // spills (256^3 D3Q19-MRT + D3Q7 + pyrolysis, FP32: 11.7 against 11.3 GLUPS), while
-  // in the diagnostics step it costs spills that nearly double the time.
-  template <bool ADIA, bool RT = false>
-  __device__ __forceinline__ static void store_thermal(const P& p, const Nbhd& nb, int c, const C G[QT],
-                                                       uint32_t nbits, bool solid) {
+  // Post-collision temperature populations of cell c, in its own slots (the adiabatic
+  // links of the two-field mode are resolved by the pull).
+  __device__ __forceinline__ static void store_thermal(const P& p, int c, const C G[QT]) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      size_t idx = (size_t)k * p.N + c;
-      if constexpr ((ADIA || RT) && k > 0) {
-        if ((ADIA || p.adiabatic) && ((nbits >> k) & 1) != (uint32_t)solid)
-          idx = (size_t)L::opp(k) * p.N + nb.at(L::ex(k), L::ey(k), L::ez(k));
-      }
-      Store<S>::st(p.gB, idx, G[k], gshift<L, S, k>(p));
+      Store<S>::st(p.gB, (size_t)k * p.N + c, G[k], gshift<L, S, k>(p));
     });
   }
 
@@ -676,8 +674,10 @@ struct GlobalPull {
                                        C F[L::Q]) const {
     Kern<L, S>::template pull_flow<PYRO>(p, nb, c, nbits, F);
   }
-  __device__ __forceinline__ void thermal(const StepParams<S>& p, const Nbhd& nb, int c, C G[L::QT]) const {
-    Kern<L, S>::pull_thermal(p, nb, c, G);
+  template <bool ADIA, bool RT>
+  __device__ __forceinline__ void thermal(const StepParams<S>& p, const Nbhd& nb, int c, uint32_t nbits, bool solid,
+                                          C G[L::QT]) const {
+    Kern<L, S>::template pull_thermal<ADIA, RT>(p, nb, c, nbits, solid, G);
   }
   __device__ __forceinline__ C alpha(const StepParams<S>& p, int c) const { return p.alpha[c]; }
 };
@@ -699,7 +699,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
   C G[QT > 0 ? QT : 1];
   C T = 0, dS = 0, rho = 0, ux = 0, uy = 0, uz = 0;
   if constexpr (THERMAL) {
-    src.thermal(p, nb, c, G);
+    src.template thermal<THERM == 3, RT>(p, nb, c, nbits, solid, G);
     static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
   }
   bool solid_next = solid;
@@ -710,7 +710,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
     K::moments(p, F, rho, ux, uy, uz);
     if (!peek) {
       K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T);
-      K::store_flow(p, nb, c, nbits, F);
+      K::store_flow(p, c, F);
     }
     if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);  // after the store: fewer live registers
   } else if constexpr (PYRO) {
@@ -757,7 +757,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
       const bool fl = !solid;
       K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
                          fl ? uz : (C)0, dS);
-      K::template store_thermal<THERM == 3, RT>(p, nb, c, G, nbits, solid);
+      K::store_thermal(p, c, G);
     }
     if (diag) diag_thermal(p, acc, c, T);
   }
@@ -861,11 +861,11 @@ __device__ __forceinline__ void list_turn_fluid(const StepParams<S>& p, int c, c
 // Cells that turned fluid on this pass (mask bit par solid, bit par^1 fluid).
 // Runs after step_bulk and step_boundary, over the whole mask (in a peek pass it
 // only reports the flow state of cells that turned fluid on the last pass):
-//  1. fluid neighbours z = X - e_k stored their population towards X in X's
-//     mirror slot f[opp k][X]; it moves to f[k][z], where X now pulls it from;
-//  2. X takes the mean post-stream (rho, u) of its fluid neighbours, collides
-//     from that equilibrium and stores with the mirror rule of the next parity;
-//  3. its temperature populations collide as fluid with the heat source that
+//  1. X takes the mean post-stream (rho, u) of its fluid neighbours, collides
+//     from that equilibrium and stores in its own slots, which its fluid
+//     neighbours pull from on the next pass (their own post-collision values are
+//     already in their own slots, where X pulls them from);
+//  2. its temperature populations collide as fluid with the heat source that
 //     step_bulk left in rel[B][X].
 template <class L, class S, int COLL, int THERM>
 __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typename Store<S>::C>& acc, bool diag,
@@ -887,42 +887,26 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
     if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
     return;
   }
-  {
-    C mir[Q];
-    static_for<Q>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      if constexpr (k > 0)
-        mir[k] = Store<S>::ld(p.fB, (size_t)L::opp(k) * p.N + c, fshift<L, S, L::opp(k)>(p));
-    });
-    static_for<Q>([&](auto kk) {
-      constexpr int k = decltype(kk)::value;
-      if constexpr (k > 0) {
-        const int zc = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
-        if (!K::solid_bit(p, zc, p.par)) Store<S>::st(p.fB, (size_t)k * p.N + zc, mir[k], fshift<L, S, k>(p));
-      }
-    });
-  }
   // temperature first: the collision's viscosity may depend on it (the pull reads the
   // input half, which the flow store below does not touch)
   C G[QT > 0 ? QT : 1];
   C T = 0;
   if constexpr (THERMAL) {
-    K::pull_thermal(p, nb, c, G);
+    K::pull_thermal(p, nb, c, 0u, true, G);  // conjugate field only (pyrolysis)
     static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
   }
   {
     C F[Q];
     K::feq_all(p, rb, ux, uy, uz, F);
     K::template collide_flow<COLL>(p, F, rb, ux, uy, uz, T);
-    const uint32_t nbn = K::neighbour_bits(p, nb, np);
-    K::store_flow(p, nb, c, nbn, F);
-    if (p.lhdr) list_turn_fluid<L>(p, c, nb, nbn);
+    K::store_flow(p, c, F);
+    if (p.ent_c) list_turn_fluid<L>(p, c, nb, K::neighbour_bits(p, nb, np));
   }
   if constexpr (THERMAL) {
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
     K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
-    K::template store_thermal<false>(p, nb, c, G, 0u, false);  // pyrolysis runs with the conjugate field only
+    K::store_thermal(p, c, G);
   }
   if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
 }
@@ -1013,13 +997,14 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
   if constexpr (PASS < 0) {
     const int c = x + p.nx * (y + p.ny * z);
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-    const uint32_t nbits = PYRO ? K::neighbour_bits(p, nb, p.par) : 0u;
+    const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
     K::template pull_flow<PYRO>(p, nb, c, nbits, s.F);
     K::moments(p, s.F, s.rho, s.ux, s.uy, s.uz);
     s.T = 0;
     if constexpr (THERMAL) {
       if (needT) {
-        K::pull_thermal(p, nb, c, s.G);
+        // side cells and the inner cells NEE reads are fluid
+        K::template pull_thermal<false, true>(p, nb, c, nbits, false, s.G);
         static_for<L::QT>([&](auto kk) { s.T += s.G[decltype(kk)::value]; });
       }
     }
@@ -1152,13 +1137,11 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
     if (THERMAL) diag_thermal(p, acc, c, s.T);
   }
   if (!(p.flags & kStepPeek)) {
-    const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-    const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
     K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz, s.T);
-    K::store_flow(p, nb, c, nbits, s.F);
+    K::store_flow(p, c, s.F);
     if constexpr (THERMAL) {
       K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
-      K::template store_thermal<THERM == 3>(p, nb, c, s.G, nbits, false);
+      K::store_thermal(p, c, s.G);
     }
   }
 }
@@ -1184,7 +1167,7 @@ __global__ void __launch_bounds__(128) step_boundary(const __grid_constant__ Ste
 // Equilibrium initialisation: post-collision state of f = feq(rho,u), g = geq(T,u),
 // i.e. what the reference's first collision produces after init_kernel
 // (src/LBM/LBM2D/_initialize.py:37-65).  Writes the B side of `p` (the buffer the
-// first pass reads) with the mirror rule; `solid_bit` selects the input mask bit.
+// first pass reads), own slots; `solid_bit` selects the input mask bit.
 template <class L, class S, int COLL, int THERM>
 __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p, const float* rho_in,
                                         const float* u_in,
@@ -1197,10 +1180,7 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
   if (c >= p.N) return;
   const uint8_t m0 = p.mask[c];
   const bool solid = (m0 >> solid_bit) & 1;
-  const int x = (int)(c % p.nx), y = (int)((c / p.nx) % p.ny), z = (int)(c / ((size_t)p.nx * p.ny));
-  const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
-  // neighbours' bit `solid_bit` keeps its value while the bytes are normalised
-  const uint32_t nbits = K::neighbour_bits(p, nb, solid_bit);
+  const int x = (int)(c % p.nx);
   const C rho = (C)rho_in[c];
   C ux = (C)u_in[c], uy = (C)u_in[p.N + c], uz = (C)u_in[2 * p.N + c];
   if (p.inlet && x <= 1) {
@@ -1214,13 +1194,13 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
     C F[Q];
     K::feq_all(p, rho, ux, uy, uz, F);
     K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T_in ? (C)T_in[c] : (C)0);
-    K::store_flow(p, nb, (int)c, nbits, F);
+    K::store_flow(p, (int)c, F);
   }
   if constexpr (THERMAL) {
     C G[QT];
     if (solid) K::geq_all((C)T_in[c], (C)0, (C)0, (C)0, G);
     else K::geq_all((C)T_in[c], ux, uy, uz, G);
-    K::template store_thermal<THERM == 3>(p, nb, (int)c, G, nbits, solid);
+    K::store_thermal(p, (int)c, G);
   }
   if constexpr (PYRO) {
     p.alpha[c] = alpha_in ? (C)alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? (C)1 : (C)0);

@@ -41,10 +41,6 @@ class Lattice:
         self.device = torch.device(device)
         self.stream = stream
         self._desc = cfg.to_desc()
-        self._staged_env = os.environ.get("LBM_STAGED", "0")[:1] == "1"
-        bulk = cfg.bulk_form if cfg.bulk_form != "auto" else os.environ.get("LBM_BULK", "")
-        self._tile_env = bulk == "tile" or (bulk != "list" and cfg.ncells < 65536)
-        self._list_forced = bulk == "list"
         h = ctypes.c_void_p()
         N.check(self.lib.lbm_create(ctypes.byref(self._desc), ctypes.byref(h)))
         self._h = h
@@ -78,19 +74,18 @@ class Lattice:
     def mask(self) -> torch.Tensor:
         return self.buf[N.LBM_FIELD_MASK]
 
-    def _staged(self) -> bool:
-        """True if the bulk update uses the shared-memory staged kernel (LBM_STAGED=1, rows a
-        multiple of 128)."""
-        return self.cfg.nx % 128 == 0 and self._staged_env
-
     @property
     def bulk_kernel(self) -> str:
-        """Form of the bulk update this lattice runs: "list" (cell lists; the default from
-        65536 cells, or LBM_BULK=list), "tile" (smaller lattices, or LBM_BULK=tile) or
-        "staged" (LBM_STAGED=1); fixed when the lattice is created."""
-        if self._staged() and not self._list_forced:
-            return "staged"
-        return "tile" if self._tile_env else "list"
+        """Form of the bulk update this lattice runs, fixed when the lattice is created:
+        "list" (cell lists; the default from 65536 cells, or LBM_BULK=list), "tile" (smaller
+        lattices, or LBM_BULK=tile) or "dense" (TMA-staged tiles, 3D: bulk_form="dense" or
+        LBM_BULK=dense)."""
+        return {1: "tile", 2: "list", 3: "dense"}[int(self.lib.lbm_bulk_form(self._h))]
+
+    def set_wait_limit(self, tries: int) -> None:
+        """Bound of the dense form's staged-load waits (tries of about a microsecond; 0 gives
+        up at once, which is how the timeout path is tested)."""
+        N.check(self.lib.lbm_set_wait_limit(self._h, int(tries)))
 
     @property
     def nsteps(self) -> int:

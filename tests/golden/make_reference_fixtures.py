@@ -184,8 +184,30 @@ def case_channel3d_thermal():
                 T=T, steps=20, thermal=(Df, Ds), channel=(0.03, 1.0))
 
 
+def case_periodic3d_x32():
+    """32 x 8 x 8: a shape the dense (TMA-staged) 3D bulk form runs too."""
+    shape = (32, 8, 8)
+    solid = _disks(shape, 3, 1.5, 2.2, 0, 9)
+    rho, u, T = _common_inputs(shape, 61, solid)
+    cfg = LatticeConfig(dim=3, nx=32, ny=8, nz=8, collision="bgk", precision="fp64", nu=0.1)
+    return dict(name="ref_periodic3d_x32", cfg=cfg, bc_model="NONE", solid=solid, rho=rho, u=u, T=T,
+                steps=16, thermal=None)
+
+
+def case_channel3d_flow_x32():
+    """NEE channel without temperature, 32 x 8 x 8 (dense-form shape)."""
+    nx, ny, nz = 32, 8, 8
+    shape = (nx, ny, nz)
+    solid = np.zeros(shape, dtype=bool)
+    solid[:, 2:ny - 2, 2:nz - 2] = _disks((nx, ny - 4, nz - 4), 3, 1.2, 1.8, 3, 10)
+    rho, u, T = _common_inputs(shape, 71, solid)
+    cfg = LatticeConfig(dim=3, nx=nx, ny=ny, nz=nz, collision="bgk", precision="fp64", nu=0.1)
+    return dict(name="ref_channel3d_flow_x32", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T,
+                steps=16, thermal=None, channel=(0.03, 1.0))
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
-         case_periodic3d, case_channel3d_thermal]
+         case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32]
 
 
 # --------------------------------------------------------------------------- driver

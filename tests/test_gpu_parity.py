@@ -198,54 +198,6 @@ def test_flip_steps_within_one(oracle_mod):
     assert np.array_equal(fg > 0, conv)
 
 
-# --- the staged bulk kernel (rows are a multiple of 128 cells) ---------------------------
-
-@pytest.fixture
-def staged(monkeypatch):
-    monkeypatch.setenv("LBM_STAGED", "1")
-
-
-@pytest.mark.parametrize("coll", ["bgk", "mrt"])
-def test_staged_pyro3d_fp64_with_flips(oracle_mod, coll, staged):
-    w = _fast_pyro(workloads.pyro3d(128, seed=5, collision=coll, ny=12, nz=10), A=1.2e11)
-    lat, o = _run_pair(oracle_mod, w, 120, "f64", "fp64")
-    assert lat._staged()
-    g, r = _compare(lat, o, 1e-10, 1e-10, 1e-10)
-    assert (w.solid & ~r["solid"]).any()
-
-
-def test_staged_flow2d_fp64(oracle_mod, staged):
-    w = workloads.flow2d(128, 40, seed=4)
-    w.cfg.force = (1e-5, 0.0, 0.0)
-    lat, o = _run_pair(oracle_mod, w, 200, "f64", "fp64")
-    assert lat._staged()
-    _compare(lat, o, 1e-10, 1e-10, 1e-10)
-
-
-def test_staged_pyro3d_fp32(oracle_mod, staged):
-    w = _fast_pyro(workloads.pyro3d(128, seed=6, ny=12, nz=10), A=1.2e11)
-    _fp32_check(oracle_mod, w, 120)
-
-
-@pytest.mark.parametrize("precision", ["fp32", "fp16"])
-def test_staged_equals_unstaged(precision, monkeypatch):
-    """The staged kernel performs the same arithmetic as step_bulk: identical bits."""
-    from lbm_porouschem_b200.lattice import Lattice
-    w = _fast_pyro(workloads.pyro3d(128, seed=7, ny=16, nz=8, precision=precision), A=1.2e11)
-    out = {}
-    for staged in ("1", "0"):
-        monkeypatch.setenv("LBM_STAGED", staged)
-        lat = Lattice(w.cfg)
-        assert lat._staged() == (staged == "1")
-        lat.set_geometry(w.solid, w.reactive)
-        lat.init(**w.init)
-        lat.step(90)
-        out[staged] = lat.fields()
-        lat.close()
-    for k in ("rho", "u", "T", "alpha", "solid"):
-        assert np.array_equal(out["1"][k], out["0"][k]), k
-
-
 @pytest.mark.parametrize("dim", [2, 3])
 def test_two_field_thermal_fp64(oracle_mod, dim):
     """The reference's two temperature fields (adiabatic fluid-solid interface) with a

@@ -4,11 +4,15 @@ Fixtures: ``tests/golden/ref_*.npz``, written by ``tests/golden/make_reference_f
 from the unmodified reference modules (``src/LBM/LBM2D``, ``src/LBM/LBM3D``) in float64.
 
 Tolerances (relative L2 over the compared cells):
-  - FP64 kernels, tile and cell-list forms: 1e-10 for rho, u and temperature.  The kernels
-    use a pull scheme with mirror stores and fused multiply-adds, so they agree with the
-    reference's push-scheme arithmetic to rounding, not bit for bit.
-  - FP32 kernels: 1e-5 for rho and temperature, and for u measured against the velocity
-    scale (RMS error / max |u|): the velocity is a small difference of O(1) populations.
+  - FP64 kernels, tile, cell-list and dense (TMA-staged, 3D) forms: 1e-10 for rho, u and
+    temperature.  The kernels use a pull scheme with own-slot bounce-back and fused
+    multiply-adds, so they agree with the reference's push-scheme arithmetic to rounding,
+    not bit for bit.
+  - FP32 kernels: 1e-5 for rho and temperature.  The velocity is a small difference of O(1)
+    populations, so float32 rounding alone moves it by ~1e-5 of its scale over these runs
+    (2e-5 RMS / max|u| on the 2D periodic case); the bound is that the kernel's velocity
+    error against the reference stays within 2x that of a plain float32 restatement of the
+    reference (the FP32 oracle) on the same inputs.
 Cells compared: fluid cells for rho and u; for temperature every fluid cell, and the solid
 cells only where the reference's solid temperature evolves (in its two-field model the
 pure-solid cells keep their initial temperature, ``src/LBM/LBM2D/_evolution.py:119``, while
@@ -51,10 +55,16 @@ def _run(cfg, z, steps):
     return out
 
 
-@pytest.mark.parametrize("form", ["tile", "list"])
+def _dense_ok(cfg) -> bool:
+    return cfg.dim == 3 and cfg.nx % 32 == 0 and cfg.ny % 4 == 0 and cfg.nz % 2 == 0 and cfg.thermal != "two_field"
+
+
+@pytest.mark.parametrize("form", ["tile", "list", "dense"])
 @pytest.mark.parametrize("name", CASES)
 def test_fp64_kernels_match_reference(name, form):
     z, meta, cfg = _load(name)
+    if form == "dense" and not _dense_ok(cfg):
+        pytest.skip("shape or temperature mode outside the dense form")
     g = _run(cfg.replace(precision="fp64", bulk_form=form), z, meta["steps"])
     fl = ~z["solid"]
     assert np.array_equal(g["solid"], z["solid"])
@@ -66,13 +76,18 @@ def test_fp64_kernels_match_reference(name, form):
 
 
 @pytest.mark.parametrize("name", CASES)
-def test_fp32_kernels_match_reference(name):
+def test_fp32_kernels_match_reference(oracle_mod, name):
     z, meta, cfg = _load(name)
-    g = _run(cfg.replace(precision="fp32"), z, meta["steps"])
+    cfg32 = cfg.replace(precision="fp32")
+    g = _run(cfg32, z, meta["steps"])
+    o = oracle_mod.Oracle(cfg32, real="f32", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
+    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+    o.step(meta["steps"])
+    r32 = o.fields()
     fl = ~z["solid"]
     assert _rel(g["rho"][fl], z["rho_ref"][fl]) < 1e-5
-    du = g["u"][:, fl] - z["u_ref"][:, fl]
-    e_u = np.sqrt(np.mean(du ** 2)) / np.abs(z["u_ref"][:, fl]).max()
-    assert e_u < 1e-5, e_u
+    e_kernel = np.linalg.norm(g["u"][:, fl] - z["u_ref"][:, fl])
+    e_f32 = np.linalg.norm(r32["u"][:, fl] - z["u_ref"][:, fl])
+    assert e_kernel <= 2.0 * e_f32 + 1e-9 * np.sqrt(fl.sum()), (e_kernel, e_f32)
     if cfg.thermal != "none":
         assert _rel(g["T"][fl], z["T_ref"][fl]) < 1e-5
