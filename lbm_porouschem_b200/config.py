@@ -105,6 +105,8 @@ class LatticeConfig:
     viscosity: str = "constant"     # "constant" (nu) | "sutherland" (per cell from T; thermal only)
     suth_A: float = 0.0             # Sutherland: nu = suth_A TK^1.5 / (TK + suth_Ts), TK = T_ref + T_scale T
     suth_Ts: float = 0.0            #   (suth_A = As dt/dx^2 in lattice units, suth_Ts in K)
+    porous: str = "none"            # porous cells (0 < solid fraction < 1): "none" | "ergun" | "darcy"
+                                    #   | "darcy_forchheimer" (the reference's PORO_MODEL)
 
     @property
     def shape(self) -> tuple:

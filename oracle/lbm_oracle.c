@@ -93,6 +93,8 @@ typedef struct orc_cfg {
                               * cells (LBM2D/_evolution.py:119), so their TS.S never changes and
                               * TS.g keeps its own post-collision values instead of the streamed
                               * ones (collision :96-100 writes TS.g in place).  1 reproduces that. */
+    int poro_model;          /* porous cells (0 < solid < 1, src/LBM/util/flag.py PORO_MODEL): 0 none,
+                              * 1 SPHERICAL (Ergun from the porosity), 2 DARCY, 3 DARCYFORCHHEIMER */
 } orc_cfg;
 
 /* mask bits */
@@ -113,6 +115,7 @@ typedef struct orc {
     int cons_row[19];         /* 1 if the moment is conserved (rho, j): never relaxed */
     REAL *f, *F, *g, *G;
     REAL *rho, *u, *T, *dS, *alpha, *rel;
+    REAL *sfrac, *cdarcy, *cforch;  /* solid fraction, Darcy and Forchheimer coefficients per cell */
     uint8_t *mask, *mask_next;
     /* flow-rate inlet on side 0, per side cell j = y + ny*z: what the reference's
      * updateBC_kernel reads (rho*u_x at x = 0, u at x = 1, 3 per cell) and the
@@ -182,14 +185,21 @@ static inline long nbr(const orc* o, long c, int k, int sign) {
 }
 static inline int is_solid(const uint8_t* m, long c) { return (m[c] & ORC_SOLID) != 0; }
 
-/* feq9 / feq19: src/LBM/LBM2D/_evolution.py:213-225, eps = 1 - solid = 1 for fluid cells */
-static inline REAL feq(const orc* o, int k, REAL rho, const REAL* u) {
+/* feq9 / feq19: src/LBM/LBM2D/_evolution.py:213-225, with eps = 1 - solid (1 in a fluid
+ * cell, 0 < eps < 1 in a porous one) */
+static inline REAL feq_e(const orc* o, int k, REAL rho, const REAL* u, REAL eps0) {
     REAL eu = (REAL)o->e[k][0]*u[0] + (REAL)o->e[k][1]*u[1] + (REAL)o->e[k][2]*u[2];
     REAL uv = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
-    REAL eps = (REAL)1.0 + (REAL)1e-12;
+    REAL eps = eps0 + (REAL)1e-12;
     if (o->c.eos == 1)
         return o->w[k]*(rho + (REAL)3.0*eu + (REAL)4.5*eu*eu/eps - (REAL)1.5*uv/eps);
     return o->w[k]*rho*((REAL)1.0 + (REAL)3.0*eu + (REAL)4.5*eu*eu/eps - (REAL)1.5*uv/eps);
+}
+static inline REAL feq(const orc* o, int k, REAL rho, const REAL* u) { return feq_e(o, k, rho, u, (REAL)1.0); }
+/* eps = 1 - solid of a cell, src/LBM/LBM2D/_evolution.py:119 */
+static inline REAL eps_of(const orc* o, long c) { return (REAL)1.0 - o->sfrac[c]; }
+static inline int is_porous(const orc* o, long c) {
+    return o->c.poro_model != 0 && o->sfrac[c] != 0 && o->sfrac[c] != 1;
 }
 /* TemperatureFluid.geq5 / geq7: src/LBM/LBM2D/_thermal.py:54-61, LBM3D/_thermal.py:54-61 */
 static inline REAL geq_fluid(const orc* o, int k, REAL T, const REAL* u) {
@@ -197,22 +207,75 @@ static inline REAL geq_fluid(const orc* o, int k, REAL T, const REAL* u) {
     REAL uv = u[0]*u[0] + u[1]*u[1] + u[2]*u[2];
     return o->wt[k]*T*((REAL)1.0 + o->ta*eu + o->tb*eu*eu - o->tc*uv);
 }
-/* tau: src/LBM/LBM2D/_evolution.py:228-249 (viscosity(i): constant or Sutherland at the
- * fluid temperature GetTF(i) = T_ref + T_scale*T, :304-307; IDEAL_GAS divides by rho) */
-static inline REAL tau_flow(const orc* o, REAL rho, REAL T) {
+/* viscosity(i) in lattice units: constant or Sutherland at the fluid temperature GetTF(i)
+ * = T_ref + T_scale*T (src/LBM/LBM2D/_evolution.py:227-235, :304-307) */
+static inline REAL visc_lu(const orc* o, REAL T) {
     REAL nu = (REAL)o->c.nu;
     if (o->c.visc_model == 1) {
         REAL TK = T*(REAL)o->c.T_scale + (REAL)o->c.T_ref;
         nu = (REAL)o->c.suth_A*(REAL)pow(TK, 1.5)/(TK + (REAL)o->c.suth_Ts);
     }
-    if (o->c.eos == 0) nu = nu / rho;
-    return (REAL)3*nu + (REAL)0.5;
+    return nu;
 }
-/* forceTermGuo: src/LBM/LBM2D/_evolution.py:284-298 */
-static inline REAL guo(const orc* o, int k, REAL rho, const REAL* u, REAL tau) {
-    REAL Fx = (REAL)o->c.force[0], Fy = (REAL)o->c.force[1], Fz = (REAL)o->c.force[2];
+/* kinetic_viscosity(i): IDEAL_GAS divides by rho (:236-240) */
+static inline REAL visc_kin(const orc* o, REAL rho, REAL T) {
+    REAL nu = visc_lu(o, T);
+    if (o->c.eos == 0) nu = nu / rho;
+    return nu;
+}
+/* tau = 3 kinetic_viscosity + 1/2 (:241-249) */
+static inline REAL tau_flow(const orc* o, REAL rho, REAL T) { return (REAL)3*visc_kin(o, rho, T) + (REAL)0.5; }
+
+/* darcy_force(i) of a porous cell, src/LBM/LBM2D/_evolution.py:262-283: SPHERICAL (Ergun
+ * with perm = eps^3/(1.000001-eps)^2, :250-253), DARCY, DARCYFORCHHEIMER.  The 2D solver
+ * uses kinetic_viscosity(i); the 3D one uses viscosity(i) (LBM3D/_evolution.py:262-278). */
+static void darcy_force(const orc* o, long c, REAL rho, const REAL* u, REAL T, REAL* F) {
+    REAL eps = eps_of(o, c);
+    REAL nu = o->c.dim == 2 ? visc_kin(o, rho, T) : visc_lu(o, T);
+    REAL v = (REAL)sqrt((double)(u[0]*u[0] + u[1]*u[1] + u[2]*u[2]));
+    REAL a = 0;
+    if (o->c.poro_model == 1) {
+        REAL perm = (REAL)pow((double)eps, 3.0)/(REAL)pow((double)((REAL)1.000001 - eps), 2.0)*(REAL)1;
+        REAL beta = (REAL)1.75/(REAL)sqrt((double)((REAL)150*eps*perm));
+        a = -nu/perm*eps - beta*v;
+    } else if (o->c.poro_model == 2) {
+        a = -eps*nu*o->cdarcy[c];
+    } else if (o->c.poro_model == 3) {
+        a = -eps*nu*o->cdarcy[c] - eps*o->cforch[c]*v;
+    }
+    for (int d = 0; d < 3; ++d) F[d] = a*u[d];
+}
+
+/* macro's porous velocity correction, src/LBM/LBM2D/_evolution.py:131-151 (3D: :130-149),
+ * at the cell's new rho */
+static void porous_correct(const orc* o, long c, REAL rho, REAL T, REAL* u) {
+    REAL eps = eps_of(o, c);
+    REAL nu = visc_kin(o, rho, T);
+    REAL div;
+    if (o->c.poro_model == 2) {
+        div = (REAL)1 + eps*nu*o->cdarcy[c]/(REAL)2;
+    } else {
+        REAL Dc, Fc;
+        if (o->c.poro_model == 1) {
+            REAL perm = (REAL)pow((double)eps, 3.0)/(REAL)pow((double)((REAL)1.000001 - eps), 2.0)*(REAL)1;
+            Dc = (REAL)1.0/perm;
+            Fc = (REAL)1.75/(REAL)sqrt((double)((REAL)150*(REAL)pow((double)eps, 3.0)));
+        } else {
+            Dc = o->cdarcy[c];
+            Fc = o->cforch[c];
+        }
+        REAL c0 = (REAL)0.5*((REAL)1 + eps*nu/(REAL)2*Dc);
+        REAL c1 = (REAL)0.5*eps*Fc;
+        REAL v = (REAL)sqrt((double)(u[0]*u[0] + u[1]*u[1] + u[2]*u[2]));
+        div = c0 + (REAL)sqrt((double)((REAL)pow((double)c0, 2.0) + c1*v));
+    }
+    for (int d = 0; d < 3; ++d) u[d] /= div;
+}
+/* forceTermGuo: src/LBM/LBM2D/_evolution.py:284-298, force F (volume + darcy) and eps */
+static inline REAL guo(const orc* o, int k, REAL rho, const REAL* u, REAL tau, const REAL* Fv, REAL eps0) {
+    REAL Fx = Fv[0], Fy = Fv[1], Fz = Fv[2];
     if (Fx == 0 && Fy == 0 && Fz == 0) return 0;
-    REAL eps = (REAL)1.0 + (REAL)1e-12;
+    REAL eps = eps0 + (REAL)1e-12;
     REAL ex = (REAL)o->e[k][0], ey = (REAL)o->e[k][1], ez = (REAL)o->e[k][2];
     REAL t1 = (ex - u[0]/eps)*Fx + (ey - u[1]/eps)*Fy + (ez - u[2]/eps)*Fz;
     REAL eu = ex*u[0] + ey*u[1] + ez*u[2];
@@ -223,15 +286,25 @@ static inline REAL guo(const orc* o, int k, REAL rho, const REAL* u, REAL tau) {
     return pre*rho*o->w[k]*((REAL)3.0*t1 + (REAL)9.0*eu*eF/eps);
 }
 
-/* Post-collision flow populations of a fluid cell (BGK: _evolution.py:33; MRT new). */
-static void collide_flow(const orc* o, const REAL* fin, REAL rho, const REAL* u, REAL T, REAL* fout) {
+/* Post-collision flow populations of fluid cell c (BGK: _evolution.py:33; MRT new).  A
+ * porous cell (0 < solid < 1) relaxes towards its eps-equilibrium and adds the Guo term of
+ * its Darcy force (force(i) = volume_force + darcy_force, :254-261). */
+static void collide_flow(const orc* o, long c, const REAL* fin, REAL rho, const REAL* u, REAL T, REAL* fout) {
     int Q = o->Q;
     REAL tau = tau_flow(o, rho, T);
+    REAL eps = 1;
+    REAL Fv[3] = {(REAL)o->c.force[0], (REAL)o->c.force[1], (REAL)o->c.force[2]};
+    if (c >= 0 && is_porous(o, c)) {
+        REAL Fd[3];
+        eps = eps_of(o, c);
+        darcy_force(o, c, rho, u, T, Fd);
+        for (int d = 0; d < 3; ++d) Fv[d] = (REAL)0 + Fv[d] + Fd[d];
+    }
     REAL fe[19];
-    for (int k = 0; k < Q; ++k) fe[k] = feq(o, k, rho, u);
+    for (int k = 0; k < Q; ++k) fe[k] = feq_e(o, k, rho, u, eps);
     if (o->c.collision == 0) {
         for (int k = 0; k < Q; ++k)
-            fout[k] = fin[k] - (REAL)1/tau*(fin[k] - fe[k]) + guo(o, k, rho, u, tau);
+            fout[k] = fin[k] - (REAL)1/tau*(fin[k] - fe[k]) + guo(o, k, rho, u, tau, Fv, eps);
         return;
     }
     REAL mneq[19];
@@ -245,7 +318,7 @@ static void collide_flow(const orc* o, const REAL* fin, REAL rho, const REAL* u,
     for (int k = 0; k < Q; ++k) {
         REAL acc = 0;
         for (int r = 0; r < Q; ++r) if (!o->cons_row[r]) acc += (REAL)o->M[r][k]*mneq[r];
-        fout[k] = fin[k] - acc + guo(o, k, rho, u, tau);
+        fout[k] = fin[k] - acc + guo(o, k, rho, u, tau, Fv, eps);
     }
 }
 
@@ -298,6 +371,9 @@ orc* orc_create(const orc_cfg* cfg) {
     o->alpha = (REAL*)calloc(N, sizeof(REAL));
     o->rel = (REAL*)calloc(N, sizeof(REAL));
     o->mask = (uint8_t*)calloc(N, 1);
+    o->sfrac = (REAL*)calloc(N, sizeof(REAL));
+    o->cdarcy = (REAL*)calloc(N, sizeof(REAL));
+    o->cforch = (REAL*)calloc(N, sizeof(REAL));
     o->mask_next = (uint8_t*)calloc(N, 1);
     long M = (long)o->c.ny * o->c.nz;
     o->inl_m = (REAL*)calloc(M, sizeof(REAL));
@@ -310,12 +386,24 @@ void orc_destroy(orc* o) {
     if (!o) return;
     free(o->f); free(o->F); free(o->g); free(o->G); free(o->rho); free(o->u); free(o->T);
     free(o->dS); free(o->alpha); free(o->rel); free(o->mask); free(o->mask_next);
+    free(o->sfrac); free(o->cdarcy); free(o->cforch);
     free(o->inl_m); free(o->inl_w); free(o->inl_prof); free(o);
 }
 
 int orc_Q(const orc* o) { return o->Q; }
 int orc_QT(const orc* o) { return o->QT; }
 double orc_M(const orc* o, int r, int k) { return o->M[r][k]; }
+
+/* Porous cells: solid fraction (0 fluid, 1 solid, between: porous), Darcy and Forchheimer
+ * coefficients (set_poro_Darcy / set_poro_Darcy_Forchheimer, src/LBM/LBM2D/_io.py:152-172),
+ * planar, any may be NULL.  Call before orc_init. */
+void orc_set_porous(orc* o, const double* sfrac, const double* darcy, const double* forch) {
+    for (long c = 0; c < o->N; ++c) {
+        o->sfrac[c] = sfrac ? (REAL)sfrac[c] : 0;
+        o->cdarcy[c] = darcy ? (REAL)darcy[c] : 0;
+        o->cforch[c] = forch ? (REAL)forch[c] : 0;
+    }
+}
 
 /* init_kernel: f = F = feq(rho,u), g = G = geq(T,u)  (src/LBM/LBM2D/_initialize.py:37-65).
  * Inputs are planar: u[d*N + c].  mask bit0 = solid, bit2 = reactive. */
@@ -335,7 +423,7 @@ void orc_init(orc* o, const double* rho, const double* u, const double* T,
         o->rel[c] = 0;
         if (is_solid(o->mask, c)) { o->u[c*3] = o->u[c*3+1] = o->u[c*3+2] = 0; }
         for (int k = 0; k < o->Q; ++k) {
-            REAL v = is_solid(o->mask, c) ? 0 : feq(o, k, o->rho[c], &o->u[c*3]);
+            REAL v = is_solid(o->mask, c) ? 0 : feq_e(o, k, o->rho[c], &o->u[c*3], is_porous(o, c) ? eps_of(o, c) : (REAL)1.0);
             o->f[c*o->Q + k] = v;
             o->F[c*o->Q + k] = v;
         }
@@ -369,7 +457,7 @@ static void collide_stream(orc* o) {
         REAL fo[19], go[7];
         int solid = is_solid(o->mask, c);
         if (!solid) {
-            collide_flow(o, &o->f[c*Q], o->rho[c], &o->u[c*3], o->T[c], fo);
+            collide_flow(o, c, &o->f[c*Q], o->rho[c], &o->u[c*3], o->T[c], fo);
             for (int k = 0; k < Q; ++k) {
                 long ip = nbr(o, c, k, +1);
                 if (!is_solid(o->mask, ip)) o->F[ip*Q + k] = fo[k];      /* :69-70 */
@@ -430,6 +518,7 @@ static void macro(orc* o) {
             if (o->c.half_force_velocity)
                 for (int d = 0; d < 3; ++d) j[d] += (REAL)0.5*(REAL)o->c.force[d]*(o->c.eos == 0 ? r : (REAL)1);
             if (o->c.eos == 0) for (int d = 0; d < 3; ++d) j[d] /= r;
+            if (is_porous(o, c)) porous_correct(o, c, r, o->T[c], j);
             o->rho[c] = r;
             for (int d = 0; d < 3; ++d) o->u[c*3 + d] = j[d];
         }

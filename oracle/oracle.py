@@ -40,7 +40,7 @@ class orc_cfg(C.Structure):
         ("dt_phys", C.c_double), ("heat_norm", C.c_double), ("gas_coef", C.c_double),
         ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19), ("side", orc_side * 6),
         ("visc_model", C.c_int), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
-        ("ref_quirk_frozen_solid_T", C.c_int),
+        ("ref_quirk_frozen_solid_T", C.c_int), ("poro_model", C.c_int),
     ]
 
 
@@ -73,6 +73,7 @@ def _load(real: str) -> C.CDLL:
     lib.orc_create.restype = C.c_void_p
     lib.orc_destroy.argtypes = [C.c_void_p]
     lib.orc_init.argtypes = [C.c_void_p] + [C.c_void_p] * 5
+    lib.orc_set_porous.argtypes = [C.c_void_p] * 4
     lib.orc_step.argtypes = [C.c_void_p, C.c_int]
     lib.orc_get.argtypes = [C.c_void_p] + [C.c_void_p] * 5
     lib.orc_get_dist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -121,6 +122,7 @@ class Oracle:
         c.visc_model = 1 if cfg.viscosity == "sutherland" else 0
         c.suth_A, c.suth_Ts = cfg.suth_A, cfg.suth_Ts
         c.ref_quirk_frozen_solid_T = int(ref_quirk_frozen_solid_T)
+        c.poro_model = {"none": 0, "ergun": 1, "darcy": 2, "darcy_forchheimer": 3}[getattr(cfg, "porous", "none")]
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):
@@ -142,6 +144,12 @@ class Oracle:
         if ncomp == 1:
             return fortran_flat(a.reshape(self.cfg.shape)).astype(np.float64)
         return np.concatenate([fortran_flat(a[i].reshape(self.cfg.shape)) for i in range(ncomp)]).astype(np.float64)
+
+    def set_porous(self, fraction, darcy=None, forchheimer=None) -> None:
+        """Porous cells before ``init``: solid fraction per cell (0 fluid, 1 solid, between
+        porous) and the Darcy / Forchheimer coefficients, (nx, ny, nz) arrays."""
+        self._porous = tuple(self._flat(a) if a is not None else None for a in (fraction, darcy, forchheimer))
+        self.lib.orc_set_porous(self._h, *(_ptr(a) for a in self._porous))
 
     def init(self, solid, reactive=None, rho=1.0, u=(0.0, 0.0, 0.0), T=0.0, alpha=None,
              round_inputs_to_f32: bool = True) -> None:

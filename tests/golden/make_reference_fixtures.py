@@ -206,8 +206,52 @@ def case_channel3d_flow_x32():
                 steps=16, thermal=None, channel=(0.03, 1.0))
 
 
+def _porous_zone(shape, centre, r):
+    grids = np.meshgrid(*[np.arange(s) for s in shape], indexing="ij")
+    return sum((g - c) ** 2 for g, c in zip(grids, centre)) <= r * r
+
+
+def case_porous2d_darcy():
+    """NEE channel with a porous cylinder (DARCY), like examples/2D/cylinder_poro."""
+    nx, ny = 24, 12
+    shape = (nx, ny, 1)
+    zone = _porous_zone((nx, ny), (10.3, 5.7), 3.6)[..., None]
+    solid = np.zeros(shape, dtype=bool)
+    rho, u, T = _common_inputs(shape, 81, solid)
+    cfg = LatticeConfig(dim=2, nx=nx, ny=ny, nz=1, collision="bgk", precision="fp64", nu=0.1, porous="darcy")
+    return dict(name="ref_porous2d_darcy", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T, steps=60,
+                thermal=None, channel=(0.03, 1.0), porous=dict(model="darcy", zone=zone, eps=0.6, darcy=0.5))
+
+
+def case_porous2d_ergun():
+    """Periodic flow through a porous blob (default SPHERICAL model: Ergun from the
+    porosity) next to an impermeable disk."""
+    shape = (16, 12, 1)
+    zone = _porous_zone((16, 12), (5.2, 6.1), 3.3)[..., None]
+    solid = _porous_zone((16, 12), (12.4, 4.0), 2.1)[..., None] & ~zone
+    rho, u, T = _common_inputs(shape, 91, solid)
+    cfg = LatticeConfig(dim=2, nx=16, ny=12, nz=1, collision="bgk", precision="fp64", nu=0.1, porous="ergun")
+    return dict(name="ref_porous2d_ergun", cfg=cfg, bc_model="NONE", solid=solid, rho=rho, u=u, T=T, steps=60,
+                thermal=None, porous=dict(model="ergun", zone=zone, eps=0.5))
+
+
+def case_porous3d_df():
+    """3D NEE channel with a porous sphere (DARCYFORCHHEIMER; the 3D drag uses viscosity(i))."""
+    nx, ny, nz = 12, 8, 8
+    shape = (nx, ny, nz)
+    zone = _porous_zone(shape, (5.6, 3.6, 3.6), 1.9)
+    solid = np.zeros(shape, dtype=bool)
+    rho, u, T = _common_inputs(shape, 101, solid)
+    cfg = LatticeConfig(dim=3, nx=nx, ny=ny, nz=nz, collision="bgk", precision="fp64", nu=0.1,
+                        porous="darcy_forchheimer")
+    return dict(name="ref_porous3d_df", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T, steps=20,
+                thermal=None, channel=(0.03, 1.0),
+                porous=dict(model="darcy_forchheimer", zone=zone, eps=0.7, darcy=0.5, forch=0.3))
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
-         case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32]
+         case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32,
+         case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df]
 
 
 # --------------------------------------------------------------------------- driver
@@ -217,7 +261,8 @@ def run_reference(case, Solver2D, Solver3D, flag):
     nx, ny, nz = cfg.nx, cfg.ny, cfg.nz
     thermal = case.get("thermal")
     Solver = Solver2D if dim == 2 else Solver3D
-    lb = Solver(nx, ny, nz, 1, 1, case["name"], thermal is not None, False, False, False)
+    poro = case.get("porous")
+    lb = Solver(nx, ny, nz, 1, 1, case["name"], thermal is not None, False, poro is not None, False)
     lb.source_term_model = flag.SOURCE_TERM.MICRO       # app.py:103-104
     lb.force_term_model = flag.FORCE_TERM.GUO
     lb.set_viscosity(cfg.nu)
@@ -261,6 +306,21 @@ def run_reference(case, Solver2D, Solver3D, flag):
     lb.init_field(lb.rho, case["rho"].copy())
     lb.init_field3(lb.v, case["u"][0].copy(), case["u"][1].copy(), case["u"][2].copy())
     lb.add_solid(case["solid"].astype(np.float64))
+    if poro is not None:
+        # app.py:537-573: solid fraction (1 - porosity) over the zone, coefficients over it
+        zs = poro["zone"].astype(np.float64)
+        frac = (1.0 - poro["eps"]) * zs
+        lb.add_solid(frac)
+        case["sfrac"] = case["solid"].astype(np.float64) + frac
+        case["darcy"] = np.zeros(zs.shape)
+        case["forch"] = np.zeros(zs.shape)
+        if poro["model"] == "darcy":
+            lb.set_poro_Darcy(zs, poro["darcy"])
+            case["darcy"] = poro["darcy"] * zs
+        elif poro["model"] == "darcy_forchheimer":
+            lb.set_poro_Darcy_Forchheimer(zs, poro["darcy"], poro["forch"])
+            case["darcy"] = poro["darcy"] * zs
+            case["forch"] = poro["forch"] * zs
     lb.init_simulation()
     t0 = time.time()
     for _ in range(case["steps"]):
@@ -289,8 +349,9 @@ def main(argv):
                     ref_quirk_frozen_solid_T=case["cfg"].thermal == "two_field",
                     generator="tests/golden/make_reference_fixtures.py")
         path = HERE / f"{case['name']}.npz"
+        extra = {k: case[k] for k in ("sfrac", "darcy", "forch") if k in case}
         np.savez_compressed(path, meta=json.dumps(meta), solid=case["solid"], rho0=case["rho"],
-                            u0=case["u"], T0=case["T"], **{k + "_ref": v for k, v in out.items()})
+                            u0=case["u"], T0=case["T"], **extra, **{k + "_ref": v for k, v in out.items()})
         print(f"{case['name']}: {case['steps']} steps in {dt:.1f} s -> {path.name} "
               f"({path.stat().st_size} B)")
     return 0

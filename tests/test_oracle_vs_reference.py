@@ -8,8 +8,10 @@ stand-in for Taichi, in float64, from float32-representable inputs.  Each case r
 ``LatticeConfig`` describing the same run here.
 
 The bar is 1e-12 relative L2 (the restatement follows the reference's arithmetic order, so
-in practice the fields agree bit for bit); fluid cells are compared for rho, u and the flow
-populations, every cell for temperature.
+in practice the fields agree bit for bit); fluid and porous cells are compared for rho, u and
+the flow populations, every cell for temperature.  The porous cases run the reference with
+``isPoro``: cells of solid fraction between 0 and 1, the eps-equilibrium, the Darcy /
+Darcy-Forchheimer / Ergun drag in the Guo term and the macro velocity correction.
 """
 from __future__ import annotations
 
@@ -49,6 +51,8 @@ def test_fixtures_present():
 def test_oracle_matches_reference(oracle_mod, name):
     z, meta, cfg = load_case(name)
     o = oracle_mod.Oracle(cfg, real="f64", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
+    if "sfrac" in z:   # porous cells: solid fraction and drag coefficients
+        o.set_porous(z["sfrac"], z["darcy"], z["forch"])
     o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
     o.step(meta["steps"])
     r = o.fields()
