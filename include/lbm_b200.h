@@ -54,6 +54,20 @@ extern "C" {
 #define LBM_PREC_FP64 2
 #define LBM_VISC_CONSTANT 0      /* nu (util/flag.py VISCOSITY_MODEL.CONSTANT) */
 #define LBM_VISC_SUTHERLAND 1    /* per cell from its temperature; needs the temperature field */
+
+/* Porous cells (lbm_desc.porous): cells whose solid fraction s (LBM_FIELD_PORO) lies
+ * between 0 and 1 are porous, eps = 1 - s (src/LBM/util/flag.py PORO_MODEL; set_poro_Darcy /
+ * set_poro_Darcy_Forchheimer, src/LBM/LBM2D/_io.py:152-172).  Such a cell relaxes towards
+ * the eps-equilibrium (src/LBM/LBM2D/_evolution.py:213-225), feels the drag of its model
+ * through the Guo term (:254-298; the 3D solver takes the lattice viscosity there,
+ * LBM3D/_evolution.py:262-278) and has its velocity corrected after the moments
+ * (:131-151).  Cells with s >= 1 are the solid of the mask; s = 0 is fluid.  Constant
+ * viscosity, no temperature field; the two outer cell layers of an active side must have
+ * s = 0. */
+#define LBM_PORO_NONE 0
+#define LBM_PORO_ERGUN 1              /* SPHERICAL: permeability eps^3/(1.000001-eps)^2, Ergun drag */
+#define LBM_PORO_DARCY 2              /* coefficient LBM_FIELD_DARCY per cell */
+#define LBM_PORO_DARCY_FORCHHEIMER 3  /* LBM_FIELD_DARCY and LBM_FIELD_FORCH per cell */
 #define LBM_EOS_IDEAL_GAS 0      /* util/flag.py:64-67 FLUID_STATE_EQUATION */
 #define LBM_EOS_INCOMPRESSIBLE 1
 #define LBM_THERMAL_NONE 0
@@ -126,7 +140,7 @@ typedef struct lbm_desc {
   double rho0, T0;        /* FP16 storage shift references */
   lbm_side_desc side[6];
   int32_t viscosity;      /* LBM_VISC_* */
-  int32_t reserved0;      /* 0 */
+  int32_t porous;         /* LBM_PORO_* */
   double suth_A, suth_Ts; /* LBM_VISC_SUTHERLAND: lattice viscosity suth_A T^1.5/(T + suth_Ts) of the
                              cell's temperature T in kelvin (T_ref + T_scale*T); suth_A = As*dt/dx^2
                              of set_viscosity_sutherland(As, Ts) (src/LBM/LBM2D/_evolution.py:228-235) */
@@ -162,7 +176,10 @@ typedef struct lbm_diag {
                                the step's coefficient F/flow0, then per step parity the
                                rho*u_x of each side cell and the velocity behind it
                                (compute precision); part of a checkpoint */
-#define LBM_NUM_FIELDS 11
+#define LBM_FIELD_PORO 11   /* solid fraction per cell (compute precision), with lbm_desc.porous */
+#define LBM_FIELD_DARCY 12  /* Darcy coefficient per cell (LBM_PORO_DARCY, _DARCY_FORCHHEIMER) */
+#define LBM_FIELD_FORCH 13  /* Forchheimer coefficient per cell (LBM_PORO_DARCY_FORCHHEIMER) */
+#define LBM_NUM_FIELDS 14
 
 /* lbm_step flags */
 #define LBM_STEP_DIAG 1      /* reduce diagnostics on the last step */

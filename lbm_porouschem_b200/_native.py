@@ -32,8 +32,10 @@ LBM_MASK_SOLID = 3
 LBM_MASK_REACTIVE = 4
 
 (LBM_FIELD_F, LBM_FIELD_G, LBM_FIELD_MASK, LBM_FIELD_ALPHA, LBM_FIELD_REL, LBM_FIELD_RHO,
- LBM_FIELD_U, LBM_FIELD_T, LBM_FIELD_UPREV, LBM_FIELD_SCRATCH, LBM_FIELD_INLET) = range(11)
-LBM_NUM_FIELDS = 11
+ LBM_FIELD_U, LBM_FIELD_T, LBM_FIELD_UPREV, LBM_FIELD_SCRATCH, LBM_FIELD_INLET,
+ LBM_FIELD_PORO, LBM_FIELD_DARCY, LBM_FIELD_FORCH) = range(14)
+LBM_NUM_FIELDS = 14
+LBM_PORO_NONE, LBM_PORO_ERGUN, LBM_PORO_DARCY, LBM_PORO_DARCY_FORCHHEIMER = 0, 1, 2, 3
 
 LBM_STEP_DIAG = 1
 LBM_STEP_MACRO = 2
@@ -74,7 +76,7 @@ class lbm_desc(C.Structure):
         ("T_scale", C.c_double), ("dt_phys", C.c_double), ("heat_norm", C.c_double),
         ("gas_coef", C.c_double), ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19),
         ("rho0", C.c_double), ("T0", C.c_double), ("side", lbm_side_desc * 6),
-        ("viscosity", C.c_int32), ("reserved0", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
+        ("viscosity", C.c_int32), ("porous", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
     ]
 
 

@@ -181,6 +181,8 @@ class LatticeConfig:
         fill_sides(d.side, self.sides)
         d.viscosity = {"constant": N.LBM_VISC_CONSTANT, "sutherland": N.LBM_VISC_SUTHERLAND}[self.viscosity]
         d.suth_A, d.suth_Ts = self.suth_A, self.suth_Ts
+        d.porous = {"none": N.LBM_PORO_NONE, "ergun": N.LBM_PORO_ERGUN, "darcy": N.LBM_PORO_DARCY,
+                    "darcy_forchheimer": N.LBM_PORO_DARCY_FORCHHEIMER}[self.porous]
         return d
 
 

@@ -277,6 +277,10 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.Tref = (C)d.T_ref; p.Tscale = (C)d.T_scale; p.dtp = (C)d.dt_phys;
   p.heat_norm = (C)d.heat_norm; p.gas_coef = (C)d.gas_coef; p.alpha_flip = (C)d.alpha_flip;
   p.suthA = (C)d.suth_A; p.suthTs = (C)d.suth_Ts;
+  p.poro = (const C*)h->ptr[LBM_FIELD_PORO];
+  p.darcy = (const C*)h->ptr[LBM_FIELD_DARCY];
+  p.forch = (const C*)h->ptr[LBM_FIELD_FORCH];
+  p.poro_model = d.porous;
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

@@ -10,10 +10,13 @@ namespace lbm {
 namespace capi {
 
 // Collision code of the kernels: LBM_COLL_*, plus kCollSutherland with the Sutherland
-// viscosity (thermal modes only: THERM 1-3)
+// viscosity (thermal modes only: THERM 1-3), or plus kCollPorous with porous cells (no
+// temperature field: THERM 0)
 constexpr int kSB = kCollSutherland + LBM_COLL_BGK, kSM = kCollSutherland + LBM_COLL_MRT;
+constexpr int kPB = kCollPorous + LBM_COLL_BGK, kPM = kCollPorous + LBM_COLL_MRT;
 inline int collision_code(const lbm_desc& d) {
-  return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0);
+  return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0) +
+         (d.porous != LBM_PORO_NONE ? kCollPorous : 0);
 }
 
 // Dynamic shared memory above the 48 KB default is a per-device attribute of a kernel:
@@ -128,6 +131,7 @@ int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
   LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
+  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -156,6 +160,7 @@ int dispatch_batch(lbm_batch* b, cudaStream_t st) {
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
   LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
+  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -175,6 +180,7 @@ int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float*
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
   LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
+  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }

@@ -52,6 +52,10 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "Sutherland viscosity needs the temperature field and suth_A > 0");
   if (d->thermal && !(d->tauT_fluid > 0.5 && d->tauT_solid > 0.5))
     return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");
+  if (d->porous < LBM_PORO_NONE || d->porous > LBM_PORO_DARCY_FORCHHEIMER)
+    return fail(LBM_ERR_ARG, "unknown porous model");
+  if (d->porous && (d->thermal != LBM_THERMAL_NONE || d->viscosity != LBM_VISC_CONSTANT))
+    return fail(LBM_ERR_ARG, "porous cells run without the temperature field and with constant viscosity");
   for (int s = 0; s < 6; ++s) {
     const lbm_side_desc& sd = d->side[s];
     if (sd.active < 0 || sd.active > LBM_SIDE_ES) return fail(LBM_ERR_ARG, "side active must be 0, 1 (NEE) or 2 (ES)");
@@ -73,14 +77,18 @@ static int validate(const lbm_desc* d) {
 }
 
 // Sets bit 2 of *flag if a cell on an active (NEE) side, or its inner neighbour,
-// is solid: NEE replaces every population of a side cell from the post-stream
-// state of the inner neighbour (src/LBM/LBM2D/_boundary.py:54-101), which
-// presumes two fluid cells, and solid cells here carry no flow populations.
-static __global__ void __launch_bounds__(256) check_sides_kernel(const uint8_t* mask, int nx, int ny, int nz,
-                                                                 int active, size_t N, int* flag) {
+// is solid or porous: NEE replaces every population of a side cell from the
+// post-stream state of the inner neighbour (src/LBM/LBM2D/_boundary.py:54-101), which
+// presumes two fluid cells; solid cells here carry no flow populations, and the
+// boundary pass takes a cell's moments without the porous velocity correction.
+// poro: solid fraction per cell (float, or double when poro_f64), or null.
+static __global__ void __launch_bounds__(256) check_sides_kernel(const uint8_t* mask, const void* poro, int poro_f64,
+                                                                 int nx, int ny, int nz, int active, size_t N,
+                                                                 int* flag) {
   const size_t stride = (size_t)gridDim.x * blockDim.x;
   for (size_t c = (size_t)blockIdx.x * blockDim.x + threadIdx.x; c < N; c += stride) {
-    if (!(mask[c] & LBM_MASK_SOLID)) continue;
+    const bool porous = poro && (poro_f64 ? ((const double*)poro)[c] != 0.0 : ((const float*)poro)[c] != 0.0f);
+    if (!(mask[c] & LBM_MASK_SOLID) && !porous) continue;
     const int x = (int)(c % nx), y = (int)((c / nx) % ny), z = (int)(c / ((size_t)nx * ny));
     const bool near = ((active & 1) && x <= 1) || ((active & 2) && x >= nx - 2) || ((active & 4) && y <= 1) ||
                       ((active & 8) && y >= ny - 2) || ((active & 16) && z <= 1) || ((active & 32) && z >= nz - 2);
@@ -105,8 +113,10 @@ static int check_sides(lbm_handle* h, cudaStream_t st) {
   int flag = 0;
   LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
   if (active) {
-    check_sides_kernel<<<2 * sm_count(), 256, 0, st>>>((const uint8_t*)h->ptr[LBM_FIELD_MASK], h->d.nx, h->d.ny,
-                                                      h->d.nz, active, h->N, scratch_err(h));
+    check_sides_kernel<<<2 * sm_count(), 256, 0, st>>>((const uint8_t*)h->ptr[LBM_FIELD_MASK],
+                                                      h->d.porous ? h->ptr[LBM_FIELD_PORO] : nullptr,
+                                                      h->d.precision == LBM_PREC_FP64, h->d.nx, h->d.ny, h->d.nz,
+                                                      active, h->N, scratch_err(h));
     LBM_CUDA_TRY(cudaGetLastError());
     LBM_CUDA_TRY(cudaMemcpyAsync(&flag, scratch_err(h), sizeof(int), cudaMemcpyDeviceToHost, st));
     LBM_CUDA_TRY(cudaStreamSynchronize(st));
@@ -114,8 +124,8 @@ static int check_sides(lbm_handle* h, cudaStream_t st) {
   if (flag & 4) {
     LBM_CUDA_TRY(cudaMemsetAsync(scratch_err(h), 0, sizeof(int), st));
     return fail(LBM_ERR_ARG,
-                "a solid cell lies on an active (NEE) side or next to one; the two outer layers of an active "
-                "side must be fluid");
+                "a solid or porous cell lies on an active (NEE) side or next to one; the two outer layers of "
+                "an active side must be fluid");
   }
   return LBM_OK;
 }
@@ -181,6 +191,9 @@ int32_t lbm_required_bytes(const lbm_desc* d, int32_t field, size_t* bytes) {
     case LBM_FIELD_T: *bytes = d->thermal ? N * cb : 0; break;
     case LBM_FIELD_UPREV: *bytes = 3 * N * 4; break;
     case LBM_FIELD_INLET: *bytes = has_flowrate(*d) ? inlet_elems(*d) * cb : 0; break;
+    case LBM_FIELD_PORO: *bytes = d->porous ? N * cb : 0; break;
+    case LBM_FIELD_DARCY: *bytes = d->porous >= LBM_PORO_DARCY ? N * cb : 0; break;
+    case LBM_FIELD_FORCH: *bytes = d->porous == LBM_PORO_DARCY_FORCHHEIMER ? N * cb : 0; break;
     case LBM_FIELD_SCRATCH: {
       const Launch L = plan(*d, default_tx(*d));
       *bytes = scratch_bytes(L);
@@ -271,6 +284,9 @@ static int check_bound(lbm_handle* h) {
     return fail(LBM_ERR_UNBOUND, "pyrolysis needs ALPHA and REL bound");
   if (has_flowrate(h->d) && !h->ptr[LBM_FIELD_INLET])
     return fail(LBM_ERR_UNBOUND, "a flow-rate inlet needs INLET bound");
+  if (h->d.porous && (!h->ptr[LBM_FIELD_PORO] || (h->d.porous >= LBM_PORO_DARCY && !h->ptr[LBM_FIELD_DARCY]) ||
+                      (h->d.porous == LBM_PORO_DARCY_FORCHHEIMER && !h->ptr[LBM_FIELD_FORCH])))
+    return fail(LBM_ERR_UNBOUND, "porous cells need PORO (and DARCY / FORCH for their models) bound");
   return LBM_OK;
 }
 

@@ -63,8 +63,12 @@ template <> struct Store<__half> {
 
 constexpr int kNumDiag = 10;              // partial slots per block (order of lbm_diag fields)
 // Internal collision codes: LBM_COLL_BGK / LBM_COLL_MRT, plus kCollSutherland when the
-// viscosity follows the cell's temperature (LBM_VISC_SUTHERLAND)
+// viscosity follows the cell's temperature (LBM_VISC_SUTHERLAND), or plus kCollPorous
+// when the lattice has porous cells (lbm_desc.porous)
 constexpr int kCollSutherland = 2;
+constexpr int kCollPorous = 4;
+__host__ __device__ constexpr bool coll_sutherland(int coll) { return (coll & ~1) == kCollSutherland; }
+__host__ __device__ constexpr bool coll_porous(int coll) { return (coll & ~1) == kCollPorous; }
 
 // Flow-rate inlet state (LBM_FIELD_INLET, compute precision): slot 0 holds the
 // coefficient F/flow0 of the current step; after kInletHead slots come two halves,
@@ -118,6 +122,10 @@ struct StepParams {
   C rho0, T0;
   C pyA, pyb, pyEaR, pyTmin, Tref, Tscale, dtp, heat_norm, gas_coef, alpha_flip;  // pyEaR = Ea/R
   C suthA, suthTs;  // Sutherland viscosity (collision codes kCollSutherland + BGK/MRT)
+  const C* poro;   // porous cells (collision codes kCollPorous + BGK/MRT): solid fraction,
+  const C* darcy;  //   Darcy and Forchheimer coefficients per cell, and the model
+  const C* forch;  //   (LBM_PORO_*)
+  int poro_model;
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -292,12 +300,15 @@ struct Kern {
     rho = r; ux = jx; uy = jy; uz = jz;
   }
 
-  // feq9/feq19 (src/LBM/LBM2D/_evolution.py:213-225, eps = 1) split into the
-  // part even under e -> -e (ev) and the odd part (od): feq_k = ev + od,
+  // 1/(eps + 1e-12) of a fluid cell (eps = 1 - solid = 1), src/LBM/LBM2D/_evolution.py:216
+  __host__ __device__ static constexpr C kie() { return (C)1 / ((C)1 + (C)1e-12); }
+
+  // feq9/feq19 (src/LBM/LBM2D/_evolution.py:213-225; ie = 1/(eps + 1e-12), eps = 1 - solid)
+  // split into the part even under e -> -e (ev) and the odd part (od): feq_k = ev + od,
   // feq_opp(k) = ev - od.
   template <int k>
-  __device__ __forceinline__ static void feq_pair(const P& p, C rho, C ux, C uy, C uz, C usq, C& ev, C& od) {
-    constexpr C ie = (C)1 / ((C)1 + (C)1e-12);
+  __device__ __forceinline__ static void feq_pair(const P& p, C rho, C ux, C uy, C uz, C usq, C& ev, C& od,
+                                                  C ie = kie()) {
     const C eu = (C)L::ex(k) * ux + (C)L::ey(k) * uy + (C)L::ez(k) * uz;
     const C w = (C)L::w(k);
     if (p.eos == 1) {
@@ -308,32 +319,91 @@ struct Kern {
       od = w * rho * ((C)3.0 * eu);
     }
   }
-  __device__ __forceinline__ static C feq_rest(const P& p, C rho, C usq) {
-    constexpr C ie = (C)1 / ((C)1 + (C)1e-12);
+  __device__ __forceinline__ static C feq_rest(const P& p, C rho, C usq, C ie = kie()) {
     const C w = (C)L::w(0);
     return p.eos == 1 ? w * (rho - (C)1.5 * usq * ie) : w * rho * ((C)1.0 - (C)1.5 * usq * ie);
   }
   // Full equilibrium set of (rho, u) in F.
-  __device__ __forceinline__ static void feq_all(const P& p, C rho, C ux, C uy, C uz, C F[Q]) {
+  __device__ __forceinline__ static void feq_all(const P& p, C rho, C ux, C uy, C uz, C F[Q], C ie = kie()) {
     const C usq = ux * ux + uy * uy + uz * uz;
-    F[0] = feq_rest(p, rho, usq);
+    F[0] = feq_rest(p, rho, usq, ie);
     static_for<NP>([&](auto pp) {
       constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
       C ev, od;
-      feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+      feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od, ie);
       F[k] = ev + od;
       F[o] = ev - od;
     });
   }
 
-  // forceTermGuo, src/LBM/LBM2D/_evolution.py:284-298 (eps = 1)
+  // What drives one cell's collision besides its moments: ie = 1/(eps + 1e-12) of the
+  // equilibrium and the force of forceTermGuo (src/LBM/LBM2D/_evolution.py:254-261: the
+  // volume force, plus the Darcy drag in a porous cell).
+  struct Drive {
+    C ie, Fx, Fy, Fz;
+    bool force;
+  };
+  __device__ __forceinline__ static Drive plain_drive(const P& p) { return Drive{kie(), p.Fx, p.Fy, p.Fz, p.has_force != 0}; }
+
+  // A porous cell's drive: eps = 1 - solid and the drag of its model added to the volume
+  // force (darcy_force, src/LBM/LBM2D/_evolution.py:262-283; the 3D solver takes the lattice
+  // viscosity there instead of the kinetic one, LBM3D/_evolution.py:262-278).  s: solid
+  // fraction (0 < s < 1), velocity and density of the cell.
+  __device__ __forceinline__ static Drive porous_drive(const P& p, int c, C s, C rho, C ux, C uy, C uz) {
+    const C eps = (C)1 - s;
+    const C nu = L::DIM == 2 && p.eos == 0 ? p.nu / rho : p.nu;
+    const C v = sqrt(ux * ux + uy * uy + uz * uz);
+    C a;
+    if (p.poro_model == LBM_PORO_ERGUN) {
+      const C perm = eps * eps * eps / (((C)1.000001 - eps) * ((C)1.000001 - eps));
+      const C beta = (C)1.75 / sqrt((C)150 * eps * perm);
+      a = -nu / perm * eps - beta * v;
+    } else if (p.poro_model == LBM_PORO_DARCY) {
+      a = -eps * nu * p.darcy[c];
+    } else {
+      a = -eps * nu * p.darcy[c] - eps * p.forch[c] * v;
+    }
+    return Drive{(C)1 / (eps + (C)1e-12), p.Fx + a * ux, p.Fy + a * uy, p.Fz + a * uz, true};
+  }
+
+  // macro's velocity correction of a porous cell (src/LBM/LBM2D/_evolution.py:131-151) at
+  // its new density, then its drive.  Returns the plain drive for a cell that is not porous.
+  __device__ __forceinline__ static Drive porous_cell(const P& p, int c, C rho, C& ux, C& uy, C& uz) {
+    const C s = p.poro[c];
+    if (s == (C)0 || s == (C)1) return plain_drive(p);
+    const C eps = (C)1 - s;
+    const C nu = p.eos == 0 ? p.nu / rho : p.nu;  // kinetic_viscosity(i)
+    C div;
+    if (p.poro_model == LBM_PORO_DARCY) {
+      div = (C)1 + eps * nu * p.darcy[c] / (C)2;
+    } else {
+      C Dc, Fc;
+      if (p.poro_model == LBM_PORO_ERGUN) {
+        const C perm = eps * eps * eps / (((C)1.000001 - eps) * ((C)1.000001 - eps));
+        Dc = (C)1 / perm;
+        Fc = (C)1.75 / sqrt((C)150 * eps * eps * eps);
+      } else {
+        Dc = p.darcy[c];
+        Fc = p.forch[c];
+      }
+      const C c0 = (C)0.5 * ((C)1 + eps * nu / (C)2 * Dc);
+      const C c1 = (C)0.5 * eps * Fc;
+      const C v = sqrt(ux * ux + uy * uy + uz * uz);
+      div = c0 + sqrt(c0 * c0 + c1 * v);
+    }
+    const C idv = (C)1 / div;
+    ux *= idv; uy *= idv; uz *= idv;
+    return porous_drive(p, c, s, rho, ux, uy, uz);
+  }
+
+  // forceTermGuo, src/LBM/LBM2D/_evolution.py:284-298, force and ie of the drive
   template <int k>
-  __device__ __forceinline__ static C guo(const P& p, C rho, C ux, C uy, C uz, C pre) {
-    constexpr C ie = (C)1 / ((C)1 + (C)1e-12);
+  __device__ __forceinline__ static C guo(const P& p, C rho, C ux, C uy, C uz, C pre, const Drive& d) {
+    const C ie = d.ie;
     const C ex = (C)L::ex(k), ey = (C)L::ey(k), ez = (C)L::ez(k);
-    const C t1 = (ex - ux * ie) * p.Fx + (ey - uy * ie) * p.Fy + (ez - uz * ie) * p.Fz;
+    const C t1 = (ex - ux * ie) * d.Fx + (ey - uy * ie) * d.Fy + (ez - uz * ie) * d.Fz;
     const C eu = ex * ux + ey * uy + ez * uz;
-    const C eF = ex * p.Fx + ey * p.Fy + ez * p.Fz;
+    const C eF = ex * d.Fx + ey * d.Fy + ez * d.Fz;
     const C t = pre * (C)L::w(k) * ((C)3.0 * t1 + (C)9.0 * eu * eF * ie);
     return p.eos == 1 ? t : rho * t;
   }
@@ -342,8 +412,13 @@ struct Kern {
   // the post-collision populations over F.  Works on opposite-direction pairs.
   template <int COLL>
   __device__ __forceinline__ static void collide_flow(const P& p, C F[Q], C rho, C ux, C uy, C uz, C T = (C)0) {
+    collide_flow_d<COLL>(p, F, rho, ux, uy, uz, T, plain_drive(p));
+  }
+  template <int COLL>
+  __device__ __forceinline__ static void collide_flow_d(const P& p, C F[Q], C rho, C ux, C uy, C uz, C T,
+                                                        const Drive& dr) {
     C nu = p.nu;
-    if constexpr (COLL >= kCollSutherland) {
+    if constexpr (coll_sutherland(COLL)) {
       // Sutherland, src/LBM/LBM2D/_evolution.py:232-234, at the cell's temperature in kelvin
       const C TK = T * p.Tscale + p.Tref;
       nu = p.suthA * TK * sqrt(TK) / (TK + p.suthTs);
@@ -351,13 +426,13 @@ struct Kern {
     const C tau = (C)3 * (p.eos == 0 ? nu / rho : nu) + (C)0.5;
     const C itau = (C)1 / tau;
     const C usq = ux * ux + uy * uy + uz * uz;
-    const C fe0 = feq_rest(p, rho, usq);
+    const C fe0 = feq_rest(p, rho, usq, dr.ie);
     if constexpr ((COLL & 1) == LBM_COLL_BGK) {
       F[0] = F[0] - itau * (F[0] - fe0);
       static_for<NP>([&](auto pp) {
         constexpr int k = pk<L>(decltype(pp)::value), o = L::opp(k);
         C ev, od;
-        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od, dr.ie);
         F[k] = F[k] - itau * (F[k] - (ev + od));
         F[o] = F[o] - itau * (F[o] - (ev - od));
       });
@@ -369,7 +444,7 @@ struct Kern {
         constexpr int q = decltype(pp)::value;
         constexpr int k = pk<L>(q), o = L::opp(k);
         C ev, od;
-        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od);
+        feq_pair<k>(p, rho, ux, uy, uz, usq, ev, od, dr.ie);
         const C a = F[k] - (ev + od), b = F[o] - (ev - od);
         Sn[q] = a + b;
         Dn[q] = a - b;
@@ -422,11 +497,11 @@ struct Kern {
         F[o] -= E - O;
       });
     }
-    if (p.has_force) {
+    if (dr.force) {
       const C pre = (C)1.0 - (C)1.0 / (C)2.0 / tau;
       static_for<Q>([&](auto kk) {
         constexpr int k = decltype(kk)::value;
-        F[k] += guo<k>(p, rho, ux, uy, uz, pre);
+        F[k] += guo<k>(p, rho, ux, uy, uz, pre, dr);
       });
     }
   }
@@ -708,8 +783,10 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
     C F[Q];
     src.template flow<PYRO>(p, nb, c, nbits, F);
     K::moments(p, F, rho, ux, uy, uz);
+    typename K::Drive dr = K::plain_drive(p);
+    if constexpr (coll_porous(COLL)) dr = K::porous_cell(p, c, rho, ux, uy, uz);
     if (!peek) {
-      K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T);
+      K::template collide_flow_d<COLL>(p, F, rho, ux, uy, uz, T, dr);
       K::store_flow(p, c, F);
     }
     if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);  // after the store: fewer live registers
@@ -1192,8 +1269,14 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
   }
   if (!solid) {
     C F[Q];
-    K::feq_all(p, rho, ux, uy, uz, F);
-    K::template collide_flow<COLL>(p, F, rho, ux, uy, uz, T_in ? (C)T_in[c] : (C)0);
+    typename K::Drive dr = K::plain_drive(p);
+    if constexpr (coll_porous(COLL)) {
+      // the reference's first collision: eps-equilibrium and drag at the initial velocity
+      const C s = p.poro[c];
+      if (s != (C)0 && s != (C)1) dr = K::porous_drive(p, (int)c, s, rho, ux, uy, uz);
+    }
+    K::feq_all(p, rho, ux, uy, uz, F, dr.ie);
+    K::template collide_flow_d<COLL>(p, F, rho, ux, uy, uz, T_in ? (C)T_in[c] : (C)0, dr);
     K::store_flow(p, (int)c, F);
   }
   if constexpr (THERMAL) {

@@ -103,6 +103,28 @@ class Lattice:
         with self._on_stream():
             self.mask.copy_(torch.from_numpy(m).to(self.device))
 
+    def set_porous(self, fraction, darcy=None, forchheimer=None) -> None:
+        """Porous cells (``LatticeConfig.porous`` not "none"), before ``init``: the solid
+        fraction per cell (0 fluid, between 0 and 1 porous with porosity 1 - fraction; the
+        impermeable solid is the mask of ``set_geometry``) and, for the "darcy" and
+        "darcy_forchheimer" models, the Darcy / Forchheimer coefficients per cell, all in the
+        reference's (nx, ny[, nz]) layout or scalars (set_poro_Darcy /
+        set_poro_Darcy_Forchheimer, src/LBM/LBM2D/_io.py:152-172)."""
+        if self.cfg.porous == "none":
+            raise ValueError("the lattice has no porous model (LatticeConfig.porous)")
+        cd = _COMPUTE_DTYPE[self.cfg.precision]
+        with self._on_stream():
+            for fid, v in ((N.LBM_FIELD_PORO, fraction), (N.LBM_FIELD_DARCY, darcy),
+                           (N.LBM_FIELD_FORCH, forchheimer)):
+                if fid not in self.buf:
+                    continue
+                a = 0.0 if v is None else v
+                if np.isscalar(a):
+                    self._view(fid, cd).fill_(float(a))
+                else:
+                    flat = fortran_flat(np.asarray(a, dtype=np.float64).reshape(self.cfg.shape))
+                    self._view(fid, cd).copy_(torch.from_numpy(flat).to(self.device, cd))
+
     def _on_stream(self):
         """Issue torch work on the lattice's stream so it orders with the kernels."""
         return torch.cuda.stream(self.stream) if self.stream is not None else torch.cuda.stream(
@@ -260,6 +282,9 @@ class Lattice:
             out["uprev"] = self._view(N.LBM_FIELD_UPREV, torch.float32).cpu().numpy()
         if N.LBM_FIELD_INLET in self.buf:
             out["inlet"] = self._view(N.LBM_FIELD_INLET, cd).cpu().numpy()
+        for fid, name in ((N.LBM_FIELD_PORO, "poro"), (N.LBM_FIELD_DARCY, "darcy"), (N.LBM_FIELD_FORCH, "forch")):
+            if fid in self.buf:
+                out[name] = self._view(fid, cd).cpu().numpy()
         return out
 
     def save_checkpoint(self, path) -> str:
@@ -318,6 +343,10 @@ class Lattice:
                 put(self._view(N.LBM_FIELD_UPREV, torch.float32), "uprev")
             if N.LBM_FIELD_INLET in self.buf:
                 put(self._view(N.LBM_FIELD_INLET, cd), "inlet")
+            for fid, name in ((N.LBM_FIELD_PORO, "poro"), (N.LBM_FIELD_DARCY, "darcy"),
+                              (N.LBM_FIELD_FORCH, "forch")):
+                if fid in self.buf:
+                    put(self._view(fid, cd), name)
             N.check(self.lib.lbm_resume(self._h, int(step), self._s()))
         self._init_fields = {}
 

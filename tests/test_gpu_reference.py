@@ -48,6 +48,8 @@ def _run(cfg, z, steps):
     from lbm_porouschem_b200.lattice import Lattice
     lat = Lattice(cfg)
     lat.set_geometry(z["solid"])
+    if "sfrac" in z:   # porous cells: the fraction below 1 (the impermeable solid is the mask)
+        lat.set_porous(np.where(z["solid"], 0.0, z["sfrac"]), z["darcy"], z["forch"])
     lat.init(rho=z["rho0"], u=z["u0"], T=z["T0"])
     lat.step(steps)
     out = lat.fields()
@@ -81,6 +83,8 @@ def test_fp32_kernels_match_reference(oracle_mod, name):
     cfg32 = cfg.replace(precision="fp32")
     g = _run(cfg32, z, meta["steps"])
     o = oracle_mod.Oracle(cfg32, real="f32", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
+    if "sfrac" in z:
+        o.set_porous(z["sfrac"], z["darcy"], z["forch"])
     o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
     o.step(meta["steps"])
     r32 = o.fields()
