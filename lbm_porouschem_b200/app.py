@@ -267,8 +267,22 @@ def build_case(config: dict, logger: logging.Logger):
             lb.add_rho_solid(float(sdef.get("rho", 1.0)) * s)
         elif stype == "substract":
             lb.add_solid(-s)
+        elif stype == "poro" and is_poro:
+            # src/LBM/app.py:537-573: solid fraction 1 - porosity over the zone, the drag model's
+            # coefficients over it ("ergun" keeps the default SPHERICAL model)
+            zs = (s > 0) * 1.0
+            lb.add_solid((1.0 - float(sdef["porosity"])) * zs)
+            lb.add_rho_solid(float(sdef.get("rho", 1.0)) * zs)
+            model = sdef.get("porousModel")
+            if model == "darcy":
+                lb.set_poro_Darcy(zs, float(sdef["darcy"]))
+            elif model == "darcyForchheimer":
+                lb.set_poro_Darcy_Forchheimer(zs, float(sdef["darcy"]), float(sdef["forchheimer"]))
+            elif model not in (None, "ergun"):
+                raise ValueError(f"initialCondition.solid porousModel {model!r} not valid")
         elif stype == "poro":
-            raise NotImplementedError("porous solid zones (type 'poro') are not on the CUDA path")
+            # the reference skips a porous zone when module.porous_media is off (app.py:537)
+            logger.warning("initialCondition.solid of type 'poro' ignored: module.porous_media is off")
         else:
             raise ValueError(f"initialCondition.solid type {stype!r} not valid")
     lb.solid.from_numpy(np.clip(lb.solid._host, 0.0, 1.0))

@@ -25,7 +25,7 @@ from typing import Callable, Optional
 import numpy as np
 
 from .config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
-from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, SOURCE_TERM, VISCOSITY_MODEL
+from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, PORO_MODEL, SOURCE_TERM, VISCOSITY_MODEL
 from .vtk import PVDWriter, write_vts
 
 _BC_CODE = {BC.periodic: PERIODIC, BC.zeroGradient: ZERO_GRADIENT, BC.fixedValue: FIXED_VALUE}
@@ -172,6 +172,12 @@ class _SolverBase:
         self._pyro: Optional[dict] = None
         self._reactive: Optional[np.ndarray] = None
         self._lat = None
+        if self.PORO:
+            # src/LBM/LBM2D/_core.py:92-95: SPHERICAL (Ergun from the porosity) until a
+            # set_poro_* setter picks another model; per-cell coefficients
+            self.poro_model = PORO_MODEL.SPHERICAL
+            self.coefDarcy = Field(self, "coefDarcy", 0, 0.0)
+            self.coefForchheimer = Field(self, "coefForchheimer", 0, 0.0)
 
     # ------------------------------------------------------------ reference dunders
     def __repr__(self):
@@ -329,10 +335,26 @@ class _SolverBase:
         pass
 
     def set_poro_Darcy(self, s, coefDarcy):
-        raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
+        """Darcy drag in the porous cells (src/LBM/LBM2D/_io.py:152-164): the coefficient
+        (1/length^2) scaled by dx^2 over the zone s."""
+        self._need_poro()
+        self.poro_model = PORO_MODEL.DARCY
+        coefDarcy = coefDarcy * self.dx ** 2
+        self.init_field(self.coefDarcy, coefDarcy * np.asarray(s, dtype=np.float64))
 
     def set_poro_Darcy_Forchheimer(self, s, coefDarcy, coefForchheimer):
-        raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
+        """Darcy-Forchheimer drag (src/LBM/LBM2D/_io.py:165-172): coefficients scaled by dx^2
+        and dx over the zone s."""
+        self._need_poro()
+        self.poro_model = PORO_MODEL.DARCYFORCHHEIMER
+        coefDarcy = coefDarcy * self.dx ** 2
+        coefForchheimer = coefForchheimer * self.dx
+        self.init_field(self.coefDarcy, coefDarcy * np.asarray(s, dtype=np.float64))
+        self.init_field(self.coefForchheimer, coefForchheimer * np.asarray(s, dtype=np.float64))
+
+    def _need_poro(self):
+        if not self.PORO:
+            raise ValueError("porous setters need the solver created with isPoro=True")
 
     def set_specie(self, *a, **k):
         raise NotImplementedError("species transport is not on the CUDA path; use set_pyrolysis()")
@@ -444,6 +466,18 @@ class _SolverBase:
                 cfg.viscosity, cfg.suth_A, cfg.suth_Ts = "sutherland", As * self.dt / self.dx ** 2, Ts
             else:
                 cfg.nu = As * 273.15 ** 1.5 / (273.15 + Ts) * self.dt / self.dx ** 2
+        s = self.solid._host
+        if np.any((s > 0) & (s < 1)):
+            if not self.PORO:
+                raise ValueError("cells with a solid fraction between 0 and 1 need isPoro=True")
+            model = {PORO_MODEL.SPHERICAL: "ergun", PORO_MODEL.ERGUN: "ergun", PORO_MODEL.DARCY: "darcy",
+                     PORO_MODEL.DARCYFORCHHEIMER: "darcy_forchheimer"}.get(self.poro_model)
+            if model is None:
+                raise NotImplementedError(f"{self.poro_model} is not on the CUDA path")
+            if self.TEMPERATURE:
+                raise NotImplementedError("the heat exchange of porous cells (two temperature fields in a "
+                                          "cell, src/LBM/LBM2D/_evolution.py:186-202) is not on the CUDA path")
+            cfg.porous = model
         if self._pyro:
             pz = self._pyro
             cfg.pyro = True
@@ -459,8 +493,6 @@ class _SolverBase:
         """Equilibrium initialisation (src/LBM/LBM2D/_initialize.py:16-65) on the GPU."""
         from .lattice import Lattice
         s = self.solid._host
-        if np.any((s > 0) & (s < 1)):
-            raise NotImplementedError("porous (fractional) solid cells are not on the CUDA path yet")
         solid = s >= 1
         cfg = self._config()
         reactive = None
@@ -469,6 +501,9 @@ class _SolverBase:
         self._cfg = cfg
         self._lat = Lattice(cfg, device=device)
         self._lat.set_geometry(solid, reactive)
+        if cfg.porous != "none":
+            frac = np.where(solid, 0.0, s)
+            self._lat.set_porous(frac, self.coefDarcy._host, self.coefForchheimer._host)
         u = np.moveaxis(self.v._host, -1, 0)
         self._lat.init(rho=self.rho._host, u=u, T=self.TF.S._host if self.TEMPERATURE else 0.0)
         self._cache = None

@@ -124,10 +124,34 @@ def test_unsupported_options_stop_the_run():
     cfg["chemicalProperties"] = {"type": "cantera", "canteraFile": "mech.yaml"}
     with pytest.raises(NotImplementedError):
         build_case(cfg, _log())
+    # porous zones with the temperature field need the TF/TS exchange through them
     cfg = yaml.safe_load(CASE2D)
-    cfg["initialCondition"]["solid"]["s1"]["type"] = "poro"
+    cfg["module"]["porous_media"] = True
+    cfg["initialCondition"]["solid"]["s1"] = {"zone": "ALL", "type": "poro", "porosity": 0.5}
     with pytest.raises(NotImplementedError):
-        build_case(cfg, _log())
+        build_case(cfg, _log())._config()
+
+
+def test_porous_zone_maps_to_the_lattice():
+    """initialCondition.solid of type 'poro' (src/LBM/app.py:537-573): solid fraction
+    1 - porosity and the drag model's coefficients over the zone."""
+    cfg = yaml.safe_load(CASE2D)
+    cfg["module"]["temperature"] = False
+    cfg["module"]["chemistry"] = False
+    cfg.pop("chemicalProperties")
+    cfg["module"]["porous_media"] = True
+    cfg["initialCondition"]["solid"]["s1"] = {"zone": "ALL", "type": "poro", "porosity": 0.6,
+                                              "porousModel": "darcyForchheimer", "darcy": 2.0e6,
+                                              "forchheimer": 300.0}
+    lb = build_case(cfg, _log())
+    c = lb._config()
+    assert c.porous == "darcy_forchheimer" and c.thermal == "none"
+    s = lb.solid._host
+    zone = s > 0
+    assert zone.any() and np.allclose(s[zone], 0.4)
+    assert np.allclose(lb.coefDarcy._host[zone], 2.0e6 * lb.dx ** 2)
+    assert np.allclose(lb.coefForchheimer._host[zone], 300.0 * lb.dx)
+    assert np.all(lb.coefDarcy._host[~zone] == 0)
 
 
 @pytest.mark.gpu

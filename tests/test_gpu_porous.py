@@ -142,3 +142,34 @@ def test_porous_side_layers_rejected():
     with pytest.raises(LBMNativeError):
         lat.init(rho=1.0, u=(0.0, 0.0, 0.0))
     lat.close()
+
+
+def test_solver_surface_runs_porous_cells(oracle_mod):
+    """The reference's setters on the solver class (isPoro=True, add_solid with a fraction,
+    set_poro_Darcy; src/LBM/LBM2D/_io.py:123-164) drive the same porous run as the oracle."""
+    from lbm_porouschem_b200.flag import BC_FLOW
+    from lbm_porouschem_b200.solver import LBM2DSolver
+    nx, ny = 64, 32
+    lb = LBM2DSolver(nx, ny, 1, 1, 1, "poro", False, False, True, False)
+    lb.precision = "fp64"
+    lb.set_viscosity(0.1)
+    lb.set_BC(0, BC_FLOW.inlet)
+    lb.set_v_BC_value(0, [0.02, 0.0, 0.0])
+    lb.set_BC(1, BC_FLOW.outlet)
+    lb.set_rho_BC_value(1, 1.0)
+    zone = _zone((nx, ny), [(24.2, 15.3)], 7.1).reshape(nx, ny, 1) * 1.0
+    lb.add_solid(0.4 * zone)
+    lb.set_poro_Darcy(zone, 0.05)
+    lb.init_simulation()
+    for _ in range(200):
+        lb.step()
+    cfg = lb._cfg
+    assert cfg.porous == "darcy"
+    o = oracle_mod.Oracle(cfg, real="f64")
+    o.set_porous(0.4 * zone, 0.05 * zone, None)
+    o.init(np.zeros(zone.shape, dtype=bool), None, rho=1.0, u=(0.0, 0.0, 0.0))
+    o.step(200)
+    r = o.fields()
+    g = lb._lat.fields()
+    assert _rel(g["rho"], r["rho"]) < 1e-10
+    assert _rel(g["u"], r["u"]) < 1e-10
