@@ -55,6 +55,33 @@ def test_noalloc_matches_allocating_path_twice(precision):
     lat.close()
 
 
+@pytest.mark.parametrize("form", ["list", "dense"])
+@pytest.mark.parametrize("precision", ["fp32", "fp16"])
+def test_noalloc_matches_allocating_path_3d_lists(precision, form):
+    """The forms lattices from 65536 cells run: cell lists (kept in the lattice's own SCRATCH
+    buffer) or dense tiles, with the boundary kernel on its side stream (pressure inlet and
+    outlet on x), in 3D; two calls separated by steps in which reactive cells turn fluid."""
+    from lbm_porouschem_b200.lattice import Lattice
+    w = workloads.pyro3d(64, seed=13, ny=40, nz=32, precision=precision)   # 81920 cells
+    w.cfg.pyro_A = 1.2e11
+    w.cfg.heat_norm = 0.02
+    w.cfg.gas_coef = 0.05
+    w.init["T"] = 1.0
+    lat = Lattice(w.cfg.replace(bulk_form=form))
+    assert lat.bulk_kernel == form
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    for nsteps in (23, 60):
+        lat.step(nsteps)
+        a = _noalloc(lat)
+        b = _allocating(lat)
+        assert a["step"] == b["step"] == lat.nsteps
+        for k in KEYS:
+            assert a[k] == pytest.approx(b[k], rel=1e-6, abs=1e-12), k
+    assert (w.solid & ~lat.fields()["solid"]).any()     # cells converted between the calls
+    lat.close()
+
+
 def test_noalloc_rejects_lattice_beyond_static_scratch(monkeypatch):
     from lbm_porouschem_b200.config import LatticeConfig
     from lbm_porouschem_b200.lattice import Lattice
