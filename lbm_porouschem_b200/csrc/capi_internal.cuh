@@ -54,6 +54,13 @@ struct Launch {
   bool dense;         // bulk update by step_dense (persistent grid of bulk_blocks x kDThreads)
   int dense_smem;     // its dynamic shared memory (two stages)
   size_t N;
+  // x-face records: with an active x side the bulk kernel leaves the post-stream state of
+  // the cells at x = 1 / nx - 2 (the ones NEE extrapolates from) in SCRATCH, face-major,
+  // and the boundary kernel reads it there: face_cells = ny * nz records of face_vals
+  // values (Q + QT) per side, compute precision
+  size_t face_cells;
+  int face_vals;
+  size_t face_elem;   // bytes per value
   int list_base;      // first entry of the solid list (capacity of the fluid list)
   size_t list_cap;    // entries in both lists
   int list_nbb;       // blocks of the list build
@@ -113,6 +120,10 @@ inline Launch plan(const lbm_desc& d, int tx) {
   const bool force_list = d.bulk_form == 2 || (d.bulk_form == 0 && b && std::strcmp(b, "list") == 0);
   const bool force_dense = d.bulk_form == 3 || (d.bulk_form == 0 && b && std::strcmp(b, "dense") == 0);
   L.list = !force_tile && !force_dense && (force_list || L.N >= 65536);
+  const bool xface = (d.side[0].active || d.side[1].active) && d.nx >= 4;
+  L.face_cells = xface ? (size_t)d.ny * d.nz : 0;
+  L.face_vals = lat_q(d.dim) + (d.thermal ? lat_qt(d.dim) : 0);
+  L.face_elem = compute_bytes(d.precision);
   L.dense = force_dense;
   L.list_base = (int)((L.N + 64 + 31) / 32 * 32);
   L.list_cap = 2 * (size_t)L.list_base;
@@ -209,9 +220,14 @@ inline size_t list_bytes(const Launch& L) {
   if (!L.list) return 0;
   return (size_t)kLhSlots * 4 + (size_t)4 * L.list_nbb * 4 + 2 * L.list_cap * 4 + L.N * 4 + 2 * L.N * 4;
 }
-inline size_t scratch_bytes(const Launch& L) {
+inline size_t scratch_base_bytes(const Launch& L) {
   if (L.list || L.dense) return list_offset(L) + list_bytes(L);
   return (scratch_diag_doubles(L) * sizeof(double) + 255) / 256 * 256 + kCtrlBytes + 16;
+}
+inline size_t face_offset(const Launch& L) { return (scratch_base_bytes(L) + 255) / 256 * 256; }
+inline size_t scratch_bytes(const Launch& L) {
+  if (!L.face_cells) return scratch_base_bytes(L);
+  return face_offset(L) + 2 * (size_t)L.face_vals * L.face_cells * L.face_elem;
 }
 inline double* scratch_partials(lbm_handle* h) { return (double*)h->ptr[LBM_FIELD_SCRATCH]; }
 inline double* scratch_stage1(lbm_handle* h) {
@@ -307,6 +323,13 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
     p.flips = scratch_flips(h);
   }
   p.wait_spins = h->wait_spins;
+  p.face = nullptr;
+  p.face_sides = 0;
+  if (h->L.face_cells && h->ptr[LBM_FIELD_SCRATCH]) {
+    p.face = (C*)((char*)h->ptr[LBM_FIELD_SCRATCH] + face_offset(h->L));
+    p.face_sides = (d.side[0].active ? 1 : 0) | (d.side[1].active ? 2 : 0);
+  }
+  fastdiv_init((uint32_t)d.nx, p.nx_mul, p.nx_shr);
   return p;
 }
 

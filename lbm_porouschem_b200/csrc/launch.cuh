@@ -82,7 +82,8 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   // input half only and write disjoint slots, partial rows apart), so it runs on the
   // second stream and its blocks take the SMs that the persistent list kernel's blocks
   // leave as they finish; flip_cells waits for both
-  const bool fork = (L.list || L.dense) && L.nfaces > 0 && h->side != nullptr;
+  // (with x-face records the boundary kernel reads what the bulk kernel writes: it follows it)
+  const bool fork = (L.list || L.dense) && L.nfaces > 0 && h->side != nullptr && !p.face;
   if (fork) {
     cudaEventRecord(h->ev_fork, st);
     cudaStreamWaitEvent(h->side, h->ev_fork, 0);

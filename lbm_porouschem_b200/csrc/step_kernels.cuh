@@ -147,7 +147,27 @@ struct StepParams {
   int* pos;
   int* lhdr;
   int* flips;      // [2][N]: cells that turned fluid on a pass of parity 0 / 1
+  // x-face records (lbm SCRATCH): post-stream populations F[Q] then G[QT] of the cells at
+  // x = 1 (side 0) and x = nx - 2 (side 1), plane-major [side][value][y + ny z]; written by
+  // the bulk kernels, read by step_boundary; null: the boundary kernel pulls them itself
+  C* face;
+  int face_sides;  // bit s: side s records
+  uint32_t nx_mul; // c / nx = umulhi(c, nx_mul) >> nx_shr (exact for every 32-bit c)
+  int nx_shr;
 };
+
+// Division by the run-time constant nx with a multiply-high (Granlund & Montgomery, PLDI
+// 1994): m = ceil(2^(32+l) / d) - 2^32 with l = ceil(log2 d), then
+// q = (umulhi(n, m) + ((n - umulhi(n, m)) >> 1)) >> (l - 1) for every 32-bit n.
+inline void fastdiv_init(uint32_t d, uint32_t& m, int& l) {
+  l = 0;
+  while ((1ull << l) < d) ++l;
+  m = (uint32_t)((((1ull << l) - d) << 32) / d + 1);
+}
+__device__ __forceinline__ uint32_t fastdiv(uint32_t n, uint32_t m, int l) {
+  const uint32_t t = __umulhi(n, m);
+  return l == 0 ? n : (t + ((n - t) >> 1)) >> (l - 1);
+}
 
 // Cell-list entries (step_list<>): bit k (1..Q-1) of the bit word is set if
 // c + e_k is solid; kEntReactive marks a reactive cell, kEntDead an entry whose
@@ -738,6 +758,31 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
 // THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis, 3 two-field
 // (adiabatic fluid-solid links).
 
+// x-face record of cell c (post-stream F, and G with the temperature field) if it sits at
+// x = 1 or x = nx - 2 next to an active x side: step_boundary<> extrapolates that side from
+// it.  The bulk kernels update only cells off the active sides, so a record exists for a
+// face cell exactly when its inner cell is not on another active side (face_record).
+template <class L, class S, bool THERMAL>
+__device__ __forceinline__ void record_face(const StepParams<S>& p, int c, const typename Store<S>::C* F,
+                                            const typename Store<S>::C* G) {
+  const uint32_t j = fastdiv((uint32_t)c, p.nx_mul, p.nx_shr);  // y + ny z
+  const int x = c - (int)j * p.nx;
+  const int side = (x == 1 && (p.face_sides & 1)) ? 0 : ((x == p.nx - 2 && (p.face_sides & 2)) ? 1 : -1);
+  if (side < 0) return;
+  constexpr int FV = L::Q + (THERMAL ? L::QT : 0);
+  const size_t M = (size_t)p.ny * p.nz;
+  typename Store<S>::C* o = p.face + (size_t)side * FV * M + j;
+  static_for<L::Q>([&](auto kk) { o[(size_t)decltype(kk)::value * M] = F[decltype(kk)::value]; });
+  if constexpr (THERMAL)
+    static_for<L::QT>([&](auto kk) { o[(size_t)(L::Q + decltype(kk)::value) * M] = G[decltype(kk)::value]; });
+}
+template <class L, class S>
+__device__ __forceinline__ bool face_record(const StepParams<S>& p, int x, int y, int z) {
+  if (!p.face) return false;
+  if (!((x == 1 && (p.face_sides & 1)) || (x == p.nx - 2 && (p.face_sides & 2)))) return false;
+  return !Kern<L, S>::on_active_side(p, x, y, z);
+}
+
 // Where cell_update<> takes its post-stream populations from: straight from the
 // input buffers in HBM (this source), or from copies staged in shared memory
 // (StagedPull in list_kernel.cuh).
@@ -782,6 +827,7 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
   if (!solid) {
     C F[Q];
     src.template flow<PYRO>(p, nb, c, nbits, F);
+    if (p.face) record_face<L, S, THERMAL>(p, c, F, G);
     K::moments(p, F, rho, ux, uy, uz);
     typename K::Drive dr = K::plain_drive(p);
     if constexpr (coll_porous(COLL)) dr = K::porous_cell(p, c, rho, ux, uy, uz);
@@ -1073,6 +1119,22 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
   MState<L, S> s;
   if constexpr (PASS < 0) {
     const int c = x + p.nx * (y + p.ny * z);
+    if (face_record<L, S>(p, x, y, z)) {
+      // recorded by the bulk kernel of this pass: coalesced reads
+      constexpr int FV = L::Q + (THERMAL ? L::QT : 0);
+      const size_t M = (size_t)p.ny * p.nz;
+      const C* o = p.face + (size_t)(x == 1 ? 0 : 1) * FV * M + (size_t)y + (size_t)p.ny * z;
+      static_for<L::Q>([&](auto kk) { s.F[decltype(kk)::value] = o[(size_t)decltype(kk)::value * M]; });
+      K::moments(p, s.F, s.rho, s.ux, s.uy, s.uz);
+      s.T = 0;
+      if constexpr (THERMAL) {
+        if (needT) {
+          static_for<L::QT>([&](auto kk) { s.G[decltype(kk)::value] = o[(size_t)(L::Q + decltype(kk)::value) * M]; });
+          static_for<L::QT>([&](auto kk) { s.T += s.G[decltype(kk)::value]; });
+        }
+      }
+      return s;
+    }
     const Nbhd nb(x, y, z, p.nx, p.ny, p.nz);
     const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
     K::template pull_flow<PYRO>(p, nb, c, nbits, s.F);
