@@ -62,8 +62,17 @@ extern "C" {
  * through the Guo term (:254-298; the 3D solver takes the lattice viscosity there,
  * LBM3D/_evolution.py:262-278) and has its velocity corrected after the moments
  * (:131-151).  Cells with s >= 1 are the solid of the mask; s = 0 is fluid.  Constant
- * viscosity, no temperature field; the two outer cell layers of an active side must have
- * s = 0. */
+ * viscosity; the two outer cell layers of an active side must have s = 0.  Temperature:
+ * none, or LBM_THERMAL_TWOFIELD, where a porous cell carries both fields, TF in
+ * LBM_FIELD_G and TS in LBM_FIELD_GS.  TF lives in cells with s < 1 and bounces back at
+ * pure-solid neighbours; TS lives in cells with s > 0 and bounces back at pure-fluid
+ * neighbours (src/LBM/LBM2D/_evolution.py:30-100).  In a porous cell the two exchange
+ * heat, dH = h a (T_f,phys - T_s,phys) dt, TS gaining dH/(c_s rhos Ts_scale) and TF losing
+ * dH/(c_f rho T_scale), and with lbm_desc.radiation its surface radiates
+ * q = e sigma a_r/dx (T_ambient^4 - T_s,phys^4), TS gaining q dt/(c_s rhos Ts_scale), as
+ * sources of the next collision (TF's enters as geq(dS, u), TS's as w dS) (:186-202,
+ * src/LBM/LBM2D/_thermal.py:213-220; 3D LBM3D/_evolution.py:179-195).  Per cell
+ * (LBM_FIELD_XHEAT): h a, rhos and e a_r. */
 #define LBM_PORO_NONE 0
 #define LBM_PORO_ERGUN 1              /* SPHERICAL: permeability eps^3/(1.000001-eps)^2, Ergun drag */
 #define LBM_PORO_DARCY 2              /* coefficient LBM_FIELD_DARCY per cell */
@@ -144,6 +153,13 @@ typedef struct lbm_desc {
   double suth_A, suth_Ts; /* LBM_VISC_SUTHERLAND: lattice viscosity suth_A T^1.5/(T + suth_Ts) of the
                              cell's temperature T in kelvin (T_ref + T_scale*T); suth_A = As*dt/dx^2
                              of set_viscosity_sutherland(As, Ts) (src/LBM/LBM2D/_evolution.py:228-235) */
+  /* porous cells with two temperature fields (see LBM_PORO_*): */
+  double Ts_ref, Ts_scale;     /* solid temperature T_s,phys = T_s*Ts_scale + Ts_ref (set_solid_Trange) */
+  double cap_fluid, cap_solid; /* constant mass heat capacities c_f, c_s (TF.cm, TS.cm), J/(kg K) */
+  double dx_phys;              /* cell size (m), for the radiating surface per volume a_r/dx */
+  double T_ambient;            /* K (TS.Tambient, set_radiation) */
+  int32_t radiation;           /* 1: surface radiation (RADIATION_MODEL.SURFACE_UNIFORM) */
+  int32_t reserved1;
 } lbm_desc;
 
 /* Diagnostics (FP64 accumulation).  No reference counterpart except umax,
@@ -169,7 +185,7 @@ typedef struct lbm_diag {
 #define LBM_FIELD_REL 4     /* gas release per cell, 2 planes (compute precision) */
 #define LBM_FIELD_RHO 5     /* macro outputs: rho (compute precision) */
 #define LBM_FIELD_U 6       /* 3 planes */
-#define LBM_FIELD_T 7
+#define LBM_FIELD_T 7       /* 1 plane; 2 with porous cells and two temperature fields (TS of the porous cells) */
 #define LBM_FIELD_UPREV 8   /* 3 float32 planes, residual reference */
 #define LBM_FIELD_SCRATCH 9 /* reduction partials, control block, cell lists of the bulk update */
 #define LBM_FIELD_INLET 10  /* flow-rate inlet state (side 0 of type LBM_BC_FLOWRATE, else 0 bytes):
@@ -179,7 +195,9 @@ typedef struct lbm_diag {
 #define LBM_FIELD_PORO 11   /* solid fraction per cell (compute precision), with lbm_desc.porous */
 #define LBM_FIELD_DARCY 12  /* Darcy coefficient per cell (LBM_PORO_DARCY, _DARCY_FORCHHEIMER) */
 #define LBM_FIELD_FORCH 13  /* Forchheimer coefficient per cell (LBM_PORO_DARCY_FORCHHEIMER) */
-#define LBM_NUM_FIELDS 14
+#define LBM_FIELD_GS 14     /* TS populations of porous cells, 2 x QT planes (two fields with porous cells) */
+#define LBM_FIELD_XHEAT 15  /* 3 planes (compute precision): h*a, rhos, emissivity*a_r per cell */
+#define LBM_NUM_FIELDS 16
 
 /* lbm_step flags */
 #define LBM_STEP_DIAG 1      /* reduce diagnostics on the last step */
@@ -211,7 +229,10 @@ LBM_API int32_t lbm_bind(lbm_handle* h, int32_t field, void* dev_ptr, size_t byt
 LBM_API int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stream);
 
 /* Equilibrium initialisation from device planes rho[N], u[3N], T[N] (T may be
- * NULL without thermal), alpha[N] (NULL: 1 on reactive cells), all float32.
+ * NULL without thermal), alpha[N] (NULL: 1 on reactive cells), all float32.  With
+ * porous cells and two temperature fields T holds 2N values: the temperature of the
+ * cell's first field (TF where s < 1, TS in pure-solid cells), then TS of the porous
+ * cells (init_kernel sets TS.g = w TS.S in every cell, _initialize.py:62-63).
  * Compute precision is float32 for FP32/FP16 storage and float64 for FP64.  The solid mask must be bound first.  Replaces init_simulation /
  * init_kernel (src/LBM/LBM2D/_initialize.py:16-65, LBM3D/_initialize.py:17-77).
  * Resets the step counter and builds the cell lists of the bulk update (in

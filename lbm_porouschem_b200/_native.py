@@ -33,8 +33,8 @@ LBM_MASK_REACTIVE = 4
 
 (LBM_FIELD_F, LBM_FIELD_G, LBM_FIELD_MASK, LBM_FIELD_ALPHA, LBM_FIELD_REL, LBM_FIELD_RHO,
  LBM_FIELD_U, LBM_FIELD_T, LBM_FIELD_UPREV, LBM_FIELD_SCRATCH, LBM_FIELD_INLET,
- LBM_FIELD_PORO, LBM_FIELD_DARCY, LBM_FIELD_FORCH) = range(14)
-LBM_NUM_FIELDS = 14
+ LBM_FIELD_PORO, LBM_FIELD_DARCY, LBM_FIELD_FORCH, LBM_FIELD_GS, LBM_FIELD_XHEAT) = range(16)
+LBM_NUM_FIELDS = 16
 LBM_PORO_NONE, LBM_PORO_ERGUN, LBM_PORO_DARCY, LBM_PORO_DARCY_FORCHHEIMER = 0, 1, 2, 3
 
 LBM_STEP_DIAG = 1
@@ -77,6 +77,8 @@ class lbm_desc(C.Structure):
         ("gas_coef", C.c_double), ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19),
         ("rho0", C.c_double), ("T0", C.c_double), ("side", lbm_side_desc * 6),
         ("viscosity", C.c_int32), ("porous", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
+        ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
+        ("dx_phys", C.c_double), ("T_ambient", C.c_double), ("radiation", C.c_int32), ("reserved1", C.c_int32),
     ]
 
 

@@ -9,7 +9,8 @@ GPU; ``collision`` / ``precision`` select BGK|MRT and fp32|fp16|fp64), ``spaceCo
 (single-step pyrolysis of reactive solid zones), ``boundaryCondition`` (inlet / outlet / wall /
 periodic flow sides, fixedValue / zeroGradient / periodic temperature), ``geometry`` (sphere,
 cylinder, cone, box voxelised analytically at cell centres), ``initialCondition`` (flow, thermal,
-concrete / substract solids) and ``outputControl`` (log interval; ``vtk`` writes ``.vts`` files
+concrete / substract / poro solids, a porous zone with its heat exchange and, with
+``module.radiation`` and ``radiationProperties`` type mean_temp, its radiating border) and ``outputControl`` (log interval; ``vtk`` writes ``.vts`` files
 and the ``.pvd`` series; ``snapshot`` writes checkpoints).  ``timeControl.restart`` names a
 checkpoint to continue from instead of initialising (no reference counterpart).  Options outside
 that set stop the run with NotImplementedError naming the option.
@@ -22,7 +23,8 @@ import time
 
 import numpy as np
 
-from .flag import BC, BC_FLOW
+from .flag import BC, BC_FLOW, RADIATION_MODEL
+from .geometry import surface_weights
 
 _SIDES = ["left", "right", "down", "up", "forward", "back"]
 
@@ -90,6 +92,14 @@ def voxelise(shape: dict, grid, dx: float) -> np.ndarray:
     return inside.astype(np.float64)
 
 
+def _zone_names(zone, geo: dict) -> list:
+    if zone in ("ALL", "all"):
+        return list(geo)
+    if isinstance(zone, (list, tuple)):
+        return list(zone)
+    return [zone]
+
+
 def _zone_mask(zone, geo: dict, shape) -> np.ndarray:
     s = np.zeros(shape)
     if zone in ("ALL", "all"):
@@ -129,10 +139,9 @@ def build_case(config: dict, logger: logging.Logger):
     is_thermal = bool(module.get("temperature", False))
     is_poro = bool(module.get("porous_media", False))
     is_chem = bool(module.get("chemistry", False))
-    if module.get("radiation"):
-        raise NotImplementedError("module.radiation is not on the CUDA path")
+    is_rad = bool(module.get("radiation", False))
 
-    lb = lbm(x, y, z, dx, dt, name, is_thermal, is_chem, is_poro, False)
+    lb = lbm(x, y, z, dx, dt, name, is_thermal, is_chem, is_poro, is_rad)
     lb.set_collision(str(basic.get("collision", "bgk")))
     lb.set_precision(str(basic.get("precision", "fp32")))
 
@@ -184,6 +193,14 @@ def build_case(config: dict, logger: logging.Logger):
                 setter(prop + "_mixture")()
             else:
                 raise ValueError(f"{key}.{prop}.type {ptype!r} not valid")
+
+    # src/LBM/app.py:220-227: surface radiation to a uniform ambient temperature
+    rad = config.get("radiationProperties")
+    if is_rad and rad is not None:
+        if rad.get("type") == "mean_temp":
+            lb.set_radiation(RADIATION_MODEL.SURFACE_UNIFORM, float(rad.get("Tambient", 300)))
+        else:
+            raise ValueError(f"radiationProperties.type {rad.get('type')!r} not valid")
 
     chem = config.get("chemicalProperties")
     pyro_zone = None
@@ -268,11 +285,20 @@ def build_case(config: dict, logger: logging.Logger):
         elif stype == "substract":
             lb.add_solid(-s)
         elif stype == "poro" and is_poro:
-            # src/LBM/app.py:537-573: solid fraction 1 - porosity over the zone, the drag model's
-            # coefficients over it ("ergun" keeps the default SPHERICAL model)
+            # src/LBM/app.py:537-573: solid fraction 1 - porosity over the zone, its density,
+            # heat exchange surface and coefficient, radiating border and emissivity (the
+            # reference reads the key "emisssivity"), the drag model's coefficients over it
+            # ("ergun" keeps the default SPHERICAL model)
             zs = (s > 0) * 1.0
             lb.add_solid((1.0 - float(sdef["porosity"])) * zs)
             lb.add_rho_solid(float(sdef.get("rho", 1.0)) * zs)
+            lb.set_heat_exchange_surface(float(sdef.get("exchangeSurface", 1.0)) * zs)
+            lb.set_heat_exchange_coef(float(sdef.get("exchangeCoef", 1.0)) * zs)
+            if is_rad:
+                border = sum((surface_weights(geo[z], dim) for z in _zone_names(zone, geo)), np.zeros(lb._shape))
+                emis = float(sdef.get("emisssivity", sdef.get("emissivity", 1.0)))
+                lb.init_field(lb.TS.radiation_surface, border)
+                lb.init_field(lb.TS.emissivity, border * emis)
             model = sdef.get("porousModel")
             if model == "darcy":
                 lb.set_poro_Darcy(zs, float(sdef["darcy"]))

@@ -107,6 +107,14 @@ class LatticeConfig:
     suth_Ts: float = 0.0            #   (suth_A = As dt/dx^2 in lattice units, suth_Ts in K)
     porous: str = "none"            # porous cells (0 < solid fraction < 1): "none" | "ergun" | "darcy"
                                     #   | "darcy_forchheimer" (the reference's PORO_MODEL)
+    # two fields with porous cells: TF and TS exchange heat in porous cells
+    Ts_ref: float | None = None     # solid temperature mapping (TS.v_ref / v_scale); None: T_ref / T_scale
+    Ts_scale: float | None = None
+    cap_fluid: float = 1000.0       # mass heat capacities (J/(kg K)), TF.cm / TS.cm
+    cap_solid: float = 1000.0
+    dx_phys: float = 1.0            # cell size (m): radiation per volume, a / dx
+    radiation: bool = False         # surface radiation of porous cells (RADIATION_MODEL.SURFACE_UNIFORM)
+    T_ambient: float = 300.0        # K
 
     @property
     def shape(self) -> tuple:
@@ -183,7 +191,16 @@ class LatticeConfig:
         d.suth_A, d.suth_Ts = self.suth_A, self.suth_Ts
         d.porous = {"none": N.LBM_PORO_NONE, "ergun": N.LBM_PORO_ERGUN, "darcy": N.LBM_PORO_DARCY,
                     "darcy_forchheimer": N.LBM_PORO_DARCY_FORCHHEIMER}[self.porous]
+        d.Ts_ref = self.T_ref if self.Ts_ref is None else self.Ts_ref
+        d.Ts_scale = self.T_scale if self.Ts_scale is None else self.Ts_scale
+        d.cap_fluid, d.cap_solid, d.dx_phys = self.cap_fluid, self.cap_solid, self.dx_phys
+        d.T_ambient, d.radiation = self.T_ambient, int(self.radiation)
         return d
+
+    @property
+    def porous_heat(self) -> bool:
+        """Porous cells with two temperature fields: a porous cell carries TF and TS."""
+        return self.porous != "none" and self.thermal == "two_field"
 
 
 def fill_sides(arr, sides) -> None:

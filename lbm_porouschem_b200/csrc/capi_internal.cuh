@@ -39,6 +39,8 @@ inline int lat_qt(int dim) { return dim == 2 ? 5 : 7; }
 // Flow-rate inlet (side 0 of velocity type LBM_BC_FLOWRATE) and the element count of
 // its state in LBM_FIELD_INLET (compute precision).
 inline bool has_flowrate(const lbm_desc& d) { return d.side[0].active && d.side[0].v_type == LBM_BC_FLOWRATE; }
+// porous cells with two temperature fields: TS of the porous cells in LBM_FIELD_GS
+inline bool porous_heat(const lbm_desc& d) { return d.porous != LBM_PORO_NONE && d.thermal == LBM_THERMAL_TWOFIELD; }
 inline size_t inlet_elems(const lbm_desc& d) { return kInletHead + 2 * 4 * (size_t)d.ny * d.nz; }
 
 struct Launch {
@@ -297,6 +299,14 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.darcy = (const C*)h->ptr[LBM_FIELD_DARCY];
   p.forch = (const C*)h->ptr[LBM_FIELD_FORCH];
   p.poro_model = d.porous;
+  S* gs = (S*)h->ptr[LBM_FIELD_GS];
+  if (gs) { p.gsA = gs + (size_t)buf * QT * h->N; p.gsB = gs + (size_t)(buf ^ 1) * QT * h->N; }
+  p.xheat = (const C*)h->ptr[LBM_FIELD_XHEAT];
+  p.Trs = (C)d.Ts_ref; p.Tss = (C)d.Ts_scale;
+  p.cap_f = (C)d.cap_fluid; p.cap_s = (C)d.cap_solid;
+  p.sig_dx = d.dx_phys > 0 ? (C)(5.670374419e-8 / d.dx_phys) : (C)0;  // Stefan-Boltzmann, util/constant.py:20
+  p.Tamb4 = (C)(d.T_ambient * d.T_ambient * d.T_ambient * d.T_ambient);
+  p.radiation = d.radiation;
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

@@ -11,12 +11,20 @@ namespace capi {
 
 // Collision code of the kernels: LBM_COLL_*, plus kCollSutherland with the Sutherland
 // viscosity (thermal modes only: THERM 1-3), or plus kCollPorous with porous cells (no
-// temperature field: THERM 0)
+// temperature field, THERM 0, or two fields exchanging heat in them, THERM 4)
 constexpr int kSB = kCollSutherland + LBM_COLL_BGK, kSM = kCollSutherland + LBM_COLL_MRT;
 constexpr int kPB = kCollPorous + LBM_COLL_BGK, kPM = kCollPorous + LBM_COLL_MRT;
 inline int collision_code(const lbm_desc& d) {
   return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0) +
          (d.porous != LBM_PORO_NONE ? kCollPorous : 0);
+}
+// Temperature code of the kernels (THERM): 0 none, 1 conjugate, 2 conjugate + pyrolysis,
+// 3 two fields, 4 two fields with porous cells
+inline int therm_code(const lbm_desc& d) {
+  if (!d.thermal) return 0;
+  if (d.pyro) return 2;
+  if (d.thermal == LBM_THERMAL_TWOFIELD) return d.porous != LBM_PORO_NONE ? 4 : 3;
+  return 1;
 }
 
 // Dynamic shared memory above the 48 KB default is a per-device attribute of a kernel:
@@ -35,7 +43,7 @@ inline void opt_in_smem(std::atomic<unsigned long long>& done, K* kernel, int by
 
 template <class Lt, class S, int COLL, int THERM, int MODE>
 static void launch_list(const Launch& L, const StepParams<S>& p, cudaStream_t st) {
-  constexpr size_t smem = list_smem_bytes<Lt, S>(128);
+  constexpr size_t smem = list_smem_bytes<Lt, S, THERM>(128);
   if (smem > 0) {
     // opt in above the 48 KB default: with the static reduction buffer the total can
     // pass it even when the stages alone do not
@@ -120,7 +128,7 @@ static void launch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
 template <class Lt, class S>
 int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   const int coll = collision_code(h->d);
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
+  const int therm = therm_code(h->d);
   if (h->L.dense) {
     const char* why = dense_unsupported(h->d);
     if (why) return fail(LBM_ERR_ARG, why);
@@ -132,7 +140,7 @@ int dispatch_step(lbm_handle* h, StepParams<S> p, cudaStream_t st) {
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
   LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
-  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0)
+  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0) LBM_CASE(kPB, 4) LBM_CASE(kPM, 4)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }
@@ -155,7 +163,7 @@ template <class Lt, class S>
 int dispatch_batch(lbm_batch* b, cudaStream_t st) {
   const lbm_desc& d = b->hs[0]->d;
   const int coll = collision_code(d);
-  const int therm = d.thermal ? (d.pyro ? 2 : (d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
+  const int therm = therm_code(d);
 #define LBM_CASE(C_, T_) \
   if (coll == C_ && therm == T_) { launch_batch<Lt, S, C_, T_>(b, st); return LBM_OK; }
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
@@ -170,7 +178,7 @@ template <class Lt, class S>
 int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float* u, const float* T,
                   const float* alpha, int solid_bit, cudaStream_t st) {
   const int coll = collision_code(h->d);
-  const int therm = h->d.thermal ? (h->d.pyro ? 2 : (h->d.thermal == LBM_THERMAL_TWOFIELD ? 3 : 1)) : 0;
+  const int therm = therm_code(h->d);
   const int bs = 256;
   const unsigned nb = (unsigned)((h->N + bs - 1) / bs);
 #define LBM_CASE(C_, T_)                                                                       \
@@ -181,7 +189,7 @@ int dispatch_init(lbm_handle* h, StepParams<S> p, const float* rho, const float*
   LBM_CASE(LBM_COLL_BGK, 0) LBM_CASE(LBM_COLL_BGK, 1) LBM_CASE(LBM_COLL_BGK, 2) LBM_CASE(LBM_COLL_BGK, 3)
   LBM_CASE(LBM_COLL_MRT, 0) LBM_CASE(LBM_COLL_MRT, 1) LBM_CASE(LBM_COLL_MRT, 2) LBM_CASE(LBM_COLL_MRT, 3)
   LBM_CASE(kSB, 1) LBM_CASE(kSB, 2) LBM_CASE(kSB, 3) LBM_CASE(kSM, 1) LBM_CASE(kSM, 2) LBM_CASE(kSM, 3)
-  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0)
+  LBM_CASE(kPB, 0) LBM_CASE(kPM, 0) LBM_CASE(kPB, 4) LBM_CASE(kPM, 4)
 #undef LBM_CASE
   return fail(LBM_ERR_ARG, "unsupported collision/thermal combination");
 }

@@ -54,8 +54,16 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "thermal tau must be > 0.5");
   if (d->porous < LBM_PORO_NONE || d->porous > LBM_PORO_DARCY_FORCHHEIMER)
     return fail(LBM_ERR_ARG, "unknown porous model");
-  if (d->porous && (d->thermal != LBM_THERMAL_NONE || d->viscosity != LBM_VISC_CONSTANT))
-    return fail(LBM_ERR_ARG, "porous cells run without the temperature field and with constant viscosity");
+  if (d->porous && (d->thermal == LBM_THERMAL_CONJUGATE || d->viscosity != LBM_VISC_CONSTANT))
+    return fail(LBM_ERR_ARG, "porous cells run with constant viscosity, without temperature or with the two-field "
+                             "temperature");
+  if (d->porous && d->thermal == LBM_THERMAL_TWOFIELD &&
+      !(d->cap_fluid > 0 && d->cap_solid > 0 && d->T_scale != 0 && d->Ts_scale != 0 && d->dt_phys > 0 &&
+        (!d->radiation || d->dx_phys > 0)))
+    return fail(LBM_ERR_ARG, "the heat exchange of porous cells needs cap_fluid, cap_solid, dt_phys > 0, non-zero "
+                             "T_scale and Ts_scale, and dx_phys > 0 with radiation");
+  if (d->radiation && !(d->porous && d->thermal == LBM_THERMAL_TWOFIELD))
+    return fail(LBM_ERR_ARG, "radiation is a source of porous cells in the two-field temperature model");
   for (int s = 0; s < 6; ++s) {
     const lbm_side_desc& sd = d->side[s];
     if (sd.active < 0 || sd.active > LBM_SIDE_ES) return fail(LBM_ERR_ARG, "side active must be 0, 1 (NEE) or 2 (ES)");
@@ -188,12 +196,14 @@ int32_t lbm_required_bytes(const lbm_desc* d, int32_t field, size_t* bytes) {
     case LBM_FIELD_REL: *bytes = d->pyro ? 2 * N * cb : 0; break;
     case LBM_FIELD_RHO: *bytes = N * cb; break;
     case LBM_FIELD_U: *bytes = 3 * N * cb; break;
-    case LBM_FIELD_T: *bytes = d->thermal ? N * cb : 0; break;
+    case LBM_FIELD_T: *bytes = d->thermal ? (porous_heat(*d) ? 2 : 1) * N * cb : 0; break;
     case LBM_FIELD_UPREV: *bytes = 3 * N * 4; break;
     case LBM_FIELD_INLET: *bytes = has_flowrate(*d) ? inlet_elems(*d) * cb : 0; break;
     case LBM_FIELD_PORO: *bytes = d->porous ? N * cb : 0; break;
     case LBM_FIELD_DARCY: *bytes = d->porous >= LBM_PORO_DARCY ? N * cb : 0; break;
     case LBM_FIELD_FORCH: *bytes = d->porous == LBM_PORO_DARCY_FORCHHEIMER ? N * cb : 0; break;
+    case LBM_FIELD_GS: *bytes = porous_heat(*d) ? 2 * (size_t)lat_qt(d->dim) * N * s : 0; break;
+    case LBM_FIELD_XHEAT: *bytes = porous_heat(*d) ? 3 * N * cb : 0; break;
     case LBM_FIELD_SCRATCH: {
       const Launch L = plan(*d, default_tx(*d));
       *bytes = scratch_bytes(L);
@@ -287,6 +297,8 @@ static int check_bound(lbm_handle* h) {
   if (h->d.porous && (!h->ptr[LBM_FIELD_PORO] || (h->d.porous >= LBM_PORO_DARCY && !h->ptr[LBM_FIELD_DARCY]) ||
                       (h->d.porous == LBM_PORO_DARCY_FORCHHEIMER && !h->ptr[LBM_FIELD_FORCH])))
     return fail(LBM_ERR_UNBOUND, "porous cells need PORO (and DARCY / FORCH for their models) bound");
+  if (porous_heat(h->d) && (!h->ptr[LBM_FIELD_GS] || !h->ptr[LBM_FIELD_XHEAT]))
+    return fail(LBM_ERR_UNBOUND, "porous cells with two temperature fields need GS and XHEAT bound");
   return LBM_OK;
 }
 
@@ -316,6 +328,8 @@ int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector
       return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, viscosity, thermal and pyro");
     if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
     if (has_flowrate(h->d)) return fail(LBM_ERR_ARG, "batch members cannot have a flow-rate inlet");
+    if (porous_heat(h->d))
+      return fail(LBM_ERR_ARG, "batch members cannot have porous cells with two temperature fields");
     for (int j = 0; j < i; ++j)
       if (hs[j] == h) return fail(LBM_ERR_ARG, "a lattice appears twice in the batch");
   }

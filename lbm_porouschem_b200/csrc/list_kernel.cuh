@@ -300,7 +300,8 @@ template <class L, class S, int COLL, int THERM, int MODE>
 __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ StepParams<S> p) {
   constexpr int Q = L::Q, QT = L::QT;
   constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
-  constexpr bool STAGE = ListStaged<L, S>::value;
+  // the two fields with porous cells (THERM 4) pull directly
+  constexpr bool STAGE = ListStaged<L, S>::value && THERM != 4;
   using SP = StagedPull<L, S>;
   extern __shared__ __align__(16) unsigned char list_smem[];
   // modes 1 and 2 run only with an output flag set (lbm_step, lbm_compute_macro)
@@ -465,9 +466,9 @@ __global__ void __maxnreg__(BulkRegs<S>::v) step_list(const __grid_constant__ St
 }
 
 // Dynamic shared memory of step_list<> per block of `threads` (two stages).
-template <class L, class S>
+template <class L, class S, int THERM>
 constexpr size_t list_smem_bytes(int threads) {
-  return ListStaged<L, S>::value ? (size_t)2 * StagedPull<L, S>::kElems * threads * sizeof(S) : 0;
+  return ListStaged<L, S>::value && THERM != 4 ? (size_t)2 * StagedPull<L, S>::kElems * threads * sizeof(S) : 0;
 }
 
 }  // namespace lbm

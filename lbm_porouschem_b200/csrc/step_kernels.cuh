@@ -126,6 +126,14 @@ struct StepParams {
   const C* darcy;  //   Darcy and Forchheimer coefficients per cell, and the model
   const C* forch;  //   (LBM_PORO_*)
   int poro_model;
+  // porous cells with two temperature fields (THERM 4): TS populations of the porous cells
+  // (read and write halves), per cell h*a, rhos and emissivity*a_r (3 planes), the solid
+  // temperature mapping, heat capacities, sigma/dx, T_ambient^4 and the radiation switch
+  const S* gsA;
+  S* gsB;
+  const C* xheat;
+  C Trs, Tss, cap_f, cap_s, sig_dx, Tamb4;
+  int radiation;
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -295,6 +303,47 @@ struct Kern {
             idx = (size_t)L::opp(k) * p.N + c;
         }
         G[k] = Store<S>::ld(p.gA, idx, gshift<L, S, k>(p));
+      }
+    });
+  }
+
+  // Two fields with porous cells (THERM 4).  A cell's first temperature field (in G) is
+  // TF where the cell is fluid or porous and TS in a pure-solid cell.  TF crosses to fluid
+  // and porous neighbours and bounces back at pure-solid ones; TS of a pure-solid cell
+  // crosses to solid neighbours and to porous ones (whose TS is in GS) and bounces back at
+  // pure-fluid ones (src/LBM/LBM2D/_evolution.py:69-100).
+  __device__ __forceinline__ static void pull_thermal_ph(const P& p, const Nbhd& nb, int c, uint32_t nbits,
+                                                         bool solid, C G[QT]) {
+    static_for<QT>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if constexpr (k == 0) {
+        G[0] = Store<S>::ld(p.gA, c, gshift<L, S, 0>(p));
+      } else {
+        const int n = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
+        const S* src = p.gA;
+        size_t idx = (size_t)k * p.N + n;
+        if (((nbits >> L::opp(k)) & 1) != (uint32_t)solid) {
+          if (solid && p.poro[n] > (C)0) src = p.gsA;
+          else idx = (size_t)L::opp(k) * p.N + c;
+        }
+        G[k] = Store<S>::ld(src, idx, gshift<L, S, k>(p));
+      }
+    });
+  }
+  // TS of a porous cell: from the G of pure-solid neighbours, the GS of porous ones, and
+  // its own slot of the opposite direction at pure-fluid ones.
+  __device__ __forceinline__ static void pull_ts(const P& p, const Nbhd& nb, int c, uint32_t nbits, C GS[QT]) {
+    static_for<QT>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      if constexpr (k == 0) {
+        GS[0] = Store<S>::ld(p.gsA, c, gshift<L, S, 0>(p));
+      } else {
+        const int n = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
+        const S* src = p.gsA;
+        size_t idx = (size_t)k * p.N + n;
+        if ((nbits >> L::opp(k)) & 1) src = p.gA;
+        else if (!(p.poro[n] > (C)0)) idx = (size_t)L::opp(k) * p.N + c;
+        GS[k] = Store<S>::ld(src, idx, gshift<L, S, k>(p));
       }
     });
   }
@@ -529,12 +578,17 @@ struct Kern {
   // Thermal collision with source, one code path for fluid and solid cells:
   // fluid geq = TF.geq (advected), solid geq = w T (TS.geq, LBM2D/_thermal.py:162-166),
   // i.e. the fluid form with u = 0; source wt*dS (_evolution.py:54-58).
+  // USRC: the source enters as TF.geq(k, dS) with the cell's velocity (the two-field
+  // exchange source of a fluid or porous cell, src/LBM/LBM2D/_evolution.py:54-56), else as
+  // w dS (the pyrolysis heat sink of a solid cell, where u = 0 makes the two equal)
+  template <bool USRC = false>
   __device__ __forceinline__ static void collide_thermal(const P& p, C G[QT], C T, C itau, C ux, C uy, C uz,
                                                          C dS) {
     const C usq = ux * ux + uy * uy + uz * uz;
     {
       const C ge = (C)L::wt(0) * T * ((C)1.0 - (C)L::tc * usq);
-      G[0] = G[0] - itau * (G[0] - ge) + (C)L::wt(0) * dS;
+      const C src = USRC ? (C)L::wt(0) * dS * ((C)1.0 - (C)L::tc * usq) : (C)L::wt(0) * dS;
+      G[0] = G[0] - itau * (G[0] - ge) + src;
     }
     static_for<(QT - 1) / 2>([&](auto pp) {
       constexpr int k = pkt<L, QT>(decltype(pp)::value), o = L::opp(k);
@@ -542,9 +596,26 @@ struct Kern {
       const C wT = (C)L::wt(k) * T;
       const C ev = wT * ((C)1.0 + (C)L::tb * eu * eu - (C)L::tc * usq);
       const C od = wT * ((C)L::ta * eu);
-      const C src = (C)L::wt(k) * dS;
-      G[k] = G[k] - itau * (G[k] - (ev + od)) + src;
-      G[o] = G[o] - itau * (G[o] - (ev - od)) + src;
+      if constexpr (USRC) {
+        const C wd = (C)L::wt(k) * dS;
+        const C sev = wd * ((C)1.0 + (C)L::tb * eu * eu - (C)L::tc * usq);
+        const C sod = wd * ((C)L::ta * eu);
+        G[k] = G[k] - itau * (G[k] - (ev + od)) + (sev + sod);
+        G[o] = G[o] - itau * (G[o] - (ev - od)) + (sev - sod);
+      } else {
+        const C src = (C)L::wt(k) * dS;
+        G[k] = G[k] - itau * (G[k] - (ev + od)) + src;
+        G[o] = G[o] - itau * (G[o] - (ev - od)) + src;
+      }
+    });
+  }
+  // TS collision of a porous cell: towards w T_s with the source w dS_s (TS.geq,
+  // src/LBM/LBM2D/_thermal.py:162-166; _evolution.py:39-41, :56-57)
+  __device__ __forceinline__ static void collide_ts(const P& p, C GS[QT], C Ts, C dSs) {
+    static_for<QT>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      const C w = (C)L::wt(k);
+      GS[k] = GS[k] - p.itauT_s * (GS[k] - w * Ts) + w * dSs;
     });
   }
   // geq of (T, u) itself (initialisation).
@@ -567,6 +638,13 @@ struct Kern {
     static_for<Q>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       Store<S>::st(p.fB, (size_t)k * p.N + c, F[k], fshift<L, S, k>(p));
+    });
+  }
+  // Post-collision TS populations of porous cell c, in its own slots.
+  __device__ __forceinline__ static void store_ts(const P& p, int c, const C GS[QT]) {
+    static_for<QT>([&](auto kk) {
+      constexpr int k = decltype(kk)::value;
+      Store<S>::st(p.gsB, (size_t)k * p.N + c, GS[k], gshift<L, S, k>(p));
     });
   }
   // Post-collision temperature populations of cell c, in its own slots (the adiabatic
@@ -756,7 +834,8 @@ __device__ __noinline__ void neighbour_mean(const StepParams<S>& p, int x, int y
 
 // ------------------------------------------------------------------ kernels
 // THERM: 0 no temperature, 1 conjugate, 2 conjugate + pyrolysis, 3 two-field
-// (adiabatic fluid-solid links).
+// (adiabatic fluid-solid links), 4 two-field with porous cells (TF and TS in a porous cell,
+// exchanging heat there).
 
 // x-face record of cell c (post-stream F, and G with the temperature field) if it sits at
 // x = 1 or x = nx - 2 next to an active x side: step_boundary<> extrapolates that side from
@@ -781,6 +860,39 @@ __device__ __forceinline__ bool face_record(const StepParams<S>& p, int x, int y
   if (!p.face) return false;
   if (!((x == 1 && (p.face_sides & 1)) || (x == p.nx - 2 && (p.face_sides & 2)))) return false;
   return !Kern<L, S>::on_active_side(p, x, y, z);
+}
+
+// The TS field of porous cell c and the heat its two fields exchange (THERM 4): pulls and
+// sums TS, computes the exchange dH = h a (T_f,phys - T_s,phys) dt and the surface
+// radiation q = e sigma a_r/dx (T_amb^4 - T_s,phys^4) as the reference's macro does
+// (src/LBM/LBM2D/_evolution.py:186-202, _thermal.py:213-220), collides and stores TS with
+// its source, and returns TF's source -dH/(c_f rho T_scale).  Tf: the cell's TF, rho its
+// density.
+template <class L, class S>
+__device__ __forceinline__ typename Store<S>::C porous_heat(const StepParams<S>& p, const Nbhd& nb, int c,
+                                                            uint32_t nbits, typename Store<S>::C Tf,
+                                                            typename Store<S>::C rho, bool peek) {
+  using K = Kern<L, S>;
+  using C = typename Store<S>::C;
+  C GS[L::QT];
+  K::pull_ts(p, nb, c, nbits, GS);
+  C Ts = 0;
+  static_for<L::QT>([&](auto kk) { Ts += GS[decltype(kk)::value]; });
+  if (p.flags & LBM_STEP_MACRO) p.T_out[p.N + c] = Ts;  // second plane of the macro temperature
+  const C TsP = Ts * p.Tss + p.Trs;
+  const C dH = p.xheat[c] * ((Tf * p.Tscale + p.Tref) - TsP) * p.dtp;
+  const C rs = p.xheat[p.N + c];
+  C dSs = dH / p.cap_s / rs / p.Tss;
+  if (p.radiation) {
+    const C T2 = TsP * TsP;
+    const C q = p.xheat[2 * p.N + c] * p.sig_dx * (p.Tamb4 - T2 * T2);
+    dSs += q * p.dtp / p.cap_s / rs / p.Tss;
+  }
+  if (!peek) {
+    K::collide_ts(p, GS, Ts, dSs);
+    K::store_ts(p, c, GS);
+  }
+  return -dH / p.cap_f / rho / p.Tscale;
 }
 
 // Where cell_update<> takes its post-stream populations from: straight from the
@@ -815,11 +927,12 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
   using K = Kern<L, S>;
   using C = typename Store<S>::C;
   constexpr int Q = L::Q, QT = L::QT;
-  constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2;
+  constexpr bool THERMAL = THERM >= 1, PYRO = THERM == 2, PHEAT = THERM == 4;
   C G[QT > 0 ? QT : 1];
   C T = 0, dS = 0, rho = 0, ux = 0, uy = 0, uz = 0;
   if constexpr (THERMAL) {
-    src.template thermal<THERM == 3, RT>(p, nb, c, nbits, solid, G);
+    if constexpr (PHEAT) K::pull_thermal_ph(p, nb, c, nbits, solid, G);
+    else src.template thermal<THERM == 3, RT>(p, nb, c, nbits, solid, G);
     static_for<QT>([&](auto kk) { T += G[decltype(kk)::value]; });
   }
   bool solid_next = solid;
@@ -831,6 +944,9 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
     K::moments(p, F, rho, ux, uy, uz);
     typename K::Drive dr = K::plain_drive(p);
     if constexpr (coll_porous(COLL)) dr = K::porous_cell(p, c, rho, ux, uy, uz);
+    if constexpr (PHEAT) {
+      if (p.poro[c] > (C)0) dS = porous_heat<L, S>(p, nb, c, nbits, T, rho, peek);
+    }
     if (!peek) {
       K::template collide_flow_d<COLL>(p, F, rho, ux, uy, uz, T, dr);
       K::store_flow(p, c, F);
@@ -878,8 +994,8 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
   if constexpr (THERMAL) {
     if (!peek && !flipping) {
       const bool fl = !solid;
-      K::collide_thermal(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
-                         fl ? uz : (C)0, dS);
+      K::template collide_thermal<PHEAT>(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
+                                         fl ? uz : (C)0, dS);
       K::store_thermal(p, c, G);
     }
     if (diag) diag_thermal(p, acc, c, T);
@@ -1346,6 +1462,14 @@ __global__ void init_equilibrium_kernel(const __grid_constant__ StepParams<S> p,
     if (solid) K::geq_all((C)T_in[c], (C)0, (C)0, (C)0, G);
     else K::geq_all((C)T_in[c], ux, uy, uz, G);
     K::store_thermal(p, (int)c, G);
+  }
+  if constexpr (THERM == 4) {
+    // TS of a porous cell: w T_s, its temperature the second half of T_in
+    if (!solid && p.poro[c] > (C)0) {
+      C GS[QT];
+      K::geq_all((C)T_in[p.N + c], (C)0, (C)0, (C)0, GS);
+      K::store_ts(p, (int)c, GS);
+    }
   }
   if constexpr (PYRO) {
     p.alpha[c] = alpha_in ? (C)alpha_in[c] : ((m0 & LBM_MASK_REACTIVE) ? (C)1 : (C)0);

@@ -114,6 +114,28 @@ def packing(shape, rmin: float, rmax: float, porosity: float, seed: int, *,
     return mask
 
 
+# surface weight by the number of solid face neighbours (src/LBM/GEO/STL.py:216-259)
+_SURFACE_2D = {4: 0.0, 3: 1.0, 2: 1.414, 1: 2.0, 0: 4.0}
+_SURFACE_3D = {6: 0.0, 5: 1.0, 4: 1.414, 3: 2.0, 2: 3.0, 1: 4.0, 0: 6.0}
+
+
+def surface_weights(solid: np.ndarray, dim: int) -> np.ndarray:
+    """Surface weight of every solid cell of an (nx, ny, nz) indicator from its number of solid
+    face neighbours (in-plane ones in 2D), cells beyond the grid counting as empty; 0 for
+    empty cells.  The same table as the STL voxeliser's (stl_surface)."""
+    m = np.asarray(solid) > 0
+    pad = np.pad(m, 1)
+    n = np.zeros(m.shape, dtype=np.int32)
+    for ax in range(dim):
+        for sh in (1, -1):
+            n += np.roll(pad, sh, axis=ax)[1:-1, 1:-1, 1:-1]
+    table = _SURFACE_2D if dim == 2 else _SURFACE_3D
+    out = np.zeros(m.shape)
+    for k, w in table.items():
+        out[m & (n == k)] = w
+    return out
+
+
 def fortran_flat(a: np.ndarray) -> np.ndarray:
     """(nx,ny[,nz]) array -> flat device order c = x + nx*(y + ny*z)."""
     if a.ndim == 2:

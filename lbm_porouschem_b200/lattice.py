@@ -103,27 +103,43 @@ class Lattice:
         with self._on_stream():
             self.mask.copy_(torch.from_numpy(m).to(self.device))
 
-    def set_porous(self, fraction, darcy=None, forchheimer=None) -> None:
+    def set_porous(self, fraction, darcy=None, forchheimer=None, h=None, a=None, rho_solid=1.0,
+                   emissivity=None, radiation_surface=None) -> None:
         """Porous cells (``LatticeConfig.porous`` not "none"), before ``init``: the solid
         fraction per cell (0 fluid, between 0 and 1 porous with porosity 1 - fraction; the
         impermeable solid is the mask of ``set_geometry``) and, for the "darcy" and
         "darcy_forchheimer" models, the Darcy / Forchheimer coefficients per cell, all in the
         reference's (nx, ny[, nz]) layout or scalars (set_poro_Darcy /
-        set_poro_Darcy_Forchheimer, src/LBM/LBM2D/_io.py:152-172)."""
+        set_poro_Darcy_Forchheimer, src/LBM/LBM2D/_io.py:152-172).
+
+        With two temperature fields (``thermal="two_field"``) the porous cells also take the
+        heat exchange coefficient ``h`` and surface ``a`` (set_heat_exchange_coef / _surface),
+        the solid density ``rho_solid`` (add_rho_solid) and, with ``radiation``, the
+        ``emissivity`` and ``radiation_surface`` per cell (src/LBM/app.py:537-566)."""
         if self.cfg.porous == "none":
             raise ValueError("the lattice has no porous model (LatticeConfig.porous)")
         cd = _COMPUTE_DTYPE[self.cfg.precision]
+
+        def arr(v):
+            return np.full(self.cfg.shape, float(v)) if np.isscalar(v) else np.asarray(v, np.float64).reshape(self.cfg.shape)
+
         with self._on_stream():
             for fid, v in ((N.LBM_FIELD_PORO, fraction), (N.LBM_FIELD_DARCY, darcy),
                            (N.LBM_FIELD_FORCH, forchheimer)):
                 if fid not in self.buf:
                     continue
-                a = 0.0 if v is None else v
-                if np.isscalar(a):
-                    self._view(fid, cd).fill_(float(a))
+                x = 0.0 if v is None else v
+                if np.isscalar(x):
+                    self._view(fid, cd).fill_(float(x))
                 else:
-                    flat = fortran_flat(np.asarray(a, dtype=np.float64).reshape(self.cfg.shape))
+                    flat = fortran_flat(np.asarray(x, dtype=np.float64).reshape(self.cfg.shape))
                     self._view(fid, cd).copy_(torch.from_numpy(flat).to(self.device, cd))
+            if N.LBM_FIELD_XHEAT in self.buf:
+                ha = arr(0.0 if h is None else h) * arr(0.0 if a is None else a)
+                er = arr(0.0 if emissivity is None else emissivity) * arr(0.0 if radiation_surface is None
+                                                                           else radiation_surface)
+                planes = np.concatenate([fortran_flat(x) for x in (ha, arr(rho_solid), er)])
+                self._view(N.LBM_FIELD_XHEAT, cd).copy_(torch.from_numpy(planes).to(self.device, cd))
 
     def _on_stream(self):
         """Issue torch work on the lattice's stream so it orders with the kernels."""
@@ -141,14 +157,16 @@ class Lattice:
             flat = np.concatenate([fortran_flat(a[i].reshape(self.cfg.shape)) for i in range(ncomp)])
         return torch.from_numpy(flat.astype(np.float32)).to(self.device)
 
-    def init(self, rho=1.0, u=(0.0, 0.0, 0.0), T=0.0, alpha=None) -> None:
+    def init(self, rho=1.0, u=(0.0, 0.0, 0.0), T=0.0, alpha=None, Ts=None) -> None:
         """Equilibrium initialisation (reference init_kernel) from scalars or (nx,ny,nz) arrays.
 
-        ``u`` is a 3-tuple of scalars or an array shaped (3, nx, ny, nz)."""
+        ``u`` is a 3-tuple of scalars or an array shaped (3, nx, ny, nz).  ``Ts``: with two
+        temperature fields, the solid temperature (TS.S) where it differs from ``T`` (TF.S):
+        pure-solid cells and the TS of porous cells start from it."""
         with self._on_stream():
-            self._init(rho, u, T, alpha)
+            self._init(rho, u, T, alpha, Ts)
 
-    def _init(self, rho, u, T, alpha) -> None:
+    def _init(self, rho, u, T, alpha, Ts=None) -> None:
         cfg = self.cfg
         r = self._plane(rho)
         if isinstance(u, (tuple, list)) and all(np.isscalar(x) for x in u):
@@ -157,11 +175,16 @@ class Lattice:
         else:
             uu = self._plane(u, 3)
         tt = self._plane(T) if cfg.thermal != "none" else None
+        tin = tt
+        if cfg.thermal == "two_field" and (Ts is not None or cfg.porous_heat):
+            ts = self._plane(T if Ts is None else Ts)
+            tt = torch.where((self.mask & 1).bool(), ts, tt)
+            tin = torch.cat([tt, ts]) if cfg.porous_heat else tt
         aa = self._plane(alpha) if (cfg.pyro and alpha is not None) else None
         self._init_fields = {"rho": r, "u": uu, "T": tt}
         N.check(self.lib.lbm_init_equilibrium(
             self._h, ctypes.c_void_p(r.data_ptr()), ctypes.c_void_p(uu.data_ptr()),
-            ctypes.c_void_p(tt.data_ptr()) if tt is not None else None,
+            ctypes.c_void_p(tin.data_ptr()) if tin is not None else None,
             ctypes.c_void_p(aa.data_ptr()) if aa is not None else None, self._s()))
         # macro planes start at the initial state (solid cells keep these values)
         if N.LBM_FIELD_RHO in self.buf:
@@ -169,7 +192,7 @@ class Lattice:
             self._view(N.LBM_FIELD_RHO, cd).copy_(r.to(cd))
             self._view(N.LBM_FIELD_U, cd).copy_(uu.to(cd))
             if tt is not None:
-                self._view(N.LBM_FIELD_T, cd).copy_(tt.to(cd))
+                self._view(N.LBM_FIELD_T, cd).copy_(tin.to(cd))
         if N.LBM_FIELD_UPREV in self.buf:
             # residual reference: the initial velocity (the first residual measures
             # the change since the start)
@@ -252,12 +275,18 @@ class Lattice:
         u = np.stack([from_flat(uf[i * n:(i + 1) * n], cfg.shape) for i in range(3)])
         out = {"rho": rho, "u": u}
         if cfg.thermal != "none":
-            out["T"] = from_flat(self._view(N.LBM_FIELD_T, cd).cpu().numpy(), cfg.shape)
+            out["T"] = from_flat(self._view(N.LBM_FIELD_T, cd)[:n].cpu().numpy(), cfg.shape)
         if cfg.pyro:
             out["alpha"] = from_flat(self._view(N.LBM_FIELD_ALPHA, cd).cpu().numpy(), cfg.shape)
         par = self.nsteps & 1
         m = self.mask.cpu().numpy()
         out["solid"] = from_flat(((m >> par) & 1).astype(bool), cfg.shape)
+        if cfg.porous_heat:
+            # TS: of porous cells the second plane of the macro temperature, of pure-solid
+            # cells their one field, 0 in pure-fluid cells
+            poro = self._view(N.LBM_FIELD_PORO, cd).cpu().numpy()
+            ts = np.where(poro > 0, self._view(N.LBM_FIELD_T, cd)[n:].cpu().numpy(), 0.0)
+            out["Ts"] = np.where(out["solid"], out["T"], from_flat(ts, cfg.shape))
         return out
 
     # ------------------------------------------------------- checkpoint / resume
@@ -282,9 +311,12 @@ class Lattice:
             out["uprev"] = self._view(N.LBM_FIELD_UPREV, torch.float32).cpu().numpy()
         if N.LBM_FIELD_INLET in self.buf:
             out["inlet"] = self._view(N.LBM_FIELD_INLET, cd).cpu().numpy()
-        for fid, name in ((N.LBM_FIELD_PORO, "poro"), (N.LBM_FIELD_DARCY, "darcy"), (N.LBM_FIELD_FORCH, "forch")):
+        for fid, name in ((N.LBM_FIELD_PORO, "poro"), (N.LBM_FIELD_DARCY, "darcy"), (N.LBM_FIELD_FORCH, "forch"),
+                          (N.LBM_FIELD_XHEAT, "xheat")):
             if fid in self.buf:
                 out[name] = self._view(fid, cd).cpu().numpy()
+        if N.LBM_FIELD_GS in self.buf:
+            out["gs"] = self._view(N.LBM_FIELD_GS, sd).view(2, cfg.QT, n)[half].cpu().numpy()
         return out
 
     def save_checkpoint(self, path) -> str:
@@ -344,9 +376,11 @@ class Lattice:
             if N.LBM_FIELD_INLET in self.buf:
                 put(self._view(N.LBM_FIELD_INLET, cd), "inlet")
             for fid, name in ((N.LBM_FIELD_PORO, "poro"), (N.LBM_FIELD_DARCY, "darcy"),
-                              (N.LBM_FIELD_FORCH, "forch")):
+                              (N.LBM_FIELD_FORCH, "forch"), (N.LBM_FIELD_XHEAT, "xheat")):
                 if fid in self.buf:
                     put(self._view(fid, cd), name)
+            if N.LBM_FIELD_GS in self.buf:
+                put(self._view(N.LBM_FIELD_GS, sd).view(2, cfg.QT, n)[half], "gs")
             N.check(self.lib.lbm_resume(self._h, int(step), self._s()))
         self._init_fields = {}
 

@@ -25,7 +25,8 @@ from typing import Callable, Optional
 import numpy as np
 
 from .config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
-from .flag import BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, PORO_MODEL, SOURCE_TERM, VISCOSITY_MODEL
+from .flag import (BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, PORO_MODEL, RADIATION_MODEL, SOURCE_TERM,
+                   VISCOSITY_MODEL)
 from .vtk import PVDWriter, write_vts
 
 _BC_CODE = {BC.periodic: PERIODIC, BC.zeroGradient: ZERO_GRADIENT, BC.fixedValue: FIXED_VALUE}
@@ -92,10 +93,14 @@ class ScalarFieldView:
         self.derived = False
         self.cond: Optional[float] = None
         self.cm: Optional[float] = None
-        # radiation fields the reference's driver fills (src/LBM/app.py); radiation itself
-        # is not on the CUDA path (set_radiation raises)
+        # heat exchange and radiation of porous cells (TS, src/LBM/LBM2D/_thermal.py:110-120):
+        # per-cell exchange coefficient and surface, radiating surface and emissivity
+        self.exchangeCoef = Field(solver, name + "_exchangeCoef")
+        self.exchangeSurface = Field(solver, name + "_exchangeSurface")
         self.radiation_surface = Field(solver, name + "_radiation_surface")
         self.emissivity = Field(solver, name + "_emissivity")
+        self.radiation_model = RADIATION_MODEL.NONE
+        self.Tambient = 300.0
 
     def get_physical_value(self, v):
         return v * self.v_scale + self.v_ref
@@ -329,10 +334,12 @@ class _SolverBase:
         self.TS.set_s_BC_value(i, T)
 
     def set_heat_exchange_surface(self, surface):
-        pass  # binary masks only: no exchange (two fields) or exchange through the interface (conjugate)
+        """Exchange surface of the porous cells (src/LBM/LBM2D/_io.py:133-135)."""
+        self.init_field(self.TS.exchangeSurface, surface)
 
     def set_heat_exchange_coef(self, coef):
-        pass
+        """Exchange coefficient of the porous cells (src/LBM/LBM2D/_io.py:136-138)."""
+        self.init_field(self.TS.exchangeCoef, coef)
 
     def set_poro_Darcy(self, s, coefDarcy):
         """Darcy drag in the porous cells (src/LBM/LBM2D/_io.py:152-164): the coefficient
@@ -360,8 +367,13 @@ class _SolverBase:
         raise NotImplementedError("species transport is not on the CUDA path; use set_pyrolysis()")
 
     def set_radiation(self, model, param):
-        raise NotImplementedError("surface radiation of the solid (src/LBM/LBM2D/_thermal.py:213-220) is not on "
-                                  "the CUDA path")
+        """Surface radiation of the porous cells to the ambient temperature ``param`` (K)
+        (src/LBM/LBM2D/_io.py:259-271, _thermal.py:213-220); needs isRadiation."""
+        if model == RADIATION_MODEL.SURFACE_UNIFORM:
+            self.TS.radiation_model = model
+            self.TS.Tambient = float(param)
+        elif model != RADIATION_MODEL.NONE:
+            raise NotImplementedError(f"radiation model {model} is not on the CUDA path (SURFACE_UNIFORM is)")
 
     def add_reaction(self, *a, **k):
         raise NotImplementedError("general reaction networks are not on the CUDA path; use set_pyrolysis()")
@@ -475,8 +487,16 @@ class _SolverBase:
             if model is None:
                 raise NotImplementedError(f"{self.poro_model} is not on the CUDA path")
             if self.TEMPERATURE:
-                raise NotImplementedError("the heat exchange of porous cells (two temperature fields in a "
-                                          "cell, src/LBM/LBM2D/_evolution.py:186-202) is not on the CUDA path")
+                if self._pyro:
+                    raise NotImplementedError("pyrolysis with porous cells is not on the CUDA path")
+                # two fields in a porous cell, exchanging heat there and radiating
+                # (src/LBM/LBM2D/_evolution.py:186-202)
+                cfg.Ts_ref, cfg.Ts_scale = self.TS.v_ref, self.TS.v_scale
+                cfg.cap_fluid = 1000.0 if self.TF.cm is None else self.TF.cm   # capacity_m defaults,
+                cfg.cap_solid = 1000.0 if self.TS.cm is None else self.TS.cm   # _thermal.py:18, :128
+                cfg.dt_phys, cfg.dx_phys = self.dt, self.dx
+                if self.RADIATION and self.TS.radiation_model == RADIATION_MODEL.SURFACE_UNIFORM:
+                    cfg.radiation, cfg.T_ambient = True, self.TS.Tambient
             cfg.porous = model
         if self._pyro:
             pz = self._pyro
@@ -503,9 +523,15 @@ class _SolverBase:
         self._lat.set_geometry(solid, reactive)
         if cfg.porous != "none":
             frac = np.where(solid, 0.0, s)
-            self._lat.set_porous(frac, self.coefDarcy._host, self.coefForchheimer._host)
+            heat = {}
+            if cfg.porous_heat:
+                heat = dict(h=self.TS.exchangeCoef._host, a=self.TS.exchangeSurface._host, rho_solid=self.rhos._host,
+                            emissivity=self.TS.emissivity._host, radiation_surface=self.TS.radiation_surface._host)
+            self._lat.set_porous(frac, self.coefDarcy._host, self.coefForchheimer._host, **heat)
         u = np.moveaxis(self.v._host, -1, 0)
-        self._lat.init(rho=self.rho._host, u=u, T=self.TF.S._host if self.TEMPERATURE else 0.0)
+        two = cfg.thermal == "two_field"
+        self._lat.init(rho=self.rho._host, u=u, T=self.TF.S._host if self.TEMPERATURE else 0.0,
+                       Ts=self.TS.S._host if two else None)
         self._cache = None
         self._cache_step = -1
 
@@ -549,6 +575,8 @@ class _SolverBase:
             return out
         if name == "solid":
             return st["solid"].astype(np.float64)
+        if name == "TS" and "Ts" in st:   # porous cells carry a TS of their own
+            return np.where(self.solid._host > 0, st["Ts"], st["T"])
         if name in ("TF", "TS"):
             return st["T"].copy()
         return host.copy()

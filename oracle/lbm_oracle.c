@@ -95,7 +95,16 @@ typedef struct orc_cfg {
                               * ones (collision :96-100 writes TS.g in place).  1 reproduces that. */
     int poro_model;          /* porous cells (0 < solid < 1, src/LBM/util/flag.py PORO_MODEL): 0 none,
                               * 1 SPHERICAL (Ergun from the porosity), 2 DARCY, 3 DARCYFORCHHEIMER */
+    /* Two fields with porous cells: a porous cell carries both TF and TS, which exchange
+     * heat there (src/LBM/LBM2D/_evolution.py:186-202, LBM3D/_evolution.py:179-195) */
+    double Ts_ref, Ts_scale; /* TS.v_ref, TS.v_scale (set_solid_Trange, LBM2D/_io.py:253-256) */
+    double cap_fluid, cap_solid; /* TF.cm, TS.cm: constant capacity_m (LBM2D/_thermal.py:86-88, :189-191) */
+    double dx_phys;          /* cell size: radiation per volume a/dx (_thermal.py:213-220) */
+    int radiation;           /* 1: RADIATION_MODEL.SURFACE_UNIFORM (set_radiation, _io.py:259-271) */
+    double T_ambient;        /* TS.Tambient (K) */
 } orc_cfg;
+
+#define ORC_SIGMA 5.670374419e-8   /* Stefan-Boltzmann constant, src/LBM/util/constant.py:20 */
 
 /* mask bits */
 #define ORC_SOLID 1u
@@ -116,6 +125,10 @@ typedef struct orc {
     REAL *f, *F, *g, *G;
     REAL *rho, *u, *T, *dS, *alpha, *rel;
     REAL *sfrac, *cdarcy, *cforch;  /* solid fraction, Darcy and Forchheimer coefficients per cell */
+    /* two fields with porous cells (NULL otherwise): TS populations of porous cells
+     * (pure-solid cells keep theirs in g/G), their temperature and source, and the
+     * per-cell exchangeCoef, exchangeSurface, rhos, emissivity, radiation_surface */
+    REAL *gs, *Gs, *Ts, *dSs, *xh, *xa, *rhos, *emis, *rsurf;
     uint8_t *mask, *mask_next;
     /* flow-rate inlet on side 0, per side cell j = y + ny*z: what the reference's
      * updateBC_kernel reads (rho*u_x at x = 0, u at x = 1, 3 per cell) and the
@@ -201,6 +214,8 @@ static inline REAL eps_of(const orc* o, long c) { return (REAL)1.0 - o->sfrac[c]
 static inline int is_porous(const orc* o, long c) {
     return o->c.poro_model != 0 && o->sfrac[c] != 0 && o->sfrac[c] != 1;
 }
+/* porous cells carry a TS field of their own (two fields with porous cells) */
+static inline int porous_ts(const orc* o, long c) { return o->gs != NULL && is_porous(o, c); }
 /* TemperatureFluid.geq5 / geq7: src/LBM/LBM2D/_thermal.py:54-61, LBM3D/_thermal.py:54-61 */
 static inline REAL geq_fluid(const orc* o, int k, REAL T, const REAL* u) {
     REAL eu = (REAL)o->e[k][0]*u[0] + (REAL)o->e[k][1]*u[1] + (REAL)o->e[k][2]*u[2];
@@ -375,6 +390,17 @@ orc* orc_create(const orc_cfg* cfg) {
     o->cdarcy = (REAL*)calloc(N, sizeof(REAL));
     o->cforch = (REAL*)calloc(N, sizeof(REAL));
     o->mask_next = (uint8_t*)calloc(N, 1);
+    if (o->c.thermal == 2 && o->c.poro_model != 0) {
+        o->gs = (REAL*)calloc(N*o->QT, sizeof(REAL));
+        o->Gs = (REAL*)calloc(N*o->QT, sizeof(REAL));
+        o->Ts = (REAL*)calloc(N, sizeof(REAL));
+        o->dSs = (REAL*)calloc(N, sizeof(REAL));
+        o->xh = (REAL*)calloc(N, sizeof(REAL));
+        o->xa = (REAL*)calloc(N, sizeof(REAL));
+        o->rhos = (REAL*)calloc(N, sizeof(REAL));
+        o->emis = (REAL*)calloc(N, sizeof(REAL));
+        o->rsurf = (REAL*)calloc(N, sizeof(REAL));
+    }
     long M = (long)o->c.ny * o->c.nz;
     o->inl_m = (REAL*)calloc(M, sizeof(REAL));
     o->inl_w = (REAL*)calloc(3*M, sizeof(REAL));
@@ -387,6 +413,8 @@ void orc_destroy(orc* o) {
     free(o->f); free(o->F); free(o->g); free(o->G); free(o->rho); free(o->u); free(o->T);
     free(o->dS); free(o->alpha); free(o->rel); free(o->mask); free(o->mask_next);
     free(o->sfrac); free(o->cdarcy); free(o->cforch);
+    free(o->gs); free(o->Gs); free(o->Ts); free(o->dSs); free(o->xh); free(o->xa); free(o->rhos);
+    free(o->emis); free(o->rsurf);
     free(o->inl_m); free(o->inl_w); free(o->inl_prof); free(o);
 }
 
@@ -402,6 +430,22 @@ void orc_set_porous(orc* o, const double* sfrac, const double* darcy, const doub
         o->sfrac[c] = sfrac ? (REAL)sfrac[c] : 0;
         o->cdarcy[c] = darcy ? (REAL)darcy[c] : 0;
         o->cforch[c] = forch ? (REAL)forch[c] : 0;
+    }
+}
+
+/* Heat exchange and radiation inputs of porous cells (two fields): exchangeCoef and
+ * exchangeSurface (set_heat_exchange_coef / _surface, LBM2D/_io.py:133-138), rhos
+ * (add_rho_solid, :128-132), emissivity and radiation_surface (app.py:564-566); planar,
+ * any may be NULL (zero).  Call before orc_init. */
+void orc_set_porous_heat(orc* o, const double* h, const double* a, const double* rhos,
+                         const double* emis, const double* rsurf) {
+    if (!o->gs) return;
+    for (long c = 0; c < o->N; ++c) {
+        o->xh[c] = h ? (REAL)h[c] : 0;
+        o->xa[c] = a ? (REAL)a[c] : 0;
+        o->rhos[c] = rhos ? (REAL)rhos[c] : 0;
+        o->emis[c] = emis ? (REAL)emis[c] : 0;
+        o->rsurf[c] = rsurf ? (REAL)rsurf[c] : 0;
     }
 }
 
@@ -432,6 +476,11 @@ void orc_init(orc* o, const double* rho, const double* u, const double* T,
             o->g[c*o->QT + k] = v;
             o->G[c*o->QT + k] = v;
         }
+        if (porous_ts(o, c)) {      /* TS.g = TS.G = TS.geq(TS.S) = w T (:62-63), TS.S = T here */
+            o->Ts[c] = o->T[c];
+            o->dSs[c] = 0;
+            for (int k = 0; k < o->QT; ++k) o->gs[c*o->QT + k] = o->Gs[c*o->QT + k] = o->wt[k]*o->T[c];
+        }
     }
     /* init_boundary (src/LBM/LBM2D/_initialize.py:67-74): the columns x = 0 and 1 start
      * at the inlet velocity v0 = F/ny/nz and the first controller update reads it.  The
@@ -442,6 +491,21 @@ void orc_init(orc* o, const double* rho, const double* u, const double* T,
         for (long j = 0; j < (long)o->c.ny * o->c.nz; ++j) {
             o->inl_m[j] = o->rho[(long)o->c.nx * j] * v0;
             o->inl_w[3*j] = v0; o->inl_w[3*j+1] = 0; o->inl_w[3*j+2] = 0;
+        }
+    }
+}
+
+/* A solid temperature field of its own (TS.S initialised apart from TF.S, app.py:506-509):
+ * after orc_init, TS of porous cells and of pure-solid cells (two fields) from Ts, planar. */
+void orc_init_solid_T(orc* o, const double* Ts) {
+    if (o->c.thermal != 2) return;
+    for (long c = 0; c < o->N; ++c) {
+        if (porous_ts(o, c)) {
+            o->Ts[c] = (REAL)Ts[c];
+            for (int k = 0; k < o->QT; ++k) o->gs[c*o->QT + k] = o->Gs[c*o->QT + k] = o->wt[k]*o->Ts[c];
+        } else if (is_solid(o->mask, c)) {
+            o->T[c] = (REAL)Ts[c];
+            for (int k = 0; k < o->QT; ++k) o->g[c*o->QT + k] = o->G[c*o->QT + k] = o->wt[k]*o->T[c];
         }
     }
 }
@@ -473,13 +537,31 @@ static void collide_stream(orc* o) {
             for (int k = 0; k < QT; ++k) {
                 REAL gk = o->g[c*QT + k];
                 REAL ge = solid ? o->wt[k]*o->T[c] : geq_fluid(o, k, o->T[c], &o->u[c*3]);
-                REAL src = o->wt[k]*o->dS[c];
+                /* TF.geq(k, TF.dS) in fluid cells (with the velocity), TS.geq = w dS in solid */
+                REAL src = solid ? o->wt[k]*o->dS[c] : geq_fluid(o, k, o->dS[c], &o->u[c*3]);
                 go[k] = gk - (REAL)1/tauT*(gk - ge) + src;
             }
             for (int k = 0; k < QT; ++k) {
                 long ip = nbr(o, c, k, +1);
-                if (o->c.thermal == 2 && k > 0 && is_solid(o->mask, ip) != solid) o->G[c*QT + o->opp[k]] = go[k];
+                if (solid && porous_ts(o, ip)) o->Gs[ip*QT + k] = go[k];   /* TS into a porous cell, :109-110 */
+                else if (o->c.thermal == 2 && k > 0 && is_solid(o->mask, ip) != solid) o->G[c*QT + o->opp[k]] = go[k];
                 else o->G[ip*QT + k] = go[k];
+            }
+            if (porous_ts(o, c)) {
+                /* TS of a porous cell: collide towards w T_s, source w dS_s (:39-41, :56-57);
+                 * streams into cells with solid > 0 (porous ones: Gs, pure-solid ones: G) and
+                 * bounces back at pure-fluid neighbours (:82-89) */
+                REAL gso[7];
+                for (int k = 0; k < QT; ++k) {
+                    REAL gk = o->gs[c*QT + k];
+                    gso[k] = gk - (REAL)1/(REAL)o->c.tauT_solid*(gk - o->wt[k]*o->Ts[c]) + o->wt[k]*o->dSs[c];
+                }
+                for (int k = 0; k < QT; ++k) {
+                    long ip = nbr(o, c, k, +1);
+                    if (is_solid(o->mask, ip)) o->G[ip*QT + k] = gso[k];
+                    else if (porous_ts(o, ip)) o->Gs[ip*QT + k] = gso[k];
+                    else o->Gs[c*QT + o->opp[k]] = gso[k];
+                }
             }
             if (solid && o->c.thermal == 2 && o->c.ref_quirk_frozen_solid_T)
                 for (int k = 0; k < QT; ++k) o->g[c*QT + k] = go[k];   /* TS.g[i][k] = g, :96-100 */
@@ -527,6 +609,27 @@ static void macro(orc* o) {
             for (int k = 0; k < QT; ++k) { Tc += o->G[c*QT + k]; o->g[c*QT + k] = o->G[c*QT + k]; }
             o->T[c] = Tc;
             o->dS[c] = 0;
+        }
+        if (porous_ts(o, c)) {
+            /* macro of a porous cell: T_s = sum TS.G, then the exchange with TF and the surface
+             * radiation as sources of the next collision (src/LBM/LBM2D/_evolution.py:186-202) */
+            REAL Tsc = 0;
+            for (int k = 0; k < QT; ++k) { Tsc += o->Gs[c*QT + k]; o->gs[c*QT + k] = o->Gs[c*QT + k]; }
+            o->Ts[c] = Tsc;
+            o->dSs[c] = 0;
+            REAL vsf = (REAL)o->c.T_scale, vrf = (REAL)o->c.T_ref;
+            REAL vss = (REAL)o->c.Ts_scale, vrs = (REAL)o->c.Ts_ref;
+            REAL cf = (REAL)o->c.cap_fluid, cs = (REAL)o->c.cap_solid, dt = (REAL)o->c.dt_phys;
+            REAL Tsp = Tsc*vss + vrs;
+            REAL dH = o->xh[c]*o->xa[c]*((o->T[c]*vsf + vrf) - Tsp)*dt;
+            o->dSs[c] += dH/cs/o->rhos[c]/vss;
+            o->dS[c] += -dH/cf/o->rho[c]/vsf;
+            if (o->c.radiation) {
+                /* TemperatureSolid.radiation, src/LBM/LBM2D/_thermal.py:213-220 */
+                REAL q = o->emis[c]*(REAL)ORC_SIGMA*o->rsurf[c]/(REAL)o->c.dx_phys
+                         *((REAL)pow((double)(REAL)o->c.T_ambient, 4.0) - (REAL)pow((double)Tsp, 4.0));
+                o->dSs[c] += q*dt/cs/o->rhos[c]/vss;
+            }
         }
         o->rel[c] = 0;
         if (o->c.pyro && is_solid(o->mask, c) && (o->mask[c] & ORC_REACTIVE)) {
@@ -661,6 +764,17 @@ void orc_get(const orc* o, double* rho, double* u, double* T, uint8_t* mask, dou
         if (T) T[c] = o->T[c];
         if (mask) mask[c] = o->mask[c];
         if (alpha) alpha[c] = o->alpha[c];
+    }
+}
+
+/* Solid temperature TS.S of porous cells and, with two fields, of pure-solid cells (0 in
+ * pure-fluid cells), and the TS populations of porous cells (planar; 0 elsewhere). */
+void orc_get_solid_T(const orc* o, double* Ts, double* gs) {
+    long N = o->N;
+    for (long c = 0; c < N; ++c) {
+        int p = porous_ts(o, c);
+        if (Ts) Ts[c] = p ? o->Ts[c] : (o->c.thermal == 2 && is_solid(o->mask, c) ? o->T[c] : 0);
+        if (gs) for (int k = 0; k < o->QT; ++k) gs[k*N + c] = p ? o->gs[c*o->QT + k] : 0;
     }
 }
 

@@ -41,6 +41,8 @@ class orc_cfg(C.Structure):
         ("alpha_flip", C.c_double), ("mrt_s", C.c_double * 19), ("side", orc_side * 6),
         ("visc_model", C.c_int), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
         ("ref_quirk_frozen_solid_T", C.c_int), ("poro_model", C.c_int),
+        ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
+        ("dx_phys", C.c_double), ("radiation", C.c_int), ("T_ambient", C.c_double),
     ]
 
 
@@ -74,6 +76,9 @@ def _load(real: str) -> C.CDLL:
     lib.orc_destroy.argtypes = [C.c_void_p]
     lib.orc_init.argtypes = [C.c_void_p] + [C.c_void_p] * 5
     lib.orc_set_porous.argtypes = [C.c_void_p] * 4
+    lib.orc_set_porous_heat.argtypes = [C.c_void_p] * 6
+    lib.orc_init_solid_T.argtypes = [C.c_void_p] * 2
+    lib.orc_get_solid_T.argtypes = [C.c_void_p] * 3
     lib.orc_step.argtypes = [C.c_void_p, C.c_int]
     lib.orc_get.argtypes = [C.c_void_p] + [C.c_void_p] * 5
     lib.orc_get_dist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -123,6 +128,10 @@ class Oracle:
         c.suth_A, c.suth_Ts = cfg.suth_A, cfg.suth_Ts
         c.ref_quirk_frozen_solid_T = int(ref_quirk_frozen_solid_T)
         c.poro_model = {"none": 0, "ergun": 1, "darcy": 2, "darcy_forchheimer": 3}[getattr(cfg, "porous", "none")]
+        c.Ts_ref = cfg.T_ref if cfg.Ts_ref is None else cfg.Ts_ref
+        c.Ts_scale = cfg.T_scale if cfg.Ts_scale is None else cfg.Ts_scale
+        c.cap_fluid, c.cap_solid, c.dx_phys = cfg.cap_fluid, cfg.cap_solid, cfg.dx_phys
+        c.radiation, c.T_ambient = int(cfg.radiation), cfg.T_ambient
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):
@@ -151,10 +160,18 @@ class Oracle:
         self._porous = tuple(self._flat(a) if a is not None else None for a in (fraction, darcy, forchheimer))
         self.lib.orc_set_porous(self._h, *(_ptr(a) for a in self._porous))
 
+    def set_porous_heat(self, h=None, a=None, rho_solid=None, emissivity=None, radiation_surface=None) -> None:
+        """Two fields with porous cells, before ``init``: the exchange coefficient and surface,
+        the solid density and the radiation inputs per cell, (nx, ny, nz) arrays or None."""
+        self._heat = tuple(self._flat(x) if x is not None else None
+                           for x in (h, a, rho_solid, emissivity, radiation_surface))
+        self.lib.orc_set_porous_heat(self._h, *(_ptr(x) for x in self._heat))
+
     def init(self, solid, reactive=None, rho=1.0, u=(0.0, 0.0, 0.0), T=0.0, alpha=None,
-             round_inputs_to_f32: bool = True) -> None:
+             round_inputs_to_f32: bool = True, Ts=None) -> None:
         """Same inputs as ``Lattice.set_geometry`` + ``Lattice.init``.  Inputs are rounded to
-        float32 first (the CUDA path takes float32 initial fields)."""
+        float32 first (the CUDA path takes float32 initial fields).  ``Ts``: the solid
+        temperature of porous and pure-solid cells when it differs from ``T`` (two fields)."""
         from lbm_porouschem_b200.geometry import mask_bytes
         m = mask_bytes(np.asarray(solid), reactive)
         r = self._flat(rho)
@@ -168,6 +185,11 @@ class Oracle:
             r, uu, t, a = (x.astype(np.float32).astype(np.float64) for x in (r, uu, t, a))
         self._keep = (m, r, uu, t, a)
         self.lib.orc_init(self._h, _ptr(r), _ptr(uu), _ptr(t), _ptr(m), _ptr(a))
+        if Ts is not None:
+            ts = self._flat(Ts)
+            if round_inputs_to_f32:
+                ts = ts.astype(np.float32).astype(np.float64)
+            self.lib.orc_init_solid_T(self._h, _ptr(ts))
 
     def step(self, n: int = 1) -> None:
         self.lib.orc_step(self._h, int(n))
@@ -186,6 +208,10 @@ class Oracle:
                "solid": from_flat((m & 1).astype(bool), sh), "alpha": from_flat(a, sh)}
         if self.cfg.thermal != "none":
             out["T"] = from_flat(T, sh)
+        if self.cfg.thermal == "two_field" and self.cfg.porous != "none":
+            ts = np.empty(n)
+            self.lib.orc_get_solid_T(self._h, _ptr(ts), None)
+            out["Ts"] = from_flat(ts, sh)
         return out
 
     def dist(self) -> tuple:
@@ -194,6 +220,12 @@ class Oracle:
         g = np.empty(self.cfg.QT * self.n)
         self.lib.orc_get_dist(self._h, _ptr(f), _ptr(g))
         return f.reshape(self.cfg.Q, self.n), g.reshape(self.cfg.QT, self.n)
+
+    def dist_solid(self) -> np.ndarray:
+        """TS populations of porous cells, planar [QT, N] (zero elsewhere)."""
+        gs = np.empty(self.cfg.QT * self.n)
+        self.lib.orc_get_solid_T(self._h, None, _ptr(gs))
+        return gs.reshape(self.cfg.QT, self.n)
 
     def diag(self) -> dict:
         out = np.empty(8)

@@ -249,9 +249,63 @@ def case_porous3d_df():
                 porous=dict(model="darcy_forchheimer", zone=zone, eps=0.7, darcy=0.5, forch=0.3))
 
 
+def _border(zone):
+    """Zone cells with a face neighbour outside the zone, weight 1: the surface weights the
+    driver takes from the zone's geometry for radiation (src/LBM/app.py:545-566)."""
+    b = np.zeros(zone.shape, dtype=bool)
+    for ax in range(zone.ndim):
+        if zone.shape[ax] == 1:
+            continue
+        for sh in (1, -1):
+            b |= zone & ~np.roll(zone, sh, axis=ax)
+    return b.astype(np.float64)
+
+
+def case_porous2d_heat():
+    """NEE channel through a porous cylinder (DARCY) with two temperature fields: TF and TS
+    exchange heat in the porous cells (src/LBM/LBM2D/_evolution.py:186-200), whose surface
+    also radiates (SURFACE_UNIFORM, :201-202); TS starts apart from TF and has its own
+    temperature range and capacity."""
+    nx, ny = 24, 12
+    shape = (nx, ny, 1)
+    zone = _porous_zone((nx, ny), (10.3, 5.7), 3.6)[..., None]
+    solid = np.zeros(shape, dtype=bool)
+    T0 = (_smooth_field(shape, 113, 0.2) + 0.3).astype(np.float32).astype(np.float64)
+    Ts0 = (_smooth_field(shape, 117, 0.15) + 0.45).astype(np.float32).astype(np.float64)
+    rho, u, T = _common_inputs(shape, 111, solid, T0=T0)
+    Df, Ds = 1.0 / 30.0, 0.1
+    cfg = LatticeConfig(dim=2, nx=nx, ny=ny, nz=1, collision="bgk", precision="fp64", nu=0.1, porous="darcy",
+                        thermal="two_field", tauT_fluid=3 * Df + .5, tauT_solid=3 * Ds + .5,
+                        T_ref=300.0, T_scale=500.0, Ts_ref=250.0, Ts_scale=600.0, cap_fluid=1200.0,
+                        cap_solid=800.0, dt_phys=1.0, dx_phys=1.0, radiation=True, T_ambient=350.0)
+    return dict(name="ref_porous2d_heat", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T, steps=60,
+                thermal=(Df, Ds), channel=(0.03, 1.0), porous=dict(model="darcy", zone=zone, eps=0.6, darcy=0.5),
+                heat=dict(h=3.0, a=1.0, rhos=2.0, emis=0.8, Ts0=Ts0))
+
+
+def case_porous3d_heat():
+    """3D NEE channel through a porous sphere (SPHERICAL: Ergun from the porosity) with two
+    temperature fields exchanging heat in it (LBM3D/_evolution.py:179-193), no radiation."""
+    nx, ny, nz = 12, 8, 8
+    shape = (nx, ny, nz)
+    zone = _porous_zone(shape, (5.4, 3.7, 3.4), 2.1)
+    solid = np.zeros(shape, dtype=bool)
+    T0 = (_smooth_field(shape, 123, 0.2) + 0.3).astype(np.float32).astype(np.float64)
+    Ts0 = (_smooth_field(shape, 127, 0.1) + 0.6).astype(np.float32).astype(np.float64)
+    rho, u, T = _common_inputs(shape, 121, solid, T0=T0)
+    Df, Ds = 0.025, 0.1
+    cfg = LatticeConfig(dim=3, nx=nx, ny=ny, nz=nz, collision="bgk", precision="fp64", nu=0.1, porous="ergun",
+                        thermal="two_field", tauT_fluid=4 * Df + .5, tauT_solid=4 * Ds + .5,
+                        T_ref=300.0, T_scale=500.0, Ts_ref=280.0, Ts_scale=450.0, cap_fluid=1000.0,
+                        cap_solid=700.0, dt_phys=1.0, dx_phys=1.0)
+    return dict(name="ref_porous3d_heat", cfg=cfg, bc_model="NEE", solid=solid, rho=rho, u=u, T=T, steps=20,
+                thermal=(Df, Ds), channel=(0.03, 1.0), porous=dict(model="ergun", zone=zone, eps=0.55),
+                heat=dict(h=2.0, a=1.5, rhos=1.5, emis=0.0, Ts0=Ts0))
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
          case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32,
-         case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df]
+         case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df, case_porous2d_heat, case_porous3d_heat]
 
 
 # --------------------------------------------------------------------------- driver
@@ -262,7 +316,8 @@ def run_reference(case, Solver2D, Solver3D, flag):
     thermal = case.get("thermal")
     Solver = Solver2D if dim == 2 else Solver3D
     poro = case.get("porous")
-    lb = Solver(nx, ny, nz, 1, 1, case["name"], thermal is not None, False, poro is not None, False)
+    heat = case.get("heat")
+    lb = Solver(nx, ny, nz, 1, 1, case["name"], thermal is not None, False, poro is not None, bool(cfg.radiation))
     lb.source_term_model = flag.SOURCE_TERM.MICRO       # app.py:103-104
     lb.force_term_model = flag.FORCE_TERM.GUO
     lb.set_viscosity(cfg.nu)
@@ -302,7 +357,26 @@ def run_reference(case, Solver2D, Solver3D, flag):
         lb.set_fluid_thermal_diff(Df)
         lb.set_solid_thermal_diff(Ds)
         lb.init_field(lb.TF.S, case["T"].copy())
-        lb.init_field(lb.TS.S, case["T"].copy())
+        lb.init_field(lb.TS.S, (case["T"] if heat is None else heat["Ts0"]).copy())
+    if heat is not None:
+        # app.py:537-566 for a porous zone: rhos, exchange surface and coefficient over it,
+        # radiation surface and emissivity on its border; TS range and capacities
+        lb.set_fluid_Trange([cfg.T_ref, cfg.T_ref + cfg.T_scale])
+        lb.set_solid_Trange([cfg.Ts_ref, cfg.Ts_ref + cfg.Ts_scale])
+        lb.set_fluid_capacity(cfg.cap_fluid)
+        lb.set_solid_capacity(cfg.cap_solid)
+        zs = poro["zone"].astype(np.float64)
+        lb.add_rho_solid(heat["rhos"] * zs)
+        lb.set_heat_exchange_surface(heat["a"] * zs)
+        lb.set_heat_exchange_coef(heat["h"] * zs)
+        case["xh"], case["xa"], case["rhos"] = heat["h"] * zs, heat["a"] * zs, heat["rhos"] * zs
+        case["Ts0"] = heat["Ts0"]
+        if cfg.radiation:
+            lb.set_radiation(flag.RADIATION_MODEL.SURFACE_UNIFORM, cfg.T_ambient)
+            border = _border(poro["zone"])
+            lb.init_field(lb.TS.radiation_surface, border.copy())
+            lb.init_field(lb.TS.emissivity, border * heat["emis"])
+            case["emis"], case["rsurf"] = border * heat["emis"], border
     lb.init_field(lb.rho, case["rho"].copy())
     lb.init_field3(lb.v, case["u"][0].copy(), case["u"][1].copy(), case["u"][2].copy())
     lb.add_solid(case["solid"].astype(np.float64))
@@ -331,6 +405,9 @@ def run_reference(case, Solver2D, Solver3D, flag):
         tf, ts = lb.TF.S.to_numpy(), lb.TS.S.to_numpy()
         out["T"] = np.where(case["solid"], ts, tf)
         out["g"] = np.moveaxis(np.where(case["solid"][..., None], lb.TS.g.to_numpy(), lb.TF.g.to_numpy()), -1, 0)
+        if heat is not None:
+            out["Ts"] = ts
+            out["gs"] = np.moveaxis(lb.TS.g.to_numpy(), -1, 0)
     return out, time.time() - t0
 
 
@@ -349,7 +426,8 @@ def main(argv):
                     ref_quirk_frozen_solid_T=case["cfg"].thermal == "two_field",
                     generator="tests/golden/make_reference_fixtures.py")
         path = HERE / f"{case['name']}.npz"
-        extra = {k: case[k] for k in ("sfrac", "darcy", "forch") if k in case}
+        extra = {k: case[k] for k in ("sfrac", "darcy", "forch", "xh", "xa", "rhos", "emis", "rsurf", "Ts0")
+                 if k in case}
         np.savez_compressed(path, meta=json.dumps(meta), solid=case["solid"], rho0=case["rho"],
                             u0=case["u"], T0=case["T"], **extra, **{k + "_ref": v for k, v in out.items()})
         print(f"{case['name']}: {case['steps']} steps in {dt:.1f} s -> {path.name} "

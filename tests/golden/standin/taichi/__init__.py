@@ -17,7 +17,8 @@ What it emulates, and why running it sequentially gives the reference's answer:
   cell, and each boundary pass reads the inner layer that the pass does not write.
 * ``ti.static(x)`` is ``x`` (compile-time branches and unrolled ranges are plain Python).
 * Fields are NumPy arrays; ``float`` (the default real type) is float64, so the fixtures are
-  the reference's arithmetic in double precision.  Every operation is plain IEEE arithmetic
+  the reference's arithmetic in double precision.  Scalar reads are NumPy scalars, so a
+  division by zero yields inf / nan as in the compiled kernels rather than an exception.  Every operation is plain IEEE arithmetic
   in source order; Taichi's fast-math contractions would differ only in the last bits.
 * ``ti.Vector`` is a small value type.  Reading an element of a vector field returns a
   snapshot that also writes through on item assignment, so both ``u = self.v[i]`` (a value)
@@ -34,6 +35,8 @@ import math as _m
 import numpy as np
 
 from . import math  # noqa: F401  (ti.math.*)
+
+np.seterr(all="ignore")
 
 # ---------------------------------------------------------------- types and runtime
 i8, i16, i32, i64 = "i8", "i16", "i32", "i64"
@@ -85,6 +88,7 @@ class MatrixField:  # used only as an annotation by the reference
 class Vector:
     """Value-semantics small vector (``ti.Vector``)."""
     __slots__ = ("v",)
+    __array_ufunc__ = None   # NumPy scalars defer to the reflected operators below
 
     def __init__(self, v, dt=None):
         self.v = list(v)
@@ -219,7 +223,9 @@ class ScalarField:
         self.a = np.zeros(self.shape, dtype=_np_dtype(dtype))
 
     def __getitem__(self, idx):
-        return self.a[_norm_idx(idx)].item()
+        # a NumPy scalar, so that arithmetic follows IEEE rules as compiled Taichi code does
+        # (a division by zero gives inf / nan instead of raising)
+        return self.a[_norm_idx(idx)]
 
     def __setitem__(self, idx, val):
         self.a[_norm_idx(idx)] = val

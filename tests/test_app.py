@@ -124,7 +124,7 @@ def test_unsupported_options_stop_the_run():
     cfg["chemicalProperties"] = {"type": "cantera", "canteraFile": "mech.yaml"}
     with pytest.raises(NotImplementedError):
         build_case(cfg, _log())
-    # porous zones with the temperature field need the TF/TS exchange through them
+    # porous zones with pyrolysis (the case's chemistry) are not on the CUDA path
     cfg = yaml.safe_load(CASE2D)
     cfg["module"]["porous_media"] = True
     cfg["initialCondition"]["solid"]["s1"] = {"zone": "ALL", "type": "poro", "porosity": 0.5}
@@ -152,6 +152,47 @@ def test_porous_zone_maps_to_the_lattice():
     assert np.allclose(lb.coefDarcy._host[zone], 2.0e6 * lb.dx ** 2)
     assert np.allclose(lb.coefForchheimer._host[zone], 300.0 * lb.dx)
     assert np.all(lb.coefDarcy._host[~zone] == 0)
+
+
+def test_porous_zone_with_heat_and_radiation():
+    """A porous zone with the temperature field: two fields exchanging heat in it (exchange
+    surface and coefficient, solid density) and, with module.radiation and radiationProperties
+    mean_temp, its border radiating with the zone's emissivity (src/LBM/app.py:220-227, 537-566)."""
+    from lbm_porouschem_b200.geometry import surface_weights
+    cfg = yaml.safe_load(CASE2D)
+    cfg["module"]["chemistry"] = False
+    cfg.pop("chemicalProperties")
+    cfg["module"]["porous_media"] = True
+    cfg["module"]["radiation"] = True
+    cfg["radiationProperties"] = {"type": "mean_temp", "Tambient": 310.0}
+    geo = next(iter(cfg["geometry"]))
+    cfg["initialCondition"]["solid"] = {"s1": {"zone": geo, "type": "poro", "porosity": 0.6, "rho": 3.0,
+                                               "exchangeSurface": 2.0, "exchangeCoef": 5.0,
+                                               "emisssivity": 0.8}}
+    lb = build_case(cfg, _log())
+    c = lb._config()
+    assert c.porous == "ergun" and c.thermal == "two_field" and c.porous_heat
+    assert c.radiation and c.T_ambient == 310.0 and c.dt_phys == lb.dt and c.dx_phys == lb.dx
+    zone = lb.solid._host > 0
+    assert zone.any() and np.allclose(lb.solid._host[zone], 0.4)
+    assert np.allclose(lb.TS.exchangeSurface._host[zone], 2.0) and np.allclose(lb.TS.exchangeCoef._host[zone], 5.0)
+    assert np.allclose(lb.rhos._host[zone], 3.0)
+    border = surface_weights(zone * 1.0, 2)
+    assert border.max() > 0 and np.array_equal(lb.TS.radiation_surface._host, border)
+    assert np.allclose(lb.TS.emissivity._host, 0.8 * border)
+
+
+def test_surface_weights_table():
+    """Solid face neighbours -> weight (src/LBM/GEO/STL.py:216-259), cells beyond the grid empty."""
+    from lbm_porouschem_b200.geometry import surface_weights
+    m = np.zeros((5, 5, 1))
+    m[1:4, 1:4] = 1
+    w = surface_weights(m, 2)
+    assert w[2, 2, 0] == 0.0 and w[1, 2, 0] == 1.0 and w[1, 1, 0] == 1.414 and w[0, 0, 0] == 0.0
+    single = np.zeros((3, 3, 3))
+    single[1, 1, 1] = 1
+    assert surface_weights(single, 3)[1, 1, 1] == 6.0
+    assert surface_weights(np.ones((1, 1, 1)), 3)[0, 0, 0] == 6.0
 
 
 @pytest.mark.gpu

@@ -44,13 +44,21 @@ def _rel(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+def _heat_kw(z):
+    """Exchange and radiation inputs of the porous heat fixtures (h and a over the zone)."""
+    if "xh" not in z:
+        return {}
+    return dict(h=z["xh"], a=z["xa"], rho_solid=z["rhos"], emissivity=z["emis"] if "emis" in z else None,
+                radiation_surface=z["rsurf"] if "rsurf" in z else None)
+
+
 def _run(cfg, z, steps):
     from lbm_porouschem_b200.lattice import Lattice
     lat = Lattice(cfg)
     lat.set_geometry(z["solid"])
     if "sfrac" in z:   # porous cells: the fraction below 1 (the impermeable solid is the mask)
-        lat.set_porous(np.where(z["solid"], 0.0, z["sfrac"]), z["darcy"], z["forch"])
-    lat.init(rho=z["rho0"], u=z["u0"], T=z["T0"])
+        lat.set_porous(np.where(z["solid"], 0.0, z["sfrac"]), z["darcy"], z["forch"], **_heat_kw(z))
+    lat.init(rho=z["rho0"], u=z["u0"], T=z["T0"], Ts=z["Ts0"] if "Ts0" in z else None)
     lat.step(steps)
     out = lat.fields()
     lat.close()
@@ -75,6 +83,9 @@ def test_fp64_kernels_match_reference(name, form):
     if cfg.thermal != "none":
         cells = fl if meta["ref_quirk_frozen_solid_T"] else np.ones_like(fl)
         assert _rel(g["T"][cells], z["T_ref"][cells]) < 1e-10
+    if "Ts_ref" in z:   # TS of the porous cells, which exchange heat with TF there
+        pc = z["xh"] > 0
+        assert _rel(g["Ts"][pc], z["Ts_ref"][pc]) < 1e-10
 
 
 @pytest.mark.parametrize("name", CASES)
@@ -85,7 +96,10 @@ def test_fp32_kernels_match_reference(oracle_mod, name):
     o = oracle_mod.Oracle(cfg32, real="f32", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
     if "sfrac" in z:
         o.set_porous(z["sfrac"], z["darcy"], z["forch"])
-    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+    if "xh" in z:
+        o.set_porous_heat(z["xh"], z["xa"], z["rhos"], z["emis"] if "emis" in z else None,
+                          z["rsurf"] if "rsurf" in z else None)
+    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"], Ts=z["Ts0"] if "Ts0" in z else None)
     o.step(meta["steps"])
     r32 = o.fields()
     fl = ~z["solid"]
@@ -95,3 +109,6 @@ def test_fp32_kernels_match_reference(oracle_mod, name):
     assert e_kernel <= 2.0 * e_f32 + 1e-9 * np.sqrt(fl.sum()), (e_kernel, e_f32)
     if cfg.thermal != "none":
         assert _rel(g["T"][fl], z["T_ref"][fl]) < 1e-5
+    if "Ts_ref" in z:
+        pc = z["xh"] > 0
+        assert _rel(g["Ts"][pc], z["Ts_ref"][pc]) < 1e-5

@@ -11,7 +11,10 @@ The bar is 1e-12 relative L2 (the restatement follows the reference's arithmetic
 in practice the fields agree bit for bit); fluid and porous cells are compared for rho, u and
 the flow populations, every cell for temperature.  The porous cases run the reference with
 ``isPoro``: cells of solid fraction between 0 and 1, the eps-equilibrium, the Darcy /
-Darcy-Forchheimer / Ergun drag in the Guo term and the macro velocity correction.
+Darcy-Forchheimer / Ergun drag in the Guo term and the macro velocity correction.  The
+porous heat cases add two temperature fields: a porous cell carries both TF and TS, which
+exchange heat there, and its surface radiates (``_evolution.py:186-202``); TS of the porous
+cells (temperature and populations) is compared too.
 """
 from __future__ import annotations
 
@@ -53,7 +56,10 @@ def test_oracle_matches_reference(oracle_mod, name):
     o = oracle_mod.Oracle(cfg, real="f64", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
     if "sfrac" in z:   # porous cells: solid fraction and drag coefficients
         o.set_porous(z["sfrac"], z["darcy"], z["forch"])
-    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+    if "xh" in z:      # two fields with porous cells: exchange and radiation inputs
+        o.set_porous_heat(z["xh"], z["xa"], z["rhos"], z["emis"] if "emis" in z else None,
+                          z["rsurf"] if "rsurf" in z else None)
+    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"], Ts=z["Ts0"] if "Ts0" in z else None)
     o.step(meta["steps"])
     r = o.fields()
     fl = ~z["solid"]
@@ -66,6 +72,27 @@ def test_oracle_matches_reference(oracle_mod, name):
     if cfg.thermal != "none":
         assert rel(r["T"], z["T_ref"]) <= TOL
         assert rel(g, planar(z["g_ref"], cfg.QT)) <= TOL
+    if "Ts_ref" in z:
+        pc = z["xh"] > 0
+        assert rel(r["Ts"][pc], z["Ts_ref"][pc]) <= TOL
+        gs = o.dist_solid()
+        pf = pc.ravel(order="F")
+        assert rel(gs[:, pf], planar(z["gs_ref"], cfg.QT)[:, pf]) <= TOL
+
+
+def test_porous_heat_exchange_matters(oracle_mod):
+    """The porous heat case moves heat between the fields: without the exchange and radiation
+    inputs the porous cells' temperatures differ from the reference's."""
+    z, meta, cfg = load_case("ref_porous2d_heat")
+    o = oracle_mod.Oracle(cfg, real="f64")
+    o.set_porous(z["sfrac"], z["darcy"], z["forch"])
+    o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"], Ts=z["Ts0"])
+    o.set_porous_heat(None, None, z["rhos"], None, None)
+    o.step(meta["steps"])
+    pc = z["xh"] > 0
+    r = o.fields()
+    assert rel(r["Ts"][pc], z["Ts_ref"][pc]) > 1e-3
+    assert rel(r["T"][pc], z["T_ref"][pc]) > 1e-4
 
 
 def test_frozen_solid_quirk_matters(oracle_mod):

@@ -170,6 +170,7 @@ def test_solver_steps_like_lattice():
     s.add_solid(solid)
     T0 = 300.0 + 100.0 * rng.random((64, 32, 1))
     s.init_field(s.TF.S, (T0 - 300.0) / 500.0)
+    s.init_field(s.TS.S, (T0 - 300.0) / 500.0)   # the driver sets both (src/LBM/app.py:503-509)
     s.init_field(s.rho, 1.0)
     s.init_simulation()
     for _ in range(50):
