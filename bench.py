@@ -48,6 +48,9 @@ def parse(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps for the e2e leg (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
+                    help="replicas: one lattice per GPU (weak scaling); slab: one lattice split along z "
+                         "over the GPUs with a halo exchange every step (strong scaling)")
     ap.add_argument("--bulk", default="", choices=["", "tile", "list", "dense"],
                     help="bulk form of the lattice update (default: the library's choice)")
     return ap.parse_args(argv)
@@ -225,6 +228,8 @@ def main(argv=None):
 
     if args.workload == "sweep2d":
         return sweep_main(args, world, rank, local)
+    if args.decomp == "slab":
+        return slab_main(args, world, rank, local)
 
     import torch
     import torch.distributed as dist
@@ -488,6 +493,54 @@ def sweep_main(args, world, rank, local):
     batch.close()
     for lat in lats:
         lat.close()
+    if world > 1:
+        dist.destroy_process_group()
+    return 0
+
+
+def slab_main(args, world, rank, local):
+    """One lattice split along z over the ranks (lbm_porouschem_b200.slab): each step is the
+    tile-form update of every slab and its halo exchange (NCCL point-to-point between the
+    ranks, device copies on one rank).  value = the lattice's cells x steps / max-over-ranks
+    device time: strong scaling."""
+    import torch
+    import torch.distributed as dist
+    from lbm_porouschem_b200.slab import SlabLattice, lattice_views
+    torch.cuda.set_device(local)
+    if world > 1:
+        dist.init_process_group("nccl", init_method="env://", device_id=torch.device("cuda", local),
+                                timeout=__import__("datetime").timedelta(seconds=300))
+    w = make_workload(args, args.seed)           # one geometry, the same on every rank
+    cfg = w.cfg.replace(bulk_form="tile")
+    sl = SlabLattice(cfg, device=f"cuda:{local}")
+    sl.set_geometry(w.solid, w.reactive)
+    sl.init(**w.init)
+    stream = torch.cuda.current_stream()
+    sl.step(args.warmup)
+    rank_barrier(world)
+    torch.cuda.synchronize()
+    t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    t0.record(stream)
+    sl.step(args.steps)
+    t1.record(stream)
+    torch.cuda.synchronize()
+    rank_barrier(world)
+    ms = max_over_ranks(t0.elapsed_time(t1), world, f"cuda:{local}")
+    views, _ = lattice_views(sl.lat)
+    halo_bytes = sum(v[:, :sl.plan.halo].numel() * v.element_size() for v in views)
+    if rank == 0:
+        line = {
+            "metric": "coupled MLUPS", "value": round(cfg.ncells * args.steps / (ms * 1e-3) / 1e6, 3),
+            "unit": "MLUPS", "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": round(ms / args.steps, 4), "higher_is_better": True, "scaling": "strong",
+            "vs_baseline": None, "dtype": {"fp32": "f32", "fp16": "f16 storage, f32 arithmetic",
+                                           "fp64": "f64"}[args.precision],
+            "data": "synthetic (seeded packing)",
+            "config": {**describe(w, args), "parallelism": f"slab z x{world}, halo {sl.plan.halo}",
+                       "planes_per_rank": sl.plan.counts, "halo_bytes_per_neighbour_per_step": halo_bytes},
+        }
+        print(json.dumps(line), flush=True)
+    sl.close()
     if world > 1:
         dist.destroy_process_group()
     return 0

@@ -765,8 +765,10 @@ __device__ __forceinline__ void diag_flow(const StepParams<S>& p, DiagAcc<typena
                                           typename Store<S>::C uy, typename Store<S>::C uz) {
   using C = typename Store<S>::C;
   a.mass += (double)rho;
-  // in double: exact products of FP32 inputs, so no contraction choice changes it
-  const double u2 = (double)ux * ux + (double)uy * uy + (double)uz * uz;
+  // in double with explicit roundings: no contraction choice of the kernel at hand changes it
+  // (FP64 velocities would otherwise round differently in the tile, list and dense forms)
+  const double u2 = __dadd_rn(__dadd_rn(__dmul_rn((double)ux, (double)ux), __dmul_rn((double)uy, (double)uy)),
+                              __dmul_rn((double)uz, (double)uz));
   a.u2max = fmax(a.u2max, (C)u2);
   if (!finite_(rho)) a.nonfinite += 1;
   a.nfluid += 1;
@@ -1142,9 +1144,11 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
     if (p.ent_c) list_turn_fluid<L>(p, c, nb, K::neighbour_bits(p, nb, np));
   }
   if constexpr (THERMAL) {
+    // the cell is fluid now: its last heat source enters as TF.geq(k, dS) with its velocity
+    // (src/LBM/LBM2D/_evolution.py:54-56)
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
-    K::collide_thermal(p, G, T, p.itauT_f, ux, uy, uz, dS);
+    K::template collide_thermal<true>(p, G, T, p.itauT_f, ux, uy, uz, dS);
     K::store_thermal(p, c, G);
   }
   if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);

@@ -778,6 +778,33 @@ void orc_get_solid_T(const orc* o, double* Ts, double* gs) {
     }
 }
 
+/* The oracle's per-cell state that the next step reads (test infrastructure: slab
+ * decomposition tests exchange planes of it between ranks), cell-major: id 0 f [N][Q],
+ * 1 g [N][QT], 2 rho [N], 3 u [N][3], 4 T [N], 5 dS [N], 6 alpha [N], 7 rel [N],
+ * 8 mask [N] (bytes), 9 gs [N][QT], 10 Ts [N], 11 dSs [N].  *n: elements per cell
+ * (0 when the array does not exist). */
+void* orc_array(orc* o, int id, int* n) {
+    int Q = o->Q, QT = o->QT;
+    void* p = NULL;
+    int m = 0;
+    switch (id) {
+    case 0: p = o->f; m = Q; break;
+    case 1: p = o->g; m = QT; break;
+    case 2: p = o->rho; m = 1; break;
+    case 3: p = o->u; m = 3; break;
+    case 4: p = o->T; m = 1; break;
+    case 5: p = o->dS; m = 1; break;
+    case 6: p = o->alpha; m = 1; break;
+    case 7: p = o->rel; m = 1; break;
+    case 8: p = o->mask; m = 1; break;
+    case 9: p = o->gs; m = o->gs ? QT : 0; break;
+    case 10: p = o->Ts; m = o->Ts ? 1 : 0; break;
+    case 11: p = o->dSs; m = o->dSs ? 1 : 0; break;
+    }
+    *n = p ? m : 0;
+    return p;
+}
+
 /* Post-stream distributions (f after macro/NEE), planar: out[k*N + c]. */
 void orc_get_dist(const orc* o, double* f, double* g) {
     long N = o->N;

@@ -79,6 +79,8 @@ def _load(real: str) -> C.CDLL:
     lib.orc_set_porous_heat.argtypes = [C.c_void_p] * 6
     lib.orc_init_solid_T.argtypes = [C.c_void_p] * 2
     lib.orc_get_solid_T.argtypes = [C.c_void_p] * 3
+    lib.orc_array.argtypes = [C.c_void_p, C.c_int, C.POINTER(C.c_int)]
+    lib.orc_array.restype = C.c_void_p
     lib.orc_step.argtypes = [C.c_void_p, C.c_int]
     lib.orc_get.argtypes = [C.c_void_p] + [C.c_void_p] * 5
     lib.orc_get_dist.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
@@ -220,6 +222,26 @@ class Oracle:
         g = np.empty(self.cfg.QT * self.n)
         self.lib.orc_get_dist(self._h, _ptr(f), _ptr(g))
         return f.reshape(self.cfg.Q, self.n), g.reshape(self.cfg.QT, self.n)
+
+    STATE_IDS = {"f": 0, "g": 1, "rho": 2, "u": 3, "T": 4, "dS": 5, "alpha": 6, "rel": 7, "mask": 8,
+                 "gs": 9, "Ts": 10, "dSs": 11}
+
+    def state_arrays(self) -> dict:
+        """Zero-copy views of the per-cell state the next step reads, each shaped
+        (nz, nx*ny, components) in the device cell order (cells of a z plane contiguous)."""
+        real = np.float64 if self.lib is _LIBS.get("f64") else np.float32
+        P = self.cfg.nx * self.cfg.ny
+        nz = self.n // P
+        out = {}
+        for name, i in self.STATE_IDS.items():
+            m = C.c_int()
+            ptr = self.lib.orc_array(self._h, i, C.byref(m))
+            if not ptr or m.value == 0:
+                continue
+            dt = np.uint8 if name == "mask" else real
+            buf = (C.c_ubyte * (self.n * m.value * np.dtype(dt).itemsize)).from_address(ptr)
+            out[name] = np.frombuffer(buf, dtype=dt).reshape(nz, P, m.value)
+        return out
 
     def dist_solid(self) -> np.ndarray:
         """TS populations of porous cells, planar [QT, N] (zero elsewhere)."""
