@@ -307,10 +307,15 @@ def main(argv=None):
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
     e0.record(stream)
+    pending = None
     for _ in range(k2):
-        lat.set_sides(sides)          # H2D: 6 side records from host memory
+        lat.set_sides(sides)          # H2D: 6 side records from pinned host memory
         lat.step(1, diag=True)
-        pinned_diag = lat.read_diag()  # D2H: diagnostics (synchronises the stream)
+        cur = lat.read_diag_async()   # D2H of this step's diagnostics, enqueued behind it
+        if pending is not None:
+            pinned_diag = pending.result()   # the previous step's values, while this step runs
+        pending = cur
+    pinned_diag = pending.result()
     e1.record(stream)
     e1.synchronize()
     wall = time.perf_counter() - t0

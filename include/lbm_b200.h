@@ -272,6 +272,17 @@ LBM_API int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream);
  * solid-mass integral.  Returns LBM_ERR_NONFINITE if NaN/Inf was seen. */
 LBM_API int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream);
 
+/* The same copy without waiting (replaces the same reference reads, for a driver loop that
+ * keeps the GPU busy while it reads the previous step's values): enqueues on `stream` the
+ * copy of the last LBM_STEP_DIAG step's diagnostics into *pinned_out and of the step
+ * kernels' error flags into *pinned_err (both in page-locked host memory), sets
+ * pinned_out->step, and returns.  Once the stream has passed the copy (an event recorded
+ * after the call), *pinned_err bit 0 set means a bounded wait gave up (LBM_ERR_TIMEOUT),
+ * bit 1 that the fluid list overflowed, and pinned_out->nonfinite > 0 that NaN/Inf was
+ * seen, as lbm_read_diag reports them.  A later step with LBM_STEP_DIAG overwrites the
+ * device values only after the copy (stream order). */
+LBM_API int32_t lbm_read_diag_async(lbm_handle* h, lbm_diag* pinned_out, int32_t* pinned_err, void* stream);
+
 /* Lattice steps taken since lbm_init_equilibrium (tLattice counter,
  * src/LBM/LBM2D/_evolution.py:15). */
 LBM_API int64_t lbm_step_count(const lbm_handle* h);

@@ -44,7 +44,7 @@ LBM_STEP_RESIDUAL = 4
 EXPORTED = (
     "lbm_abi_version", "lbm_last_error", "lbm_required_bytes", "lbm_create", "lbm_destroy",
     "lbm_bind", "lbm_set_sides", "lbm_init_equilibrium", "lbm_resume", "lbm_step", "lbm_compute_macro",
-    "lbm_read_diag",
+    "lbm_read_diag", "lbm_read_diag_async",
     "lbm_step_count", "lbm_bulk_form", "lbm_set_wait_limit", "lbm_advance", "lbm_diag_noalloc", "lbm_stl_work_bytes", "lbm_voxelise_stl",
     "lbm_batch_required_bytes", "lbm_batch_create", "lbm_batch_step", "lbm_batch_advance", "lbm_batch_destroy",
     "lbm_batch_set_blocks",
@@ -142,6 +142,8 @@ def load(path: str | os.PathLike | None = None) -> C.CDLL:
     lib.lbm_compute_macro.restype = i32
     lib.lbm_read_diag.argtypes = [vp, C.POINTER(lbm_diag), vp]
     lib.lbm_read_diag.restype = i32
+    lib.lbm_read_diag_async.argtypes = [vp, vp, vp, vp]
+    lib.lbm_read_diag_async.restype = i32
     lib.lbm_step_count.argtypes = [vp]
     lib.lbm_step_count.restype = i64
     lib.lbm_bulk_form.argtypes = [vp]

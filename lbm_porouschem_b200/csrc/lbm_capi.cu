@@ -4,6 +4,7 @@
 // sm_100a kernels of step_kernels.cuh on the caller's stream.  No allocation
 // happens here: every buffer (including the reduction scratch) is bound by the
 // caller, sized by lbm_required_bytes().
+#include <cstddef>
 #include "capi_internal.cuh"
 
 using namespace lbm;
@@ -530,6 +531,17 @@ int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
   out->res_num = v[8]; out->res_den = v[9];
   out->step = h->step;
   if (v[6] > 0) return fail(LBM_ERR_NONFINITE, "diagnostics saw NaN/Inf");
+  return LBM_OK;
+}
+
+int32_t lbm_read_diag_async(lbm_handle* h, lbm_diag* out, int32_t* err, void* stream) {
+  if (!h || !out || !err) return fail(LBM_ERR_ARG, "NULL argument");
+  if (!h->diag_valid) return fail(LBM_ERR_ARG, "no diagnostics: call lbm_step with LBM_STEP_DIAG");
+  static_assert(sizeof(double) * kNumDiag == offsetof(lbm_diag, step), "lbm_diag leads with the partial slots");
+  cudaStream_t st = (cudaStream_t)stream;
+  out->step = h->step;
+  LBM_CUDA_TRY(cudaMemcpyAsync(out, scratch_final(h), sizeof(double) * kNumDiag, cudaMemcpyDeviceToHost, st));
+  LBM_CUDA_TRY(cudaMemcpyAsync(err, scratch_err(h), sizeof(int32_t), cudaMemcpyDeviceToHost, st));
   return LBM_OK;
 }
 

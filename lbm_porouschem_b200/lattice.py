@@ -255,6 +255,24 @@ class Lattice:
         N.check(rc)
         return out
 
+    def read_diag_async(self) -> "PendingDiag":
+        """The last LBM_STEP_DIAG step's diagnostics, copied to page-locked host memory
+        without waiting (lbm_read_diag_async): ``result()`` waits for that copy only, so a
+        driver loop can launch the next step first.  Two reads may be outstanding at a time
+        (the staging buffers alternate)."""
+        if getattr(self, "_diag_pinned", None) is None:
+            nb = ctypes.sizeof(N.lbm_diag) + 8
+            self._diag_pinned = [torch.zeros(nb, dtype=torch.uint8, pin_memory=True) for _ in range(2)]
+            self._diag_slot = 0
+        buf = self._diag_pinned[self._diag_slot]
+        self._diag_slot ^= 1
+        base = buf.data_ptr()
+        err = base + ctypes.sizeof(N.lbm_diag)
+        N.check(self.lib.lbm_read_diag_async(self._h, ctypes.c_void_p(base), ctypes.c_void_p(err), self._s()))
+        ev = torch.cuda.Event()
+        ev.record(self.stream if self.stream is not None else torch.cuda.current_stream())
+        return PendingDiag(buf, ev)
+
     def diagnostics(self) -> dict:
         """Diagnostics of the current state (recomputed if needed)."""
         if self.nsteps == 0:
@@ -398,6 +416,26 @@ class Lattice:
             self.close()
         except Exception:
             pass
+
+
+class PendingDiag:
+    """Diagnostics on their way to the host (``Lattice.read_diag_async``)."""
+
+    def __init__(self, buf: torch.Tensor, event: torch.cuda.Event):
+        self._buf, self._event = buf, event
+
+    def result(self) -> dict:
+        """Wait for the copy and return the values as ``Lattice.read_diag`` does (an error
+        flag raised by the step kernels raises ``LBMNativeError``)."""
+        self._event.synchronize()
+        base = self._buf.data_ptr()
+        d = N.lbm_diag.from_address(base)
+        err = ctypes.c_int32.from_address(base + ctypes.sizeof(N.lbm_diag)).value
+        if err & 1:
+            raise N.LBMNativeError(N.LBM_ERR_TIMEOUT, "a bounded wait in the step kernel timed out; the state is invalid")
+        if err & 2:
+            raise N.LBMNativeError(N.LBM_ERR_CUDA, "the fluid cell list overflowed; the state is invalid")
+        return {k: getattr(d, k) for k, _ in N.lbm_diag._fields_}
 
 
 class LatticeBatch:

@@ -139,6 +139,9 @@ def test_dense_wait_timeout_is_reported_and_device_stays_usable():
     with pytest.raises(N.LBMNativeError) as e:
         lat.read_diag()
     assert e.value.code == N.LBM_ERR_TIMEOUT
+    with pytest.raises(N.LBMNativeError) as e:      # the asynchronous read reports it too
+        lat.read_diag_async().result()
+    assert e.value.code == N.LBM_ERR_TIMEOUT
     lat.close()
     b = Lattice(w.cfg.replace(bulk_form="dense"))
     b.set_geometry(w.solid, w.reactive)

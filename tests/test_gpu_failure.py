@@ -40,3 +40,29 @@ def test_nan_in_initial_fields_is_reported(form):
     ok.step(2, diag=True)
     assert ok.read_diag()["nonfinite"] == 0
     ok.close()
+
+
+def test_async_diag_equals_sync_and_reports_nonfinite():
+    """lbm_read_diag_async: the values equal lbm_read_diag's for the same step, two reads may be
+    in flight while later steps run, and a NaN shows as nonfinite > 0."""
+    from lbm_porouschem_b200.lattice import Lattice
+    w = workloads.pyro3d(64, seed=3, ny=16, nz=12)
+    lat = Lattice(w.cfg.replace(bulk_form="list"))
+    lat.set_geometry(w.solid, w.reactive)
+    lat.init(**w.init)
+    lat.step(3, diag=True)
+    a = lat.read_diag_async()
+    lat.step(1, diag=True)
+    b = lat.read_diag_async()
+    ra, rb = a.result(), b.result()
+    assert rb == lat.read_diag() and ra["step"] == 3 and rb["step"] == 4
+    assert ra["mass"] != rb["mass"]
+    lat.close()
+    rho = np.ones(w.cfg.shape)
+    rho[tuple(np.argwhere(~w.solid)[0])] = np.nan
+    bad = Lattice(w.cfg.replace(bulk_form="list"))
+    bad.set_geometry(w.solid, w.reactive)
+    bad.init(rho=rho, u=(0.0, 0.0, 0.0), T=0.0)
+    bad.step(2, diag=True)
+    assert bad.read_diag_async().result()["nonfinite"] >= 1
+    bad.close()
