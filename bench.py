@@ -48,6 +48,8 @@ def parse(argv=None):
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps for the e2e leg (default: --steps)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--seed", type=int, default=0)
+    ap.add_argument("--fp16-rounding", default="stochastic", choices=["stochastic", "nearest"],
+                    help="FP16 storage: rounding of the temperature populations")
     ap.add_argument("--decomp", default="replicas", choices=["replicas", "slab"],
                     help="replicas: one lattice per GPU (weak scaling); slab: one lattice split along z "
                          "over the GPUs with a halo exchange every step (strong scaling)")
@@ -105,6 +107,7 @@ def make_workload(args, seed):
         w = workloads.flow2d(nx, nx // 2, seed=seed, precision=args.precision, collision=args.collision or "bgk")
     if args.bulk:
         w.cfg.bulk_form = args.bulk
+    w.cfg.fp16_rounding = args.fp16_rounding
     return w
 
 
@@ -118,6 +121,7 @@ def describe(w, args):
                     + f" {c.precision}",
         "cells": c.ncells, "porosity": round(w.porosity, 4),
         "l2": "state larger than L2 (no flush needed)" if c.ncells * c.Q * 8 > 126e6 else "state fits in L2",
+        **({"fp16_rounding": f"temperature populations {c.fp16_rounding}"} if c.precision == "fp16" else {}),
     }
 
 

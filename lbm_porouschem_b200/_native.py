@@ -24,6 +24,7 @@ LBM_ERR_TIMEOUT = 6
 
 LBM_COLL_BGK, LBM_COLL_MRT = 0, 1
 LBM_PREC_FP32, LBM_PREC_FP16, LBM_PREC_FP64 = 0, 1, 2
+LBM_FP16_STOCHASTIC, LBM_FP16_NEAREST = 0, 1
 LBM_EOS_IDEAL_GAS, LBM_EOS_INCOMPRESSIBLE = 0, 1
 LBM_THERMAL_NONE, LBM_THERMAL_CONJUGATE, LBM_THERMAL_TWOFIELD = 0, 1, 2
 LBM_BC_PERIODIC, LBM_BC_ZEROGRADIENT, LBM_BC_FIXEDVALUE, LBM_BC_FLOWRATE = 0, 1, 2, 3
@@ -78,7 +79,7 @@ class lbm_desc(C.Structure):
         ("rho0", C.c_double), ("T0", C.c_double), ("side", lbm_side_desc * 6),
         ("viscosity", C.c_int32), ("porous", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
         ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
-        ("dx_phys", C.c_double), ("T_ambient", C.c_double), ("radiation", C.c_int32), ("reserved1", C.c_int32),
+        ("dx_phys", C.c_double), ("T_ambient", C.c_double), ("radiation", C.c_int32), ("fp16_rounding", C.c_int32),
     ]
 
 

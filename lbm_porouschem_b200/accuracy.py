@@ -122,7 +122,9 @@ def config3_case(n: int = 256, steps: int = 20000, seed: int = 0, T0: float | No
         w.cfg.T0 = T0
     out, rates = {}, {}
     for prec in ("fp64",) + tuple(precisions):
-        lat = Lattice(w.cfg.replace(precision=prec))
+        # "fp16-nearest": FP16 storage with the temperature populations rounded to nearest
+        kw = dict(precision="fp16", fp16_rounding="nearest") if prec == "fp16-nearest" else dict(precision=prec)
+        lat = Lattice(w.cfg.replace(**kw))
         lat.set_geometry(w.solid, w.reactive)
         lat.init(**w.init)
         lat.step(10)

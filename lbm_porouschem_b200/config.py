@@ -115,6 +115,7 @@ class LatticeConfig:
     dx_phys: float = 1.0            # cell size (m): radiation per volume, a / dx
     radiation: bool = False         # surface radiation of porous cells (RADIATION_MODEL.SURFACE_UNIFORM)
     T_ambient: float = 300.0        # K
+    fp16_rounding: str = "stochastic"  # FP16 storage of the temperature populations: "stochastic" | "nearest"
 
     @property
     def shape(self) -> tuple:
@@ -195,6 +196,7 @@ class LatticeConfig:
         d.Ts_scale = self.T_scale if self.Ts_scale is None else self.Ts_scale
         d.cap_fluid, d.cap_solid, d.dx_phys = self.cap_fluid, self.cap_solid, self.dx_phys
         d.T_ambient, d.radiation = self.T_ambient, int(self.radiation)
+        d.fp16_rounding = {"stochastic": N.LBM_FP16_STOCHASTIC, "nearest": N.LBM_FP16_NEAREST}[self.fp16_rounding]
         return d
 
     @property

@@ -307,6 +307,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.sig_dx = d.dx_phys > 0 ? (C)(5.670374419e-8 / d.dx_phys) : (C)0;  // Stefan-Boltzmann, util/constant.py:20
   p.Tamb4 = (C)(d.T_ambient * d.T_ambient * d.T_ambient * d.T_ambient);
   p.radiation = d.radiation;
+  p.fp16_nearest = d.fp16_rounding == LBM_FP16_NEAREST;
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

@@ -63,6 +63,8 @@ static int validate(const lbm_desc* d) {
         (!d->radiation || d->dx_phys > 0)))
     return fail(LBM_ERR_ARG, "the heat exchange of porous cells needs cap_fluid, cap_solid, dt_phys > 0, non-zero "
                              "T_scale and Ts_scale, and dx_phys > 0 with radiation");
+  if (d->fp16_rounding != LBM_FP16_STOCHASTIC && d->fp16_rounding != LBM_FP16_NEAREST)
+    return fail(LBM_ERR_ARG, "fp16_rounding must be LBM_FP16_STOCHASTIC or LBM_FP16_NEAREST");
   if (d->radiation && !(d->porous && d->thermal == LBM_THERMAL_TWOFIELD))
     return fail(LBM_ERR_ARG, "radiation is a source of porous cells in the two-field temperature model");
   for (int s = 0; s < 6; ++s) {

@@ -43,18 +43,49 @@ template <> struct Store<float> {
   using C = float;
   __device__ __forceinline__ static C ld(const float* p, size_t i, C) { return p[i]; }
   __device__ __forceinline__ static void st(float* p, size_t i, C v, C) { p[i] = v; }
+  __device__ __forceinline__ static void st_sr(float* p, size_t i, C v, C, uint32_t) { p[i] = v; }
 };
 template <> struct Store<double> {
   using C = double;
   __device__ __forceinline__ static C ld(const double* p, size_t i, C) { return p[i]; }
   __device__ __forceinline__ static void st(double* p, size_t i, C v, C) { p[i] = v; }
+  __device__ __forceinline__ static void st_sr(double* p, size_t i, C v, C, uint32_t) { p[i] = v; }
 };
+
+// 32-bit integer hash ("lowbias32", C. Wellons, 2018: xor-shift / multiply rounds).
+__device__ __forceinline__ uint32_t hash32(uint32_t x) {
+  x ^= x >> 16; x *= 0x7feb352du;
+  x ^= x >> 15; x *= 0x846ca68bu;
+  x ^= x >> 16;
+  return x;
+}
+
+// Stochastic rounding of v to half precision: the neighbour toward zero, h0, or the next
+// one away from zero, h1, the latter with probability |v - h0| / |h1 - h0|, so the stored
+// value equals v on average.  A change of a slowly varying field smaller than half a unit
+// in the last place then survives on average instead of being rounded away at every step
+// (round to nearest stalls slow diffusion).  The threshold is a hash of v's own bits and
+// a salt per direction: a function of the stored state alone, so every bulk form, a batch,
+// a slab decomposition and a resumed run store the same bits.
+__device__ __forceinline__ __half half_sr(float v, uint32_t salt) {
+  const __half h0 = __float2half_rz(v);
+  const float v0 = __half2float(h0);
+  if (v0 == v) return h0;
+  const __half h1 = __ushort_as_half((unsigned short)(__half_as_ushort(h0) + 1u));
+  const float v1 = __half2float(h1);
+  const float u = (float)(hash32(__float_as_uint(v) + salt) >> 8) * (1.0f / 16777216.0f);
+  return fabsf(v - v0) > u * fabsf(v1 - v0) ? h1 : h0;
+}
 // FP16 storage of the deviation from the rest equilibrium (value - shift),
 // FP32 arithmetic.
 template <> struct Store<__half> {
   using C = float;
   __device__ __forceinline__ static C ld(const __half* p, size_t i, C shift) {
     return __half2float(p[i]) + shift;
+  }
+  // stochastically rounded store (the temperature populations); salt: per direction
+  __device__ __forceinline__ static void st_sr(__half* p, size_t i, C v, C shift, uint32_t salt) {
+    p[i] = half_sr(v - shift, salt);
   }
   __device__ __forceinline__ static void st(__half* p, size_t i, C v, C shift) {
     p[i] = __float2half_rn(v - shift);
@@ -134,6 +165,7 @@ struct StepParams {
   const C* xheat;
   C Trs, Tss, cap_f, cap_s, sig_dx, Tamb4;
   int radiation;
+  int fp16_nearest;  // FP16 storage: temperature populations rounded to nearest (else stochastically)
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -644,7 +676,8 @@ struct Kern {
   __device__ __forceinline__ static void store_ts(const P& p, int c, const C GS[QT]) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      Store<S>::st(p.gsB, (size_t)k * p.N + c, GS[k], gshift<L, S, k>(p));
+      if (p.fp16_nearest) Store<S>::st(p.gsB, (size_t)k * p.N + c, GS[k], gshift<L, S, k>(p));
+      else Store<S>::st_sr(p.gsB, (size_t)k * p.N + c, GS[k], gshift<L, S, k>(p), 0x9e3779b9u * (k + 1));
     });
   }
   // Post-collision temperature populations of cell c, in its own slots (the adiabatic
@@ -652,7 +685,8 @@ struct Kern {
   __device__ __forceinline__ static void store_thermal(const P& p, int c, const C G[QT]) {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
-      Store<S>::st(p.gB, (size_t)k * p.N + c, G[k], gshift<L, S, k>(p));
+      if (p.fp16_nearest) Store<S>::st(p.gB, (size_t)k * p.N + c, G[k], gshift<L, S, k>(p));
+      else Store<S>::st_sr(p.gB, (size_t)k * p.N + c, G[k], gshift<L, S, k>(p), 0x9e3779b9u * (k + 1));
     });
   }
 
