@@ -221,7 +221,10 @@ LBM_API const char* lbm_last_error(void);
 LBM_API int32_t lbm_required_bytes(const lbm_desc* desc, int32_t field, size_t* bytes);
 
 /* Validate `desc` and create a handle.  Replaces LBM2D_BASE.__init__
- * (src/LBM/LBM2D/_core.py:11-101) minus the field allocation. */
+ * (src/LBM/LBM2D/_core.py:11-101) minus the field allocation.  The handle belongs to the
+ * CUDA device current here: every later call on it makes that device current for its
+ * duration and restores the caller's afterwards (bind buffers of that device; the members
+ * of a batch share one device). */
 LBM_API int32_t lbm_create(const lbm_desc* desc, lbm_handle** out);
 LBM_API int32_t lbm_destroy(lbm_handle* h);
 

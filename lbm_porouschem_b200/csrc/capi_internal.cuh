@@ -185,6 +185,23 @@ struct lbm_handle {
   lbm::DenseMaps maps{};
   const void* maps_for[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
   uint32_t wait_spins = lbm::kDefaultWaitSpins;
+  int device = 0;  // the CUDA device current at lbm_create: every call runs its work there
+};
+
+// Makes the handle's device current for the scope of an entry point and restores the
+// caller's device afterwards (a call made with another device current still works on
+// the device whose memory the handle's buffers are).
+struct DeviceScope {
+  int prev = -1;
+  explicit DeviceScope(int dev) {  // dev < 0: leave the current device alone
+    if (dev < 0) return;
+    if (cudaGetDevice(&prev) != cudaSuccess) { prev = -1; cudaGetLastError(); return; }
+    if (prev != dev && cudaSetDevice(dev) != cudaSuccess) cudaGetLastError();
+    if (prev == dev) prev = -1;
+  }
+  ~DeviceScope() {
+    if (prev >= 0) cudaSetDevice(prev);
+  }
 };
 
 // A batch of lattices stepped together (batch_kernel.cuh).  Its device tables

@@ -222,6 +222,10 @@ int32_t lbm_create(const lbm_desc* d, lbm_handle** out) {
   if (rc) return rc;
   if (!out) return fail(LBM_ERR_ARG, "out is NULL");
   lbm_handle* h = new lbm_handle();
+  if (cudaGetDevice(&h->device) != cudaSuccess) {
+    cudaGetLastError();
+    h->device = 0;
+  }
   h->d = *d;
   h->N = (size_t)d->nx * d->ny * d->nz;
   for (int i = 0; i < LBM_NUM_FIELDS; ++i) { h->ptr[i] = nullptr; h->bytes[i] = 0; }
@@ -234,6 +238,7 @@ int32_t lbm_create(const lbm_desc* d, lbm_handle** out) {
 }
 
 int32_t lbm_destroy(lbm_handle* h) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (h) {
     if (h->ev_fork) cudaEventDestroy(h->ev_fork);
     if (h->ev_join) cudaEventDestroy(h->ev_join);
@@ -329,6 +334,7 @@ int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector
     if (h->d.dim != d0.dim || h->d.precision != d0.precision || h->d.collision != d0.collision ||
         h->d.thermal != d0.thermal || h->d.pyro != d0.pyro || h->d.viscosity != d0.viscosity)
       return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, viscosity, thermal and pyro");
+    if (h->device != hs[0]->device) return fail(LBM_ERR_ARG, "batch members must live on one device");
     if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
     if (has_flowrate(h->d)) return fail(LBM_ERR_ARG, "batch members cannot have a flow-rate inlet");
     if (porous_heat(h->d))
@@ -392,6 +398,7 @@ size_t batch_bytes(lbm_handle* const* hs, int32_t n, size_t nchunks, size_t nbc)
 extern "C" {
 
 int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h || !host_sides) return fail(LBM_ERR_ARG, "NULL argument");
   if (!h->ptr[LBM_FIELD_SCRATCH]) return fail(LBM_ERR_UNBOUND, "scratch is not bound");
   for (int s = 0; s < 6; ++s) {
@@ -408,6 +415,7 @@ int32_t lbm_set_sides(lbm_handle* h, const lbm_side_desc* host_sides, void* stre
 
 int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, const float* T,
                              const float* alpha, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
   int rc = check_bound(h);
   if (rc) return rc;
@@ -439,6 +447,7 @@ int32_t lbm_init_equilibrium(lbm_handle* h, const float* rho, const float* u, co
 }
 
 int32_t lbm_resume(lbm_handle* h, int64_t step, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
   if (step < 0) return fail(LBM_ERR_ARG, "step must be >= 0");
   int rc = check_bound(h);
@@ -458,6 +467,7 @@ int32_t lbm_resume(lbm_handle* h, int64_t step, void* stream) {
 }
 
 int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
   if (n < 0) return fail(LBM_ERR_ARG, "n must be >= 0");
   int rc = check_bound(h);
@@ -490,6 +500,7 @@ int32_t lbm_step(lbm_handle* h, int32_t n, int32_t flags, void* stream) {
 }
 
 int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h) return fail(LBM_ERR_ARG, "handle is NULL");
   if (h->step < 1) return fail(LBM_ERR_ARG, "no step taken yet: the initial fields are the state");
   if (flags & ~(LBM_STEP_DIAG | LBM_STEP_MACRO | LBM_STEP_RESIDUAL)) return fail(LBM_ERR_ARG, "bad flags");
@@ -518,6 +529,7 @@ int32_t lbm_compute_macro(lbm_handle* h, int32_t flags, void* stream) {
 }
 
 int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h || !out) return fail(LBM_ERR_ARG, "NULL argument");
   if (!h->diag_valid) return fail(LBM_ERR_ARG, "no diagnostics: call lbm_step with LBM_STEP_DIAG");
   double v[kNumDiag];
@@ -537,6 +549,7 @@ int32_t lbm_read_diag(lbm_handle* h, lbm_diag* out, void* stream) {
 }
 
 int32_t lbm_read_diag_async(lbm_handle* h, lbm_diag* out, int32_t* err, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h || !out || !err) return fail(LBM_ERR_ARG, "NULL argument");
   if (!h->diag_valid) return fail(LBM_ERR_ARG, "no diagnostics: call lbm_step with LBM_STEP_DIAG");
   static_assert(sizeof(double) * kNumDiag == offsetof(lbm_diag, step), "lbm_diag leads with the partial slots");
@@ -548,6 +561,7 @@ int32_t lbm_read_diag_async(lbm_handle* h, lbm_diag* out, int32_t* err, void* st
 }
 
 int32_t lbm_batch_required_bytes(lbm_handle* const* hs, int32_t n, void* stream, size_t* bytes) {
+  DeviceScope dev_scope(hs && n > 0 && hs[0] ? hs[0]->device : -1);
   if (!bytes) return fail(LBM_ERR_ARG, "bytes is NULL");
   std::vector<std::vector<int>> hdr;
   int rc = batch_members(hs, n, (cudaStream_t)stream, hdr);
@@ -561,6 +575,7 @@ int32_t lbm_batch_required_bytes(lbm_handle* const* hs, int32_t n, void* stream,
 
 int32_t lbm_batch_create(lbm_handle* const* hs, int32_t n, void* dev_scratch, size_t bytes, void* stream,
                          lbm_batch** out) {
+  DeviceScope dev_scope(hs && n > 0 && hs[0] ? hs[0]->device : -1);
   if (!out) return fail(LBM_ERR_ARG, "out is NULL");
   if (!dev_scratch) return fail(LBM_ERR_ARG, "the batch needs a device buffer");
   cudaStream_t st = (cudaStream_t)stream;
@@ -615,6 +630,7 @@ int32_t lbm_batch_create(lbm_handle* const* hs, int32_t n, void* dev_scratch, si
 }
 
 int32_t lbm_batch_step(lbm_batch* b, int32_t n, void* stream) {
+  DeviceScope dev_scope(b && !b->hs.empty() ? b->hs[0]->device : -1);
   if (!b) return fail(LBM_ERR_ARG, "batch is NULL");
   if (n < 0) return fail(LBM_ERR_ARG, "n must be >= 0");
   cudaStream_t st = (cudaStream_t)stream;
@@ -656,6 +672,7 @@ int32_t lbm_batch_advance(lbm_batch* b, int32_t n) {
 }
 
 int32_t lbm_batch_destroy(lbm_batch* b) {
+  DeviceScope dev_scope(b && !b->hs.empty() ? b->hs[0]->device : -1);
   delete b;
   return LBM_OK;
 }

@@ -79,6 +79,7 @@ int with_types_na(lbm_handle* h, Fn&& fn) {
 }  // namespace
 
 extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) {
+  DeviceScope dev_scope(h ? h->device : -1);
   if (!h || !out) return fail(LBM_ERR_ARG, "NULL argument");
   if (h->step < 1) return fail(LBM_ERR_ARG, "no step taken yet: the initial fields are the state");
   const int rows = partial_rows(h->L);
