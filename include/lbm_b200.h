@@ -118,6 +118,12 @@ extern "C" {
  * alone, its temperature is extrapolated as under NEE); 0 leaves it periodic. */
 #define LBM_SIDE_NEE 1
 #define LBM_SIDE_ES 2
+/* 3: non-equilibrium bounce-back (Zou & He; BC_MODEL.NEBB, src/LBM/LBM2D/_boundary.py:103-226):
+ * 2D without the temperature field, every active side NEBB.  A side cell keeps its own
+ * post-stream populations and the ones entering from outside are rebuilt so that it takes
+ * the side's velocity (v_type fixed) or density (rho_type fixed); an x side treats rows
+ * 1 .. ny-2, a y side every column, as the reference's two loops do. */
+#define LBM_SIDE_NEBB 3
 typedef struct lbm_side_desc {
   int32_t active;
   int32_t v_type;   /* LBM_BC_*, velocity  (set_BC mapping src/LBM/LBM2D/_io.py:385-402) */

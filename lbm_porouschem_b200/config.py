@@ -27,8 +27,9 @@ GAS_CONSTANT = 8.314441  # src/LBM/util/constant.py:17
 @dataclass
 class SideBC:
     """One domain side.  ``active`` False keeps the side periodic; ``model`` is the
-    boundary scheme of an active side: "nee" (non-equilibrium extrapolation) or "es"
-    (equilibrium populations of the side's state), the reference's BC_MODEL."""
+    boundary scheme of an active side: "nee" (non-equilibrium extrapolation), "es"
+    (equilibrium populations of the side's state) or "nebb" (Zou-He non-equilibrium
+    bounce-back, 2D), the reference's BC_MODEL."""
     active: bool = False
     v_type: int = PERIODIC
     rho_type: int = PERIODIC
@@ -39,12 +40,13 @@ class SideBC:
     model: str = "nee"
 
     def code(self) -> int:
-        """lbm_side_desc.active: 0 periodic, 1 NEE, 2 ES."""
+        """lbm_side_desc.active: 0 periodic, 1 NEE, 2 ES, 3 NEBB."""
         if not self.active:
             return 0
-        if self.model not in ("nee", "es"):
-            raise ValueError(f"side model {self.model!r}: 'nee' or 'es'")
-        return 2 if self.model == "es" else 1
+        codes = {"nee": 1, "es": 2, "nebb": 3}
+        if self.model not in codes:
+            raise ValueError(f"side model {self.model!r}: 'nee', 'es' or 'nebb'")
+        return codes[self.model]
 
     @staticmethod
     def inlet(v, T_type=PERIODIC, T=0.0) -> "SideBC":

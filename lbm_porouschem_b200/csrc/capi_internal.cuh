@@ -122,7 +122,9 @@ inline Launch plan(const lbm_desc& d, int tx) {
   const bool force_list = d.bulk_form == 2 || (d.bulk_form == 0 && b && std::strcmp(b, "list") == 0);
   const bool force_dense = d.bulk_form == 3 || (d.bulk_form == 0 && b && std::strcmp(b, "dense") == 0);
   L.list = !force_tile && !force_dense && (force_list || L.N >= 65536);
-  const bool xface = (d.side[0].active || d.side[1].active) && d.nx >= 4;
+  // x-face records for NEE / ES x sides (a NEBB side reads only its own cell)
+  const bool xface = (d.side[0].active || d.side[1].active) && d.nx >= 4 &&
+                     d.side[0].active != LBM_SIDE_NEBB && d.side[1].active != LBM_SIDE_NEBB;
   L.face_cells = xface ? (size_t)d.ny * d.nz : 0;
   L.face_vals = lat_q(d.dim) + (d.thermal ? lat_qt(d.dim) : 0);
   L.face_elem = compute_bytes(d.precision);
@@ -325,6 +327,8 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.Tamb4 = (C)(d.T_ambient * d.T_ambient * d.T_ambient * d.T_ambient);
   p.radiation = d.radiation;
   p.fp16_nearest = d.fp16_rounding == LBM_FP16_NEAREST;
+  p.nebb = 0;
+  for (int s = 0; s < 6; ++s) p.nebb |= d.side[s].active == LBM_SIDE_NEBB;
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

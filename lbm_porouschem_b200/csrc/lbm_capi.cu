@@ -67,9 +67,20 @@ static int validate(const lbm_desc* d) {
     return fail(LBM_ERR_ARG, "fp16_rounding must be LBM_FP16_STOCHASTIC or LBM_FP16_NEAREST");
   if (d->radiation && !(d->porous && d->thermal == LBM_THERMAL_TWOFIELD))
     return fail(LBM_ERR_ARG, "radiation is a source of porous cells in the two-field temperature model");
+  int nebb = 0, other = 0;
+  for (int s = 0; s < 6; ++s) {
+    if (d->side[s].active == LBM_SIDE_NEBB) ++nebb;
+    else if (d->side[s].active) ++other;
+  }
+  if (nebb && (other || d->dim != 2 || d->thermal != LBM_THERMAL_NONE))
+    return fail(LBM_ERR_ARG, "NEBB sides: 2D, without the temperature field, every active side NEBB "
+                             "(the reference's NEBB exists in 2D only, with one model for all sides)");
   for (int s = 0; s < 6; ++s) {
     const lbm_side_desc& sd = d->side[s];
-    if (sd.active < 0 || sd.active > LBM_SIDE_ES) return fail(LBM_ERR_ARG, "side active must be 0, 1 (NEE) or 2 (ES)");
+    if (sd.active < 0 || sd.active > LBM_SIDE_NEBB)
+      return fail(LBM_ERR_ARG, "side active must be 0, 1 (NEE), 2 (ES) or 3 (NEBB)");
+    if (sd.active == LBM_SIDE_NEBB && sd.v_type == LBM_BC_FLOWRATE)
+      return fail(LBM_ERR_ARG, "the flow-rate inlet runs under NEE or ES");
     if (!sd.active) continue;
     if (d->dim == 2 && s >= 4) return fail(LBM_ERR_ARG, "z sides cannot be active in 2D");
     const int types[3] = {sd.v_type, sd.rho_type, sd.T_type};

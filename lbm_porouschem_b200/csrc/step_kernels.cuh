@@ -166,6 +166,7 @@ struct StepParams {
   C Trs, Tss, cap_f, cap_s, sig_dx, Tamb4;
   int radiation;
   int fp16_nearest;  // FP16 storage: temperature populations rounded to nearest (else stochastically)
+  int nebb;          // the active sides use NEBB (Zou-He, 2D, no temperature field)
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -1376,6 +1377,109 @@ __device__ __forceinline__ MState<L, S> bc_state(const StepParams<S>& p, int x, 
   }
 }
 
+// Non-equilibrium bounce-back (Zou & He 1997) on the post-stream D2Q9 populations of a cell
+// of side `side` (BC_MODEL.NEBB, src/LBM/LBM2D/_boundary.py:103-226): the populations that
+// enter from outside are rebuilt from the known ones so that the cell takes the side's
+// velocity (v_type fixed: wall or inlet) or density (rho_type fixed: outlet, the normal
+// velocity then follows from the known populations; tangential velocity 0).  Every side in
+// the Zou-He form (the reference's side-1 wall, side-1 inlet and side-2/3 inlet and outlet
+// branches do otherwise; the oracle's ref_quirk_nebb restates them).
+template <class C>
+__device__ __forceinline__ void zou_he(int side, const lbm_side_desc& sd, C F[9]) {
+  const bool vel = sd.v_type == LBM_BC_FIXEDVALUE, pres = sd.rho_type == LBM_BC_FIXEDVALUE;
+  if (!vel && !pres) return;
+  const C u = (C)sd.v[0], v = (C)sd.v[1], c23 = (C)(2.0 / 3.0), c16 = (C)(1.0 / 6.0), h = (C)0.5;
+  C rho, w;
+  switch (side) {
+    case 0:  // x = 0: 1, 5, 8 enter
+      if (vel) {
+        rho = (F[0] + F[2] + F[4] + 2 * (F[3] + F[6] + F[7])) / ((C)1 - u);
+        F[1] = F[3] + c23 * rho * u;
+        F[5] = F[7] + h * (F[4] - F[2]) + c16 * rho * u + h * rho * v;
+        F[8] = F[6] + h * (F[2] - F[4]) + c16 * rho * u - h * rho * v;
+      } else {
+        rho = (C)sd.rho;
+        w = (C)1 - (F[0] + F[2] + F[4] + 2 * (F[3] + F[6] + F[7])) / rho;
+        F[1] = F[3] + c23 * rho * w;
+        F[5] = F[7] + h * (F[4] - F[2]) + c16 * rho * w;
+        F[8] = F[6] + h * (F[2] - F[4]) + c16 * rho * w;
+      }
+      break;
+    case 1:  // x = nx-1: 3, 6, 7 enter
+      if (vel) {
+        rho = (F[0] + F[2] + F[4] + 2 * (F[1] + F[5] + F[8])) / ((C)1 + u);
+        F[3] = F[1] - c23 * rho * u;
+        F[6] = F[8] + h * (F[4] - F[2]) - c16 * rho * u + h * rho * v;
+        F[7] = F[5] + h * (F[2] - F[4]) - c16 * rho * u - h * rho * v;
+      } else {
+        rho = (C)sd.rho;
+        w = (C)-1 + (2 * (F[1] + F[5] + F[8]) + F[0] + F[2] + F[4]) / rho;
+        F[3] = F[1] - c23 * rho * w;
+        F[6] = F[8] + h * (F[4] - F[2]) - c16 * rho * w;
+        F[7] = F[5] + h * (F[2] - F[4]) - c16 * rho * w;
+      }
+      break;
+    case 2:  // y = 0: 2, 5, 6 enter
+      if (vel) {
+        rho = (F[0] + F[1] + F[3] + 2 * (F[4] + F[7] + F[8])) / ((C)1 - v);
+        F[2] = F[4] + c23 * rho * v;
+        F[5] = F[7] + h * (F[3] - F[1]) + h * rho * u + c16 * rho * v;
+        F[6] = F[8] + h * (F[1] - F[3]) - h * rho * u + c16 * rho * v;
+      } else {
+        rho = (C)sd.rho;
+        w = (C)1 - (F[0] + F[1] + F[3] + 2 * (F[4] + F[7] + F[8])) / rho;
+        F[2] = F[4] + c23 * rho * w;
+        F[5] = F[7] + h * (F[3] - F[1]) + c16 * rho * w;
+        F[6] = F[8] + h * (F[1] - F[3]) + c16 * rho * w;
+      }
+      break;
+    default:  // y = ny-1: 4, 7, 8 enter
+      if (vel) {
+        rho = (F[0] + F[1] + F[3] + 2 * (F[2] + F[5] + F[6])) / ((C)1 + v);
+        F[4] = F[2] - c23 * rho * v;
+        F[7] = F[5] + h * (F[1] - F[3]) - h * rho * u - c16 * rho * v;
+        F[8] = F[6] + h * (F[3] - F[1]) + h * rho * u - c16 * rho * v;
+      } else {
+        rho = (C)sd.rho;
+        w = (C)-1 + (F[0] + F[1] + F[3] + 2 * (F[2] + F[5] + F[6])) / rho;
+        F[4] = F[2] - c23 * rho * w;
+        F[7] = F[5] + h * (F[1] - F[3]) - c16 * rho * w;
+        F[8] = F[6] + h * (F[3] - F[1]) - c16 * rho * w;
+      }
+      break;
+  }
+}
+
+// A cell on a NEBB side (2D, no temperature field): its own post-stream populations (the
+// ones that enter from outside came across the periodic wrap, as the reference streams),
+// Zou-He for the side that treats it -- an x side on rows 1 .. ny-2, a y side on every
+// column (Boundary_condition_NEBB's two loops) -- then macro and the collision.
+template <class L, class S, int COLL, int THERM>
+__device__ __forceinline__ void nebb_boundary_cell(const StepParams<S>& p, int x, int y, int c,
+                                                   DiagAcc<typename Store<S>::C>& acc, bool diag) {
+  using K = Kern<L, S>;
+  using C = typename Store<S>::C;
+  if constexpr (L::DIM == 2 && THERM == 0) {
+    const Nbhd nb(x, y, 0, p.nx, p.ny, 1);
+    const uint32_t nbits = K::neighbour_bits(p, nb, p.par);
+    C F[L::Q];
+    K::template pull_flow<false>(p, nb, c, nbits, F);
+    int side = -1;
+    if (y >= 1 && y <= p.ny - 2 && x == 0 && (p.active & 1)) side = 0;
+    else if (y >= 1 && y <= p.ny - 2 && x == p.nx - 1 && (p.active & 2)) side = 1;
+    else if (y == 0 && (p.active & 4)) side = 2;
+    else if (y == p.ny - 1 && (p.active & 8)) side = 3;
+    if (side >= 0) zou_he<C>(side, p.sides[side], F);
+    C rho, ux, uy, uz;
+    K::moments(p, F, rho, ux, uy, uz);
+    if (diag) diag_flow(p, acc, c, rho, ux, uy, uz);
+    if (!(p.flags & kStepPeek)) {
+      K::template collide_flow<COLL>(p, F, rho, ux, uy, uz);
+      K::store_flow(p, c, F);
+    }
+  }
+}
+
 // Boundary cell i of face `face` (a cell on several active faces is owned by the
 // lowest-numbered one): NEE state, collision, store.
 template <class L, class S, int COLL, int THERM>
@@ -1406,6 +1510,10 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   }
   if (!valid) return;
   const int c = x + p.nx * (y + p.ny * z);
+  if (p.nebb) {
+    nebb_boundary_cell<L, S, COLL, THERM>(p, x, y, c, acc, diag);
+    return;
+  }
   MState<L, S> s = bc_state<L, S, THERMAL, PYRO, L::NPASS - 1>(p, x, y, z, THERMAL);
   if (p.inlet && x <= 1 && !(p.flags & kStepPeek)) {
     // flow-rate inlet: record what the next step's controller reads (final values)

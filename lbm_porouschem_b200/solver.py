@@ -439,8 +439,15 @@ class _SolverBase:
                 active = False
             elif self.boundary_condition_model in (BC_MODEL.NEE, BC_MODEL.ES):
                 active = self.ref_quirk_nee_on_periodic or (vt, rt, Tt) != (PERIODIC, PERIODIC, PERIODIC)
+            elif self.boundary_condition_model == BC_MODEL.NEBB:
+                # Boundary_condition_NEBB (src/LBM/LBM2D/_boundary.py:103-226): the flow sides
+                # that are walls, inlets or outlets; 2D only (the 3D solver has none) and the
+                # scalar NEBB boundary reads the previous step's macro fields
+                if self.DIM != 2 or self.TEMPERATURE:
+                    raise NotImplementedError("NEBB is on the CUDA path in 2D without the temperature field")
+                active = (vt, rt) != (PERIODIC, PERIODIC)
             else:
-                raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path (NEE and ES only)")
+                raise NotImplementedError(f"{self.boundary_condition_model} is not on the CUDA path")
             v = self.v_BC[i]
             if self.bc[i] == BC_FLOW.inlet_flow and vt == FIXED_VALUE:
                 # the reference sets an inlet profile for side 0 only
@@ -452,7 +459,7 @@ class _SolverBase:
                     vt, v = FLOW_RATE, (self.flow_BC[0], 0.0, 0.0)
                 elif i == 0:
                     v = (self.flow_BC[0] / self.ny / self.nz, 0.0, 0.0)
-            model = "es" if self.boundary_condition_model == BC_MODEL.ES else "nee"
+            model = {BC_MODEL.ES: "es", BC_MODEL.NEBB: "nebb"}.get(self.boundary_condition_model, "nee")
             sides[i] = SideBC(active, vt, rt, Tt, v, self.rho_BC[i], self.TF.s_BC[i], model)
         return sides
 

