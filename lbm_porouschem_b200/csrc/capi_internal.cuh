@@ -329,6 +329,21 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.fp16_nearest = d.fp16_rounding == LBM_FP16_NEAREST;
   p.nebb = 0;
   for (int s = 0; s < 6; ++s) p.nebb |= d.side[s].active == LBM_SIDE_NEBB;
+  // sides whose cells store only their inward populations: NEE / ES sides where neither the
+  // side nor its opposite keeps a quantity of its own (a PERIODIC type makes the boundary
+  // kernel pull that side's own state, which reads the other slots across the wrap)
+  p.inward_only = 0;
+  for (int s = 0; s < 6; ++s) {
+    const lbm_side_desc& a = d.side[s];
+    const lbm_side_desc& b = d.side[s ^ 1];
+    auto keeps = [&d](const lbm_side_desc& q) {
+      return q.active && (q.v_type == LBM_BC_PERIODIC || q.rho_type == LBM_BC_PERIODIC ||
+                          (d.thermal && q.T_type == LBM_BC_PERIODIC));
+    };
+    const bool ok = (a.active == LBM_SIDE_NEE || a.active == LBM_SIDE_ES) && !keeps(a) && !keeps(b) &&
+                    b.active != LBM_SIDE_NEBB;
+    if (ok) p.inward_only |= 1 << s;
+  }
   p.active = 0;
   for (int s = 0; s < 6; ++s) if (d.side[s].active) p.active |= 1 << s;
   p.sides = h->ptr[LBM_FIELD_SCRATCH] ? scratch_sides(h) : nullptr;

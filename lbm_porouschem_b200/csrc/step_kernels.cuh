@@ -167,6 +167,8 @@ struct StepParams {
   int radiation;
   int fp16_nearest;  // FP16 storage: temperature populations rounded to nearest (else stochastically)
   int nebb;          // the active sides use NEBB (Zou-He, 2D, no temperature field)
+  int inward_only;   // bit s: a cell on side s alone stores only the populations that point
+                     // into the domain (the only ones any later pull reads there)
   int active;      // bit s: side s uses NEE
   const lbm_side_desc* sides;  // device copy
   int flags;       // LBM_STEP_* | kStepPeek
@@ -1539,10 +1541,36 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   }
   if (!(p.flags & kStepPeek)) {
     K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz, s.T);
-    K::store_flow(p, c, s.F);
-    if constexpr (THERMAL) {
-      K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
-      K::store_thermal(p, c, s.G);
+    if constexpr (THERMAL) K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
+    // A cell on one side whose pair keeps no quantity of its own (no PERIODIC type) is read
+    // afterwards only by the pulls of its inner neighbours, along the directions pointing
+    // into the domain (the side cells extrapolate from their inner cells, their own slots
+    // serve no bounce-back since the two outer layers are fluid); its other slots would be
+    // dead stores, each a lone 4-byte write to a sector of its own.
+    const int on = ((x == 0) ? 1 : 0) | ((x == p.nx - 1) ? 2 : 0) | ((y == 0) ? 4 : 0) | ((y == p.ny - 1) ? 8 : 0) |
+                   ((L::DIM == 3 && z == 0) ? 16 : 0) | ((L::DIM == 3 && z == p.nz - 1) ? 32 : 0);
+    const int act = on & p.active;
+    const int sd = (act && !(act & (act - 1)) && (p.inward_only & act)) ? __ffs(act) - 1 : -1;
+    if (sd < 0) {
+      K::store_flow(p, c, s.F);
+      if constexpr (THERMAL) K::store_thermal(p, c, s.G);
+    } else {
+      const int ax = sd >> 1, dir = (sd & 1) ? -1 : 1;
+      static_for<L::Q>([&](auto kk) {
+        constexpr int k = decltype(kk)::value;
+        const int e = ax == 0 ? L::ex(k) : (ax == 1 ? L::ey(k) : L::ez(k));
+        if (e == dir) Store<S>::st(p.fB, (size_t)k * p.N + c, s.F[k], fshift<L, S, k>(p));
+      });
+      if constexpr (THERMAL) {
+        static_for<L::QT>([&](auto kk) {
+          constexpr int k = decltype(kk)::value;
+          const int e = ax == 0 ? L::ex(k) : (ax == 1 ? L::ey(k) : L::ez(k));
+          if (e == dir) {
+            if (p.fp16_nearest) Store<S>::st(p.gB, (size_t)k * p.N + c, s.G[k], gshift<L, S, k>(p));
+            else Store<S>::st_sr(p.gB, (size_t)k * p.N + c, s.G[k], gshift<L, S, k>(p), 0x9e3779b9u * (k + 1));
+          }
+        });
+      }
     }
   }
 }
