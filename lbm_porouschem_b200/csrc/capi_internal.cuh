@@ -272,7 +272,12 @@ inline int* scratch_flips(lbm_handle* h) {
 }
 // Two-stage deterministic reduction of the block partials into scratch_final().
 inline void launch_reduce(lbm_handle* h, cudaStream_t st) {
-  reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), partial_rows(h->L), scratch_stage1(h));
+  const int rows = partial_rows(h->L);
+  if (rows <= kSingleReduceRows) {
+    reduce_diag_single<<<1, 1024, 0, st>>>(scratch_partials(h), rows, scratch_final(h));
+    return;
+  }
+  reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(scratch_partials(h), rows, scratch_stage1(h));
   reduce_diag_stage2<<<1, 256, 0, st>>>(scratch_stage1(h), kStage1Blocks, scratch_final(h));
 }
 

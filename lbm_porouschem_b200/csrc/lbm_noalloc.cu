@@ -118,8 +118,12 @@ extern "C" int32_t lbm_diag_noalloc(lbm_handle* h, lbm_diag* out, void* stream) 
   });
   if (rc) return rc;
   // every partial row and stage-1 slot read below is written earlier in this call
-  reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(diag, rows, diag + kStage1Off);
-  reduce_diag_stage2<<<1, 256, 0, st>>>(diag + kStage1Off, kStage1Blocks, diag + kFinalOff);
+  if (rows <= kSingleReduceRows) {   // the same reduction as the allocating path
+    reduce_diag_single<<<1, 1024, 0, st>>>(diag, rows, diag + kFinalOff);
+  } else {
+    reduce_diag_stage1<<<kStage1Blocks, 256, 0, st>>>(diag, rows, diag + kStage1Off);
+    reduce_diag_stage2<<<1, 256, 0, st>>>(diag + kStage1Off, kStage1Blocks, diag + kFinalOff);
+  }
   LBM_CUDA_TRY(cudaGetLastError());
   double v[kNumDiag];
   int flags = 0;

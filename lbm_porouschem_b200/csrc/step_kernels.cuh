@@ -1703,4 +1703,30 @@ static __global__ void __launch_bounds__(256) reduce_diag_stage2(const double* s
   }
 }
 
+// Both stages in one block of 1024 threads, for up to kSingleReduceRows partial rows (the
+// cell-list form at any size: its rows are the persistent blocks and the boundary blocks):
+// thread t combines rows t, t + 1024, ... in order, every field at once, then a fixed tree
+// per field.  Deterministic; one launch instead of two.
+constexpr int kSingleReduceRows = 8192;
+static __global__ void __launch_bounds__(1024) reduce_diag_single(const double* partials, int nrows, double* out) {
+  __shared__ double sh[1024];
+  double v[kNumDiag];
+#pragma unroll
+  for (int i = 0; i < kNumDiag; ++i) v[i] = diag_identity(i);
+  for (int r = threadIdx.x; r < nrows; r += blockDim.x) {
+#pragma unroll
+    for (int i = 0; i < kNumDiag; ++i) v[i] = diag_combine(i, v[i], partials[(size_t)i * nrows + r]);
+  }
+  for (int i = 0; i < kNumDiag; ++i) {
+    sh[threadIdx.x] = v[i];
+    __syncthreads();
+    for (int st = 512; st > 0; st >>= 1) {
+      if ((int)threadIdx.x < st) sh[threadIdx.x] = diag_combine(i, sh[threadIdx.x], sh[threadIdx.x + st]);
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[i] = (i == 3) ? sqrt(sh[0]) : sh[0];
+    __syncthreads();
+  }
+}
+
 }  // namespace lbm
