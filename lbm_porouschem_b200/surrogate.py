@@ -154,6 +154,36 @@ def fields_from_prediction(pred: np.ndarray, case: Case) -> dict:
     return {"rho": rho[..., None], "u": u, "T": T[..., None]}
 
 
+def project_solenoidal(ux: np.ndarray, uy: np.ndarray, solid: np.ndarray) -> tuple:
+    """The divergence-free part of a predicted velocity (S, S): u - grad(phi) with
+    lap(phi) = div(u) (forward-difference divergence, its adjoint as the gradient, so the
+    discrete divergence of the result is zero), periodic in y, no normal flow at the x walls;
+    then zero in the solid.  A guess with divergence starts pressure waves the relaxation has
+    to wait out; this removes the part of the guess that makes them."""
+    import scipy.sparse as sp
+    import scipy.sparse.linalg as spl
+    S = ux.shape[0]
+    n = S * S
+    idx = np.arange(n).reshape(S, S)
+    # forward differences: x (no flux through the walls: the last row's difference is 0), y periodic
+    rows, cols, vals = [], [], []
+    for i in range(S - 1):
+        rows += list(idx[i]); cols += list(idx[i + 1]); vals += [1.0] * S
+        rows += list(idx[i]); cols += list(idx[i]); vals += [-1.0] * S
+    Dx = sp.csr_matrix((vals, (rows, cols)), shape=(n, n))
+    Dy = (sp.csr_matrix((np.ones(n), (idx.ravel(), np.roll(idx, -1, axis=1).ravel())), shape=(n, n))
+          - sp.identity(n, format="csr"))
+    # gradient G = (Dx, Dy), divergence D = -G^T, so D G = -(Dx^T Dx + Dy^T Dy)
+    div = -(Dx.T @ ux.ravel()) - (Dy.T @ uy.ravel())
+    L = -(Dx.T @ Dx + Dy.T @ Dy) - 1e-9 * sp.identity(n)
+    phi = spl.spsolve(L.tocsc(), div)
+    vx = ux.ravel() - Dx @ phi
+    vy = uy.ravel() - Dy @ phi
+    vx = np.where(solid.ravel(), 0.0, vx).reshape(S, S)
+    vy = np.where(solid.ravel(), 0.0, vy).reshape(S, S)
+    return vx, vy
+
+
 # ----------------------------------------------------------------------------- steady solves
 def _t_plane(lat) -> torch.Tensor:
     from .lattice import _COMPUTE_DTYPE
@@ -570,11 +600,27 @@ def permeability(case: Case, fields: dict, nu: float = 0.1) -> float:
     return nu * float(np.mean(fields["u"][1])) / case.g
 
 
-def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, max_steps: int = 200_000) -> dict:
+def warm_fields(pred: np.ndarray, case: Case, mode: str) -> dict:
+    """Initial fields of a warm start: "warm" the prediction as it is, "warm_T" the predicted
+    temperature with the fluid at rest, "warm_proj" the prediction with its velocity made
+    divergence-free (project_solenoidal)."""
+    f0 = fields_from_prediction(pred, case)
+    if mode == "warm_T":
+        f0["u"] = np.zeros_like(f0["u"])
+    elif mode == "warm_proj":
+        vx, vy = project_solenoidal(f0["u"][0, ..., 0], f0["u"][1, ..., 0], case.solid)
+        f0["u"] = np.stack([vx, vy, np.zeros_like(vx)])[..., None]
+    return f0
+
+
+def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, max_steps: int = 200_000,
+             modes: tuple = ("warm",)) -> dict:
     """Time to the residual tolerance from rest (cold) and from the network's prediction
-    (warm) for each case, one lattice at a time; the pre-relaxation error of the
-    prediction and the converged permeability of both runs."""
+    (warm modes, warm_fields) for each case, one lattice at a time; the pre-relaxation error
+    of the prediction and the converged permeability of the runs.  The warm time includes
+    the inference and any projection."""
     from .lattice import Lattice
+    modes = ("warm",) + tuple(m for m in modes if m != "warm")
     x = inputs(cases)
     t_pred = time.perf_counter()
     pred = net.predict(x)
@@ -583,14 +629,16 @@ def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, 
     rows = []
     for c, p in zip(cases, pred):
         out = {}
-        for mode in ("cold", "warm"):
+        for mode in ("cold",) + tuple(modes):
             lat = Lattice(c.config())
             lat.set_geometry(c.solid[..., None])
+            t_prep = time.perf_counter()
             if mode == "cold":
                 lat.init(rho=1.0, u=(0.0, 0.0, 0.0), T=0.0)
             else:
-                f0 = fields_from_prediction(p, c)
+                f0 = warm_fields(p, c, mode)
                 lat.init(rho=f0["rho"], u=f0["u"], T=f0["T"])
+            prep_s = time.perf_counter() - t_prep if mode == "warm_proj" else 0.0
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             steps = relax(lat, tol, check, max_steps)
@@ -600,7 +648,7 @@ def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, 
             wall = time.perf_counter() - t0
             f = lat.fields()
             fl = {"rho": f["rho"][..., 0], "u": f["u"][:2, ..., 0], "T": f["T"][..., 0]}
-            out[mode] = {"steps": steps, "wall_s": wall + (infer_s if mode == "warm" else 0.0),
+            out[mode] = {"steps": steps, "wall_s": wall + (infer_s + prep_s if mode != "cold" else 0.0),
                          "k": permeability(c, fl), "fields": fl}
             lat.close()
         ref = out["cold"]["fields"]
@@ -614,12 +662,19 @@ def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, 
                      "cold_s": out["cold"]["wall_s"], "warm_s": out["warm"]["wall_s"],
                      "k_cold": out["cold"]["k"], "k_warm": out["warm"]["k"],
                      "k_rel_diff": abs(out["warm"]["k"] - out["cold"]["k"]) / abs(out["cold"]["k"]),
-                     "pre_err_u": err_u, "pre_err_T": err_T})
+                     "pre_err_u": err_u, "pre_err_T": err_T,
+                     **{f"{m}_steps": out[m]["steps"] for m in modes if m != "warm"},
+                     **{f"{m}_s": out[m]["wall_s"] for m in modes if m != "warm"}})
     ok = [r for r in rows if r["converged"]] or rows
     agg = {k: float(np.mean([r[k] for r in ok])) for k in ok[0] if k not in ("seed", "converged")}
     agg["time_ratio"] = float(np.sum([r["warm_s"] for r in ok]) / np.sum([r["cold_s"] for r in ok]))
     agg["steps_ratio"] = float(np.sum([r["warm_steps"] for r in ok]) / np.sum([r["cold_steps"] for r in ok]))
     agg["k_rel_diff_max"] = float(max(r["k_rel_diff"] for r in ok))
+    for m in modes:
+        if m != "warm":
+            agg[f"{m}_time_ratio"] = float(np.sum([r[f"{m}_s"] for r in ok]) / np.sum([r["cold_s"] for r in ok]))
+            agg[f"{m}_steps_ratio"] = float(np.sum([r[f"{m}_steps"] for r in ok]) /
+                                            np.sum([r["cold_steps"] for r in ok]))
     agg["infer_s_per_case"] = infer_s
     agg["cases_converged"] = len([r for r in rows if r["converged"]])
     agg["cases"] = len(rows)
@@ -627,7 +682,7 @@ def evaluate(net: UNet, cases: list[Case], tol: float = 1e-6, check: int = 100, 
 
 
 def experiment(S: int = 128, n_train: int = 1024, n_test: int = 32, epochs: int = 60, batch: int = 16,
-               lr: float = 2e-3, tol: float = 1e-6, seed0: int = 0, log=print) -> dict:
+               lr: float = 2e-3, tol: float = 1e-6, seed0: int = 0, log=print, modes: tuple = ("warm",)) -> dict:
     """The warm-start experiment: solve n_train seeded cases to steady state (one batch of
     lattices), train the U-Net on them, then compare warm and cold starts on n_test
     held-out cases.  Training and data-generation times are reported separately."""
@@ -644,7 +699,7 @@ def experiment(S: int = 128, n_train: int = 1024, n_test: int = 32, epochs: int 
     log(f"trained {net.nparams} parameters in {hist['train_s']:.1f} s, loss {hist['loss'][0]:.4f} -> {hist['loss'][-1]:.5f}")
     fit = prediction_errors(net, used[:32])
     log(f"prediction error on training cases: u {fit['u']:.3f}, T {fit['T']:.3f}, velocity scale {fit['scale']:.3f}")
-    res = evaluate(net, test_cases, tol=tol, check=100, max_steps=400_000)
+    res = evaluate(net, test_cases, tol=tol, check=100, max_steps=400_000, modes=modes)
     m = res["mean"]
     log(f"warm/cold: steps {m['steps_ratio']:.3f}, time {m['time_ratio']:.3f}; pre-relaxation error u "
         f"{m['pre_err_u']:.3f}, T {m['pre_err_T']:.3f}; permeability difference max {m['k_rel_diff_max']:.2e}")
@@ -664,8 +719,9 @@ if __name__ == "__main__":
     ap.add_argument("--test", type=int, default=32)
     ap.add_argument("--epochs", type=int, default=60)
     ap.add_argument("--out", default="")
+    ap.add_argument("--modes", default="warm", help="warm starts to time: warm, warm_T, warm_proj (comma list)")
     a = ap.parse_args()
-    r = experiment(a.size, a.train, a.test, a.epochs)
+    r = experiment(a.size, a.train, a.test, a.epochs, modes=tuple(a.modes.split(",")))
     txt = json.dumps(r, default=float)
     if a.out:
         with open(a.out, "w") as f:
