@@ -42,12 +42,14 @@ template <class S> struct Store;
 template <> struct Store<float> {
   using C = float;
   __device__ __forceinline__ static C ld(const float* p, size_t i, C) { return p[i]; }
+  __device__ __forceinline__ static C ldg(const float* p, size_t i, C) { return __ldg(p + i); }
   __device__ __forceinline__ static void st(float* p, size_t i, C v, C) { p[i] = v; }
   __device__ __forceinline__ static void st_sr(float* p, size_t i, C v, C, uint32_t) { p[i] = v; }
 };
 template <> struct Store<double> {
   using C = double;
   __device__ __forceinline__ static C ld(const double* p, size_t i, C) { return p[i]; }
+  __device__ __forceinline__ static C ldg(const double* p, size_t i, C) { return __ldg(p + i); }
   __device__ __forceinline__ static void st(double* p, size_t i, C v, C) { p[i] = v; }
   __device__ __forceinline__ static void st_sr(double* p, size_t i, C v, C, uint32_t) { p[i] = v; }
 };
@@ -82,6 +84,9 @@ template <> struct Store<__half> {
   using C = float;
   __device__ __forceinline__ static C ld(const __half* p, size_t i, C shift) {
     return __half2float(p[i]) + shift;
+  }
+  __device__ __forceinline__ static C ldg(const __half* p, size_t i, C shift) {
+    return __half2float(__ldg(p + i)) + shift;
   }
   // stochastically rounded store (the temperature populations); salt: per direction
   __device__ __forceinline__ static void st_sr(__half* p, size_t i, C v, C shift, uint32_t salt) {
@@ -303,12 +308,12 @@ struct Kern {
     static_for<Q>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       if constexpr (k == 0) {
-        F[0] = Store<S>::ld(p.fA, c, fshift<L, S, 0>(p));
+        F[0] = Store<S>::ldg(p.fA, c, fshift<L, S, 0>(p));
       } else {
         const int src = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
         const bool bb = (nbits >> L::opp(k)) & 1;
         const size_t idx = bb ? (size_t)L::opp(k) * p.N + c : (size_t)k * p.N + src;
-        C v = Store<S>::ld(p.fA, idx, fshift<L, S, k>(p));
+        C v = Store<S>::ldg(p.fA, idx, fshift<L, S, k>(p));
         if constexpr (PYRO) {
           if (bb) v += p.relA[src] * (C)L::w(k);
         }
@@ -330,14 +335,14 @@ struct Kern {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       if constexpr (k == 0) {
-        G[0] = Store<S>::ld(p.gA, c, gshift<L, S, 0>(p));
+        G[0] = Store<S>::ldg(p.gA, c, gshift<L, S, 0>(p));
       } else {
         size_t idx = (size_t)k * p.N + nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
         if constexpr (ADIA || RT) {
           if ((ADIA || p.adiabatic) && ((nbits >> L::opp(k)) & 1) != (uint32_t)solid)
             idx = (size_t)L::opp(k) * p.N + c;
         }
-        G[k] = Store<S>::ld(p.gA, idx, gshift<L, S, k>(p));
+        G[k] = Store<S>::ldg(p.gA, idx, gshift<L, S, k>(p));
       }
     });
   }
@@ -352,7 +357,7 @@ struct Kern {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       if constexpr (k == 0) {
-        G[0] = Store<S>::ld(p.gA, c, gshift<L, S, 0>(p));
+        G[0] = Store<S>::ldg(p.gA, c, gshift<L, S, 0>(p));
       } else {
         const int n = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
         const S* src = p.gA;
@@ -361,7 +366,7 @@ struct Kern {
           if (solid && p.poro[n] > (C)0) src = p.gsA;
           else idx = (size_t)L::opp(k) * p.N + c;
         }
-        G[k] = Store<S>::ld(src, idx, gshift<L, S, k>(p));
+        G[k] = Store<S>::ldg(src, idx, gshift<L, S, k>(p));
       }
     });
   }
@@ -371,14 +376,14 @@ struct Kern {
     static_for<QT>([&](auto kk) {
       constexpr int k = decltype(kk)::value;
       if constexpr (k == 0) {
-        GS[0] = Store<S>::ld(p.gsA, c, gshift<L, S, 0>(p));
+        GS[0] = Store<S>::ldg(p.gsA, c, gshift<L, S, 0>(p));
       } else {
         const int n = nb.at(-L::ex(k), -L::ey(k), -L::ez(k));
         const S* src = p.gsA;
         size_t idx = (size_t)k * p.N + n;
         if ((nbits >> L::opp(k)) & 1) src = p.gA;
         else if (!(p.poro[n] > (C)0)) idx = (size_t)L::opp(k) * p.N + c;
-        GS[k] = Store<S>::ld(src, idx, gshift<L, S, k>(p));
+        GS[k] = Store<S>::ldg(src, idx, gshift<L, S, k>(p));
       }
     });
   }
