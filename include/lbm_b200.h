@@ -172,6 +172,23 @@ typedef struct lbm_desc {
   double T_ambient;            /* K (TS.Tambient, set_radiation) */
   int32_t radiation;           /* 1: surface radiation (RADIATION_MODEL.SURFACE_UNIFORM) */
   int32_t fp16_rounding;       /* LBM_PREC_FP16: LBM_FP16_STOCHASTIC (0) or LBM_FP16_NEAREST */
+  /* Temperature-dependent thermal properties, THERMAL_DIFF_MODEL.DERIVED
+   * (src/LBM/LBM2D/_thermal.py:62-107 fluid, :167-210 solid).  Bit p of tprop (p = 0
+   * fluid, 1 solid) replaces the phase's constant tauT_fluid / tauT_solid by a per-cell
+   * rate: D = k(T) / rho / c(T) * dt / dx^2 at the cell's temperature in kelvin
+   * (T*T_scale + T_ref for the fluid, T*Ts_scale + Ts_ref for the solid), rho the cell's
+   * lattice density for the fluid and tp_rhos for the solid, and tau = 3 D + 1/2 (2D) or
+   * 4 D + 1/2 (3D).  k and c are the reference's nested form of five coefficients,
+   * c0 + T (c1 + T (c2 T + T (c3 + T c4))) (a constant is {c0, 0, 0, 0, 0}; the solid
+   * conductivity takes c4 = 0); c uses tp_cap_lo below tp_cap_Tmid and tp_cap_hi from it on
+   * (NASA7 ranges; equal arrays for one polynomial), times tp_cap_mul (the gas constant for
+   * a fluid NASA7 capacity, else 1).  Temperature fields THERMAL_CONJUGATE / TWO_FIELD
+   * only, without porous cells. */
+  int32_t tprop;
+  double tp_cond[2][5], tp_cap_lo[2][5], tp_cap_hi[2][5];
+  double tp_cap_Tmid[2], tp_cap_mul[2];
+  double tp_rhos;         /* solid density of the derived solid diffusivity (uniform) */
+  double tp_dt, tp_dx2;   /* dt and dx^2 of the physical units */
 } lbm_desc;
 
 /* Diagnostics (FP64 accumulation).  No reference counterpart except umax,

@@ -80,6 +80,9 @@ class lbm_desc(C.Structure):
         ("viscosity", C.c_int32), ("porous", C.c_int32), ("suth_A", C.c_double), ("suth_Ts", C.c_double),
         ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
         ("dx_phys", C.c_double), ("T_ambient", C.c_double), ("radiation", C.c_int32), ("fp16_rounding", C.c_int32),
+        ("tprop", C.c_int32), ("tp_cond", (C.c_double * 5) * 2), ("tp_cap_lo", (C.c_double * 5) * 2),
+        ("tp_cap_hi", (C.c_double * 5) * 2), ("tp_cap_Tmid", C.c_double * 2), ("tp_cap_mul", C.c_double * 2),
+        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double),
     ]
 
 

@@ -118,6 +118,14 @@ class LatticeConfig:
     radiation: bool = False         # surface radiation of porous cells (RADIATION_MODEL.SURFACE_UNIFORM)
     T_ambient: float = 300.0        # K
     fp16_rounding: str = "stochastic"  # FP16 storage of the temperature populations: "stochastic" | "nearest"
+    # temperature-dependent thermal properties (THERMAL_DIFF_MODEL.DERIVED) per phase: None
+    # (the constant tauT_fluid / tauT_solid) or a dict made by thermal_props(); tp_rhos is
+    # the solid density of the derived solid diffusivity, tp_dt and tp_dx2 the physical dt, dx^2
+    tprop_fluid: dict | None = None
+    tprop_solid: dict | None = None
+    tp_rhos: float = 1.0
+    tp_dt: float = 1.0
+    tp_dx2: float = 1.0
 
     @property
     def shape(self) -> tuple:
@@ -199,12 +207,57 @@ class LatticeConfig:
         d.cap_fluid, d.cap_solid, d.dx_phys = self.cap_fluid, self.cap_solid, self.dx_phys
         d.T_ambient, d.radiation = self.T_ambient, int(self.radiation)
         d.fp16_rounding = {"stochastic": N.LBM_FP16_STOCHASTIC, "nearest": N.LBM_FP16_NEAREST}[self.fp16_rounding]
+        d.tprop = 0
+        for ph, tp in enumerate((self.tprop_fluid, self.tprop_solid)):
+            if tp is None:
+                continue
+            d.tprop |= 1 << ph
+            for i in range(5):
+                d.tp_cond[ph][i] = float(tp["cond"][i])
+                d.tp_cap_lo[ph][i] = float(tp["cap_lo"][i])
+                d.tp_cap_hi[ph][i] = float(tp["cap_hi"][i])
+            d.tp_cap_Tmid[ph], d.tp_cap_mul[ph] = float(tp["cap_Tmid"]), float(tp["cap_mul"])
+        d.tp_rhos, d.tp_dt, d.tp_dx2 = self.tp_rhos, self.tp_dt, self.tp_dx2
         return d
 
     @property
     def porous_heat(self) -> bool:
         """Porous cells with two temperature fields: a porous cell carries TF and TS."""
         return self.porous != "none" and self.thermal == "two_field"
+
+
+GAS_CONSTANT = 8.314441   # J/(mol K), src/LBM/util/constant.py:17
+
+
+def thermal_props(cond=None, cond_poly=None, cap=None, cap_poly=None, nasa7=None, solid=False) -> dict:
+    """One phase's temperature-dependent diffusivity inputs (src/LBM/LBM2D/_thermal.py:62-107,
+    :167-210): a constant or polynomial conductivity, a constant, polynomial or NASA7
+    (Trange, 2 x 7 coefficients) capacity.  The polynomials keep the reference's nested form
+    c0 + T (c1 + T (c2 T + T (c3 + T c4))); the solid conductivity uses four coefficients and a
+    fluid NASA7 capacity is multiplied by the gas constant (the solid's is not)."""
+    def five(v):
+        v = [float(x) for x in v]
+        return (v + [0.0] * 5)[:5]
+    if cond_poly is not None:
+        kc = five(cond_poly)
+        if solid:
+            kc[4] = 0.0
+    elif cond is not None:
+        kc = [float(cond), 0.0, 0.0, 0.0, 0.0]
+    else:
+        raise ValueError("a derived diffusivity needs a conductivity")
+    mul, Tmid = 1.0, 0.0
+    if nasa7 is not None:
+        Trange, data = nasa7
+        lo, hi, Tmid = five(data[0]), five(data[1]), float(Trange[1])
+        mul = 1.0 if solid else GAS_CONSTANT
+    elif cap_poly is not None:
+        lo = hi = five(cap_poly)
+    elif cap is not None:
+        lo = hi = [float(cap), 0.0, 0.0, 0.0, 0.0]
+    else:
+        raise ValueError("a derived diffusivity needs a capacity")
+    return dict(cond=kc, cap_lo=lo, cap_hi=hi, cap_Tmid=Tmid, cap_mul=mul)
 
 
 def fill_sides(arr, sides) -> None:

@@ -318,7 +318,22 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.pyA = (C)d.pyro_A; p.pyb = (C)d.pyro_b; p.pyEaR = (C)(d.pyro_Ea / kGasConstant); p.pyTmin = (C)d.pyro_Tmin;
   p.Tref = (C)d.T_ref; p.Tscale = (C)d.T_scale; p.dtp = (C)d.dt_phys;
   p.heat_norm = (C)d.heat_norm; p.gas_coef = (C)d.gas_coef; p.alpha_flip = (C)d.alpha_flip;
+  p.suth = d.viscosity == LBM_VISC_SUTHERLAND;
   p.suthA = (C)d.suth_A; p.suthTs = (C)d.suth_Ts;
+  p.tprop = d.tprop;
+  for (int ph = 0; ph < 2; ++ph) {
+    for (int i = 0; i < 5; ++i) {
+      p.tp_cond[ph][i] = (C)d.tp_cond[ph][i];
+      p.tp_lo[ph][i] = (C)d.tp_cap_lo[ph][i];
+      p.tp_hi[ph][i] = (C)d.tp_cap_hi[ph][i];
+    }
+    p.tp_Tmid[ph] = (C)d.tp_cap_Tmid[ph];
+    p.tp_mul[ph] = (C)d.tp_cap_mul[ph];
+  }
+  p.tp_Tsc[0] = (C)d.T_scale; p.tp_Tref[0] = (C)d.T_ref;
+  p.tp_Tsc[1] = (C)d.Ts_scale; p.tp_Tref[1] = (C)d.Ts_ref;
+  p.tp_rhos = (C)d.tp_rhos; p.tp_dt = (C)d.tp_dt; p.tp_dx2 = (C)d.tp_dx2;
+  p.tp_lat = (C)(d.dim == 2 ? 3 : 4);
   p.poro = (const C*)h->ptr[LBM_FIELD_PORO];
   p.darcy = (const C*)h->ptr[LBM_FIELD_DARCY];
   p.forch = (const C*)h->ptr[LBM_FIELD_FORCH];

@@ -9,13 +9,14 @@
 namespace lbm {
 namespace capi {
 
-// Collision code of the kernels: LBM_COLL_*, plus kCollSutherland with the Sutherland
-// viscosity (thermal modes only: THERM 1-3), or plus kCollPorous with porous cells (no
-// temperature field, THERM 0, or two fields exchanging heat in them, THERM 4)
+// Collision code of the kernels: LBM_COLL_*, plus kCollSutherland with properties that
+// follow the cell's temperature (the Sutherland viscosity, derived thermal diffusivities;
+// thermal modes only: THERM 1-3), or plus kCollPorous with porous cells (no temperature
+// field, THERM 0, or two fields exchanging heat in them, THERM 4)
 constexpr int kSB = kCollSutherland + LBM_COLL_BGK, kSM = kCollSutherland + LBM_COLL_MRT;
 constexpr int kPB = kCollPorous + LBM_COLL_BGK, kPM = kCollPorous + LBM_COLL_MRT;
 inline int collision_code(const lbm_desc& d) {
-  return d.collision + (d.viscosity == LBM_VISC_SUTHERLAND ? kCollSutherland : 0) +
+  return d.collision + ((d.viscosity == LBM_VISC_SUTHERLAND || d.tprop) ? kCollSutherland : 0) +
          (d.porous != LBM_PORO_NONE ? kCollPorous : 0);
 }
 // Temperature code of the kernels (THERM): 0 none, 1 conjugate, 2 conjugate + pyrolysis,

@@ -4,6 +4,7 @@
 // sm_100a kernels of step_kernels.cuh on the caller's stream.  No allocation
 // happens here: every buffer (including the reduction scratch) is bound by the
 // caller, sized by lbm_required_bytes().
+#include <cmath>
 #include <cstddef>
 #include "capi_internal.cuh"
 
@@ -65,6 +66,21 @@ static int validate(const lbm_desc* d) {
                              "T_scale and Ts_scale, and dx_phys > 0 with radiation");
   if (d->fp16_rounding != LBM_FP16_STOCHASTIC && d->fp16_rounding != LBM_FP16_NEAREST)
     return fail(LBM_ERR_ARG, "fp16_rounding must be LBM_FP16_STOCHASTIC or LBM_FP16_NEAREST");
+  if (d->tprop) {
+    if ((d->tprop & ~3) || d->thermal == LBM_THERMAL_NONE || d->porous)
+      return fail(LBM_ERR_ARG, "temperature-dependent thermal properties (tprop bits 0, 1) need the conjugate or "
+                               "two-field temperature, without porous cells");
+    if (!(d->tp_dt > 0 && d->tp_dx2 > 0) || ((d->tprop & 2) && !(d->tp_rhos > 0)))
+      return fail(LBM_ERR_ARG, "tprop needs tp_dt > 0, tp_dx2 > 0 and, for the solid, tp_rhos > 0");
+    for (int ph = 0; ph < 2; ++ph) {
+      if (!((d->tprop >> ph) & 1)) continue;
+      bool ok = std::isfinite(d->tp_cap_Tmid[ph]) && std::isfinite(d->tp_cap_mul[ph]) && d->tp_cap_mul[ph] != 0;
+      for (int i = 0; i < 5; ++i)
+        ok = ok && std::isfinite(d->tp_cond[ph][i]) && std::isfinite(d->tp_cap_lo[ph][i]) &&
+             std::isfinite(d->tp_cap_hi[ph][i]);
+      if (!ok) return fail(LBM_ERR_ARG, "tprop coefficients must be finite and tp_cap_mul non-zero");
+    }
+  }
   if (d->radiation && !(d->porous && d->thermal == LBM_THERMAL_TWOFIELD))
     return fail(LBM_ERR_ARG, "radiation is a source of porous cells in the two-field temperature model");
   int nebb = 0, other = 0;
@@ -343,8 +359,10 @@ int batch_members(lbm_handle* const* hs, int32_t n, cudaStream_t st, std::vector
     if (!h->L.list)
       return fail(LBM_ERR_ARG, "batch member " + std::to_string(i) + " does not use cell lists (set bulk_form = 2)");
     if (h->d.dim != d0.dim || h->d.precision != d0.precision || h->d.collision != d0.collision ||
-        h->d.thermal != d0.thermal || h->d.pyro != d0.pyro || h->d.viscosity != d0.viscosity)
-      return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, viscosity, thermal and pyro");
+        h->d.thermal != d0.thermal || h->d.pyro != d0.pyro || h->d.viscosity != d0.viscosity ||
+        (h->d.tprop != 0) != (d0.tprop != 0))
+      return fail(LBM_ERR_ARG, "batch members must share dim, precision, collision, viscosity, thermal, pyro and "
+                               "whether tprop is set");
     if (h->device != hs[0]->device) return fail(LBM_ERR_ARG, "batch members must live on one device");
     if ((h->step & 1) != (hs[0]->step & 1)) return fail(LBM_ERR_ARG, "batch members must be at the same step parity");
     if (has_flowrate(h->d)) return fail(LBM_ERR_ARG, "batch members cannot have a flow-rate inlet");

@@ -157,7 +157,14 @@ struct StepParams {
   C itauT_f, itauT_s;
   C rho0, T0;
   C pyA, pyb, pyEaR, pyTmin, Tref, Tscale, dtp, heat_norm, gas_coef, alpha_flip;  // pyEaR = Ea/R
-  C suthA, suthTs;  // Sutherland viscosity (collision codes kCollSutherland + BGK/MRT)
+  // collision codes kCollSutherland + BGK/MRT (properties that follow the cell's
+  // temperature): the Sutherland viscosity (suth set), and per phase (bit 0 fluid, 1 solid of
+  // tprop) the derived thermal diffusivity k(T) / rho / c(T) * dt / dx^2 (lbm_desc.tprop)
+  int suth;
+  C suthA, suthTs;
+  int tprop;
+  C tp_cond[2][5], tp_lo[2][5], tp_hi[2][5], tp_Tmid[2], tp_mul[2], tp_Tsc[2], tp_Tref[2];
+  C tp_rhos, tp_dt, tp_dx2, tp_lat;
   const C* poro;   // porous cells (collision codes kCollPorous + BGK/MRT): solid fraction,
   const C* darcy;  //   Darcy and Forchheimer coefficients per cell, and the model
   const C* forch;  //   (LBM_PORO_*)
@@ -528,9 +535,11 @@ struct Kern {
                                                         const Drive& dr) {
     C nu = p.nu;
     if constexpr (coll_sutherland(COLL)) {
-      // Sutherland, src/LBM/LBM2D/_evolution.py:232-234, at the cell's temperature in kelvin
-      const C TK = T * p.Tscale + p.Tref;
-      nu = p.suthA * TK * sqrt(TK) / (TK + p.suthTs);
+      if (p.suth) {
+        // Sutherland, src/LBM/LBM2D/_evolution.py:232-234, at the cell's temperature in kelvin
+        const C TK = T * p.Tscale + p.Tref;
+        nu = p.suthA * TK * sqrt(TK) / (TK + p.suthTs);
+      }
     }
     const C tau = (C)3 * (p.eos == 0 ? nu / rho : nu) + (C)0.5;
     const C itau = (C)1 / tau;
@@ -613,6 +622,30 @@ struct Kern {
         F[k] += guo<k>(p, rho, ux, uy, uz, pre, dr);
       });
     }
+  }
+
+  // Thermal relaxation rate of a cell: its phase's constant, or where the phase's bit of
+  // tprop is set (collision codes kCollSutherland + BGK/MRT) the derived diffusivity at
+  // the cell's temperature, TF/TS.coefDiff with DERIVED (src/LBM/LBM2D/_thermal.py:62-71,
+  // :167-174), conductivity and capacity in the nested form of :72-107 / :175-210, and
+  // tau = 3 D + 1/2 (2D) or 4 D + 1/2 (3D) (_scalarField.py:56-58 of LBM2D / LBM3D).
+  template <int COLL>
+  __device__ __forceinline__ static C itau_thermal(const P& p, bool fluid, C T, C rho) {
+    if constexpr (coll_sutherland(COLL)) {
+      const int ph = fluid ? 0 : 1;
+      if ((p.tprop >> ph) & 1) {
+        const C Tp = T * p.tp_Tsc[ph] + p.tp_Tref[ph];
+        const C k = nested5(p.tp_cond[ph], Tp);
+        const C cm = (Tp < p.tp_Tmid[ph] ? nested5(p.tp_lo[ph], Tp) : nested5(p.tp_hi[ph], Tp)) * p.tp_mul[ph];
+        const C D = k / (fluid ? rho : p.tp_rhos) / cm * p.tp_dt / p.tp_dx2;
+        return (C)1 / (p.tp_lat * D + (C)0.5);
+      }
+    }
+    return fluid ? p.itauT_f : p.itauT_s;
+  }
+  // c0 + T (c1 + T (c2 T + T (c3 + T c4))), the reference's evaluation order
+  __device__ __forceinline__ static C nested5(const C* c, C T) {
+    return c[0] + T * (c[1] + T * (c[2] * T + T * (c[3] + T * c[4])));
   }
 
   // Thermal collision with source, one code path for fluid and solid cells:
@@ -1038,8 +1071,8 @@ __device__ __forceinline__ bool cell_update(const StepParams<S>& p, DiagAcc<type
   if constexpr (THERMAL) {
     if (!peek && !flipping) {
       const bool fl = !solid;
-      K::template collide_thermal<PHEAT>(p, G, T, fl ? p.itauT_f : p.itauT_s, fl ? ux : (C)0, fl ? uy : (C)0,
-                                         fl ? uz : (C)0, dS);
+      K::template collide_thermal<PHEAT>(p, G, T, K::template itau_thermal<COLL>(p, fl, T, rho), fl ? ux : (C)0,
+                                         fl ? uy : (C)0, fl ? uz : (C)0, dS);
       K::store_thermal(p, c, G);
     }
     if (diag) diag_thermal(p, acc, c, T);
@@ -1190,7 +1223,7 @@ __device__ __forceinline__ void flip_one(const StepParams<S>& p, DiagAcc<typenam
     // (src/LBM/LBM2D/_evolution.py:54-56)
     const C dS = p.relB[c];
     p.relB[c] = (C)0;
-    K::template collide_thermal<true>(p, G, T, p.itauT_f, ux, uy, uz, dS);
+    K::template collide_thermal<true>(p, G, T, K::template itau_thermal<COLL>(p, true, T, rb), ux, uy, uz, dS);
     K::store_thermal(p, c, G);
   }
   if (diag) diag_flow(p, acc, c, rb, ux, uy, uz);
@@ -1546,7 +1579,8 @@ __device__ __forceinline__ void boundary_cell(const StepParams<S>& p, int face, 
   }
   if (!(p.flags & kStepPeek)) {
     K::template collide_flow<COLL>(p, s.F, s.rho, s.ux, s.uy, s.uz, s.T);
-    if constexpr (THERMAL) K::collide_thermal(p, s.G, s.T, p.itauT_f, s.ux, s.uy, s.uz, (C)0);
+    if constexpr (THERMAL)
+      K::collide_thermal(p, s.G, s.T, K::template itau_thermal<COLL>(p, true, s.T, s.rho), s.ux, s.uy, s.uz, (C)0);
     // A cell on one side whose pair keeps no quantity of its own (no PERIODIC type) is read
     // afterwards only by the pulls of its inner neighbours, along the directions pointing
     // into the domain (the side cells extrapolate from their inner cells, their own slots

@@ -24,7 +24,7 @@ from typing import Callable, Optional
 
 import numpy as np
 
-from .config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC
+from .config import FIXED_VALUE, FLOW_RATE, PERIODIC, ZERO_GRADIENT, LatticeConfig, SideBC, thermal_props
 from .flag import (BC, BC_FLOW, BC_MODEL, FLUID_STATE_EQUATION, FORCE_TERM, PORO_MODEL, RADIATION_MODEL, SOURCE_TERM,
                    VISCOSITY_MODEL)
 from .vtk import PVDWriter, write_vts
@@ -88,11 +88,14 @@ class ScalarFieldView:
         self.BC = [BC.periodic] * solver._nsides
         self.s_BC = [0.0] * solver._nsides
         self.thermal_diff = 3e-5
-        # THERMAL_DIFF_MODEL.DERIVED with constant conductivity and capacity
-        # (src/LBM/LBM2D/_thermal.py:62-107): D = cond / (rho cm)
+        # THERMAL_DIFF_MODEL.DERIVED (src/LBM/LBM2D/_thermal.py:62-107): D = cond / (rho cm),
+        # conductivity constant or polynomial, capacity constant, polynomial or NASA7
         self.derived = False
         self.cond: Optional[float] = None
+        self.cond_poly: Optional[list] = None
         self.cm: Optional[float] = None
+        self.cm_poly: Optional[list] = None
+        self.nasa7: Optional[tuple] = None      # (Trange, 2 x 7 coefficients)
         # heat exchange and radiation of porous cells (TS, src/LBM/LBM2D/_thermal.py:110-120):
         # per-cell exchange coefficient and surface, radiating surface and emissivity
         self.exchangeCoef = Field(solver, name + "_exchangeCoef")
@@ -237,41 +240,76 @@ class _SolverBase:
     def set_solid_Trange(self, Trange):
         self.TS.v_ref, self.TS.v_scale = Trange[0], Trange[1] - Trange[0]
 
+    # each diffusivity setter selects its model (src/LBM/LBM2D/_io.py:174-184, :218-224)
     def set_fluid_thermal_diff(self, diff):
-        self.TF.thermal_diff = diff
+        self.TF.thermal_diff, self.TF.derived = diff, False
 
     def set_solid_thermal_diff(self, diff):
-        self.TS.thermal_diff = diff
+        self.TS.thermal_diff, self.TS.derived = diff, False
 
     def set_fluid_Prandtl(self, Pr):
-        self.TF.thermal_diff = self.visco / Pr
+        self.TF.thermal_diff, self.TF.derived = self.visco / Pr, False
 
-    # derived diffusivity D = cond / (rho cm) (src/LBM/LBM2D/_io.py:182-248,
-    # _thermal.py:62-107): constant conductivity and capacity only; the fluid density is
-    # taken as rho0 = 1 (the reference divides by the cell's lattice density, ~1), the
-    # solid's from add_rho_solid (uniform over the solid cells)
+    # derived diffusivity D = cond(T) / (rho cm(T)) (src/LBM/LBM2D/_io.py:182-251,
+    # _thermal.py:62-107, :167-210), evaluated per cell at its temperature by the kernels
+    # (lbm_desc.tprop): the fluid divides by the cell's lattice density, the solid by its
+    # density from add_rho_solid (uniform over the solid cells).  Each setter replaces the
+    # phase's previous conductivity or capacity model, as the reference's do.
     def set_fluid_thermal_diff_derived(self):
         self.TF.derived = True
 
     def set_fluid_conductivity(self, value):
-        self.TF.cond = float(value)
+        self.TF.cond, self.TF.cond_poly = float(value), None
+
+    def set_fluid_conductivity_poly(self, poly):
+        self.TF.cond, self.TF.cond_poly = None, [float(x) for x in poly]
 
     def set_fluid_capacity(self, value):
-        self.TF.cm = float(value)
+        self.TF.cm, self.TF.cm_poly, self.TF.nasa7 = float(value), None, None
+
+    def set_fluid_capacity_poly(self, poly):
+        self.TF.cm, self.TF.cm_poly, self.TF.nasa7 = None, [float(x) for x in poly], None
+
+    def set_fluid_capacity_NASA7(self, Trange, data):
+        self.TF.cm, self.TF.cm_poly, self.TF.nasa7 = None, None, (list(Trange), [list(r) for r in data])
 
     def set_solid_thermal_diff_derived(self):
         self.TS.derived = True
 
     def set_solid_conductivity(self, value):
-        self.TS.cond = float(value)
+        self.TS.cond, self.TS.cond_poly = float(value), None
+
+    def set_solid_conductivity_poly(self, poly):
+        self.TS.cond, self.TS.cond_poly = None, [float(x) for x in poly]
 
     def set_solid_capacity(self, value):
-        self.TS.cm = float(value)
+        self.TS.cm, self.TS.cm_poly, self.TS.nasa7 = float(value), None, None
+
+    def set_solid_capacity_poly(self, poly):
+        self.TS.cm, self.TS.cm_poly, self.TS.nasa7 = None, [float(x) for x in poly], None
+
+    def set_solid_capacity_NASA7(self, Trange, data):
+        self.TS.cm, self.TS.cm_poly, self.TS.nasa7 = None, None, (list(Trange), [list(r) for r in data])
+
+    def _thermal_props(self, view: ScalarFieldView, solid: bool) -> dict:
+        if (view.cond is None and view.cond_poly is None) or (view.cm is None and view.cm_poly is None
+                                                               and view.nasa7 is None):
+            raise ValueError(f"{view.name}: a derived diffusivity needs set_*_conductivity and set_*_capacity")
+        return thermal_props(cond=view.cond, cond_poly=view.cond_poly, cap=view.cm, cap_poly=view.cm_poly,
+                             nasa7=view.nasa7, solid=solid)
+
+    def _temperature_dependent(self, view: ScalarFieldView) -> bool:
+        return view.derived and (view.cond_poly is not None or view.cm_poly is not None or view.nasa7 is not None)
 
     def _derived_diff(self, view: ScalarFieldView, rho: float) -> float:
-        if view.cond is None or view.cm is None:
-            raise ValueError(f"{view.name}: a derived diffusivity needs set_*_conductivity and set_*_capacity")
-        return view.cond / (rho * view.cm)
+        """The phase's derived diffusivity at its reference temperature (T = 0, i.e. v_ref)
+        and density rho: the constant tauT the descriptor also carries."""
+        tp = self._thermal_props(view, view is self.TS)
+        T = view.v_ref
+        def nested(c):
+            return c[0] + T * (c[1] + T * (c[2] * T + T * (c[3] + T * c[4])))
+        cm = (nested(tp["cap_lo"]) if T < tp["cap_Tmid"] else nested(tp["cap_hi"])) * tp["cap_mul"]
+        return nested(tp["cond"]) / rho / cm
 
     def _solid_density(self) -> float:
         s = self.solid._host >= 1
@@ -477,6 +515,24 @@ class _SolverBase:
             cfg.tauT_fluid = self._tau_T(dF)
             cfg.tauT_solid = self._tau_T(dS)
             cfg.T_ref, cfg.T_scale = self.TF.v_ref, self.TF.v_scale
+            porous = bool(np.any((self.solid._host > 0) & (self.solid._host < 1)))
+            if porous and (self._temperature_dependent(self.TF) or self._temperature_dependent(self.TS)):
+                raise NotImplementedError("temperature-dependent conductivity or capacity with porous cells is not "
+                                          "on the CUDA path (their heat exchange uses constant capacities)")
+            if not porous and (self.TF.derived or self.TS.derived):
+                # per cell at its temperature and (fluid) density, _thermal.py:62-71, :167-174
+                if self.TF.derived:
+                    cfg.tprop_fluid = self._thermal_props(self.TF, False)
+                if self.TS.derived:
+                    cfg.tprop_solid = self._thermal_props(self.TS, True)
+                    cfg.tp_rhos = self._solid_density()
+                cfg.Ts_ref, cfg.Ts_scale = self.TS.v_ref, self.TS.v_scale
+                cfg.tp_dt, cfg.tp_dx2 = self.dt, self.dx ** 2
+                # the constant rates are not used where tprop is set; keep them valid
+                if cfg.tprop_fluid is not None and not cfg.tauT_fluid > 0.5:
+                    cfg.tauT_fluid = 1.0
+                if cfg.tprop_solid is not None and not cfg.tauT_solid > 0.5:
+                    cfg.tauT_solid = 1.0
         if self.viscosity_model == VISCOSITY_MODEL.SUTHERLAND:
             # src/LBM/LBM2D/_evolution.py:232-234 at GetTF (:304-307): the fluid
             # temperature, or 273.15 K without the temperature field
@@ -678,15 +734,10 @@ def _unsupported(name: str, why: str):
     return method
 
 
-_TEMP_DEP = "temperature-dependent properties are not on the CUDA path (one constant diffusivity per phase)"
 _SPECIES = "species transport is not on the CUDA path; use set_pyrolysis()"
 for _n, _why in [
-    ("set_fluid_conductivity_poly", _TEMP_DEP), ("set_fluid_conductivity_mixture", _SPECIES),
-    ("set_fluid_capacity_poly", _TEMP_DEP), ("set_fluid_capacity_NASA7", _TEMP_DEP),
-    ("set_fluid_capacity_mixture", _SPECIES),
-    ("set_solid_conductivity_poly", _TEMP_DEP), ("set_solid_conductivity_mixture", _SPECIES),
-    ("set_solid_capacity_poly", _TEMP_DEP), ("set_solid_capacity_NASA7", _TEMP_DEP),
-    ("set_solid_capacity_mixture", _SPECIES),
+    ("set_fluid_conductivity_mixture", _SPECIES), ("set_fluid_capacity_mixture", _SPECIES),
+    ("set_solid_conductivity_mixture", _SPECIES), ("set_solid_capacity_mixture", _SPECIES),
     ("set_specie_viscosity", _SPECIES), ("set_specie_viscosity_sutherland", _SPECIES),
     ("set_specie_diff", _SPECIES), ("set_specie_diff_Schmidt", _SPECIES), ("set_specie_capacity", _SPECIES),
     ("set_specie_enthalpy", _SPECIES), ("set_specie_NASA7", _SPECIES), ("set_specie_conductivity", _SPECIES),

@@ -109,6 +109,12 @@ typedef struct orc_cfg {
                               * out of the domain, side 1 inlet and the inlets / outlets of
                               * sides 2 and 3 leaving the populations as streamed; 0 the
                               * Zou-He construction on every side */
+    int tprop;               /* bit 0 fluid, bit 1 solid: THERMAL_DIFF_MODEL.DERIVED, the phase's
+                              * diffusivity k(T)/rho/c(T)*dt/dx^2 at the cell's temperature
+                              * (LBM2D/_thermal.py:62-107, :167-210) instead of tauT_fluid/solid */
+    double tp_cond[2][5], tp_cap_lo[2][5], tp_cap_hi[2][5]; /* nested-form coefficients per phase */
+    double tp_cap_Tmid[2], tp_cap_mul[2]; /* NASA7 switch temperature (K), R for a fluid NASA7 */
+    double tp_rhos, tp_dt, tp_dx2;        /* solid density, dt, dx^2 */
 } orc_cfg;
 
 #define ORC_SIGMA 5.670374419e-8   /* Stefan-Boltzmann constant, src/LBM/util/constant.py:20 */
@@ -519,6 +525,28 @@ void orc_init_solid_T(orc* o, const double* Ts) {
 
 /* --------------------------------------------------------------- the step */
 
+/* c0 + T (c1 + T (c2 T + T (c3 + T c4))): conductivity and capacity_m in the reference's
+ * evaluation order (LBM2D/_thermal.py:76-78, :86-101, :179-181, :192-201) */
+static REAL nested5(const double* c, REAL T) {
+    return (REAL)c[0] + T*((REAL)c[1] + T*((REAL)c[2]*T + T*((REAL)c[3] + T*(REAL)c[4])));
+}
+
+/* Relaxation time of a cell's temperature populations: the phase's constant, or with the
+ * phase's bit of tprop TF.tau / TS.tau with the DERIVED coefDiff, cond(T)/rho/cm(T)*dt/dx**2
+ * (LBM2D/_thermal.py:62-71, :167-174; rho the cell's density for the fluid, rhos for the
+ * solid), tau = 3 D + 1/2 in 2D and 4 D + 1/2 in 3D (_scalarField.py:56-58 of LBM2D/LBM3D),
+ * at the temperature the cell's collision uses (T*v_scale + v_ref of its phase) */
+static REAL tau_thermal(const orc* o, long c, int solid) {
+    int ph = solid ? 1 : 0;
+    if (!((o->c.tprop >> ph) & 1)) return solid ? (REAL)o->c.tauT_solid : (REAL)o->c.tauT_fluid;
+    REAL Tp = o->T[c]*(REAL)(ph ? o->c.Ts_scale : o->c.T_scale) + (REAL)(ph ? o->c.Ts_ref : o->c.T_ref);
+    REAL k = nested5(o->c.tp_cond[ph], Tp);
+    REAL cm = (Tp < (REAL)o->c.tp_cap_Tmid[ph] ? nested5(o->c.tp_cap_lo[ph], Tp)
+                                              : nested5(o->c.tp_cap_hi[ph], Tp)) * (REAL)o->c.tp_cap_mul[ph];
+    REAL D = k / (ph ? (REAL)o->c.tp_rhos : o->rho[c]) / cm * (REAL)o->c.tp_dt / (REAL)o->c.tp_dx2;
+    return (REAL)(o->c.dim == 2 ? 3 : 4)*D + (REAL)0.5;
+}
+
 /* collision_source_streaming: src/LBM/LBM2D/_evolution.py:26-115 */
 static void collide_stream(orc* o) {
     int Q = o->Q, QT = o->QT;
@@ -540,7 +568,7 @@ static void collide_stream(orc* o) {
              * LBM2D/_thermal.py:162-166); the source enters as geq(dS) (_evolution.py:54-58).
              * Two fields: TF streams only between fluid cells and TS only between solid
              * cells (_evolution.py:69-95), so a link to the other phase bounces back */
-            REAL tauT = solid ? (REAL)o->c.tauT_solid : (REAL)o->c.tauT_fluid;
+            REAL tauT = tau_thermal(o, c, solid);
             for (int k = 0; k < QT; ++k) {
                 REAL gk = o->g[c*QT + k];
                 REAL ge = solid ? o->wt[k]*o->T[c] : geq_fluid(o, k, o->T[c], &o->u[c*3]);

@@ -44,6 +44,9 @@ class orc_cfg(C.Structure):
         ("Ts_ref", C.c_double), ("Ts_scale", C.c_double), ("cap_fluid", C.c_double), ("cap_solid", C.c_double),
         ("dx_phys", C.c_double), ("radiation", C.c_int), ("T_ambient", C.c_double),
         ("ref_quirk_nebb", C.c_int),
+        ("tprop", C.c_int), ("tp_cond", (C.c_double * 5) * 2), ("tp_cap_lo", (C.c_double * 5) * 2),
+        ("tp_cap_hi", (C.c_double * 5) * 2), ("tp_cap_Tmid", C.c_double * 2), ("tp_cap_mul", C.c_double * 2),
+        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double),
     ]
 
 
@@ -136,6 +139,17 @@ class Oracle:
         c.Ts_scale = cfg.T_scale if cfg.Ts_scale is None else cfg.Ts_scale
         c.cap_fluid, c.cap_solid, c.dx_phys = cfg.cap_fluid, cfg.cap_solid, cfg.dx_phys
         c.radiation, c.T_ambient = int(cfg.radiation), cfg.T_ambient
+        for ph, tp in enumerate((getattr(cfg, "tprop_fluid", None), getattr(cfg, "tprop_solid", None))):
+            if tp is None:
+                continue
+            c.tprop |= 1 << ph
+            for i in range(5):
+                c.tp_cond[ph][i] = float(tp["cond"][i])
+                c.tp_cap_lo[ph][i] = float(tp["cap_lo"][i])
+                c.tp_cap_hi[ph][i] = float(tp["cap_hi"][i])
+            c.tp_cap_Tmid[ph], c.tp_cap_mul[ph] = float(tp["cap_Tmid"]), float(tp["cap_mul"])
+        c.tp_rhos = getattr(cfg, "tp_rhos", 1.0)
+        c.tp_dt, c.tp_dx2 = getattr(cfg, "tp_dt", 1.0), getattr(cfg, "tp_dx2", 1.0)
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):

@@ -47,7 +47,7 @@ ROOT = HERE.parent.parent
 sys.path.insert(0, str(ROOT))
 
 from lbm_porouschem_b200.config import (FIXED_VALUE, PERIODIC, ZERO_GRADIENT,  # noqa: E402
-                                        LatticeConfig, SideBC)
+                                        LatticeConfig, SideBC, thermal_props)
 
 
 def _import_reference(ref_root: str):
@@ -334,10 +334,39 @@ def case_nebb_quirks2d():
                                            2: ("inlet", (0.0, 0.01, 0.0)), 3: ("outlet", 1.0)}, 151, 40, True)
 
 
+# temperature-dependent properties (THERMAL_DIFF_MODEL.DERIVED): coefficients of the
+# reference's nested polynomials, c0 + c1 T + (c2 + c3) T^3 + c4 T^4, chosen so that the
+# lattice diffusivities stay between 0.03 and 0.1 over 300-800 K, with the NASA7 switch
+# at 550 K inside the range the channel reaches
+TP_FLUID = dict(cond_poly=[0.2, 4e-4, 2e-10, 1e-10, -1e-13],
+                nasa7=([200.0, 550.0, 3500.0], [[1.0, 4e-4, 1e-10, -5e-11, 2e-14, 0.0, 0.0],
+                                                [1.2, 2e-4, 5e-11, 0.0, 0.0, 0.0, 0.0]]))
+TP_SOLID = dict(cond_poly=[1.0, 1e-3, 1e-9, 1e-9], cap_poly=[2.0, 5e-3, 1e-10, 0.0, 0.0])
+TP_RHOS = 5.0
+
+
+def _tprop_case(base, name, steps):
+    d = base()
+    d["cfg"] = d["cfg"].replace(
+        T_ref=300.0, T_scale=500.0, Ts_ref=300.0, Ts_scale=500.0, tp_rhos=TP_RHOS, tp_dt=1.0, tp_dx2=1.0,
+        tprop_fluid=thermal_props(cond_poly=TP_FLUID["cond_poly"], nasa7=TP_FLUID["nasa7"]),
+        tprop_solid=thermal_props(cond_poly=TP_SOLID["cond_poly"], cap_poly=TP_SOLID["cap_poly"], solid=True))
+    d.update(name=name, steps=steps, tprop=(TP_FLUID, TP_SOLID, TP_RHOS))
+    return d
+
+
+def case_tprop2d():
+    return _tprop_case(case_channel2d_thermal, "ref_tprop2d", 60)
+
+
+def case_tprop3d():
+    return _tprop_case(case_channel3d_thermal, "ref_tprop3d", 20)
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
          case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32,
          case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df, case_porous2d_heat, case_porous3d_heat,
-         case_nebb_channel2d, case_nebb_quirks2d]
+         case_nebb_channel2d, case_nebb_quirks2d, case_tprop2d, case_tprop3d]
 
 
 # --------------------------------------------------------------------------- driver
@@ -398,6 +427,18 @@ def run_reference(case, Solver2D, Solver3D, flag):
         lb.set_solid_thermal_diff(Ds)
         lb.init_field(lb.TF.S, case["T"].copy())
         lb.init_field(lb.TS.S, (case["T"] if heat is None else heat["Ts0"]).copy())
+    if "tprop" in case:
+        # src/LBM/app.py:143-175 with thermalDiff "derived" and polynomial / NASA7 properties
+        fl, so, rhos = case["tprop"]
+        lb.set_fluid_Trange([cfg.T_ref, cfg.T_ref + cfg.T_scale])
+        lb.set_solid_Trange([cfg.Ts_ref, cfg.Ts_ref + cfg.Ts_scale])
+        lb.set_fluid_thermal_diff_derived()
+        lb.set_fluid_conductivity_poly(list(fl["cond_poly"]))
+        lb.set_fluid_capacity_NASA7(*fl["nasa7"])
+        lb.set_solid_thermal_diff_derived()
+        lb.set_solid_conductivity_poly(list(so["cond_poly"]))
+        lb.set_solid_capacity_poly(list(so["cap_poly"]))
+        lb.add_rho_solid(case["solid"].astype(np.float64) * rhos)
     if heat is not None:
         # app.py:537-566 for a porous zone: rhos, exchange surface and coefficient over it,
         # radiation surface and emissivity on its border; TS range and capacities

@@ -9,7 +9,7 @@ from pathlib import Path
 import pytest
 
 from lbm_porouschem_b200 import _native as N
-from lbm_porouschem_b200.config import LatticeConfig, SideBC
+from lbm_porouschem_b200.config import LatticeConfig, SideBC, thermal_props
 
 ROOT = Path(__file__).resolve().parents[1]
 HEADER = ROOT / "include" / "lbm_b200.h"
@@ -68,9 +68,15 @@ def test_required_bytes(lib):
     assert nb.value == 2 * 19 * n * 2
 
 
+_TP = thermal_props(cond=0.5, cap=10.0)
+
+
 @pytest.mark.parametrize("bad", [
     dict(dim=4), dict(nx=2), dict(nz=5), dict(thermal="none", pyro=True), dict(nu=0.0),
     dict(tauT_fluid=0.4, thermal="conjugate"),
+    dict(tprop_fluid=_TP), dict(tprop_solid=_TP, thermal="conjugate", tp_rhos=0.0),
+    dict(tprop_fluid=_TP, thermal="two_field", porous="darcy"), dict(tprop_fluid=_TP, thermal="conjugate", tp_dt=0.0),
+    dict(tprop_fluid={**_TP, "cap_mul": 0.0}, thermal="conjugate"),
 ])
 def test_descriptor_validation(lib, bad):
     kw = dict(dim=2, nx=16, ny=8, nz=1)

@@ -214,7 +214,7 @@ def test_cli_runs_case(tmp_path, monkeypatch):
 
 def test_derived_thermal_properties_from_yaml():
     """thermalDiff type derived with constant conductivity and capacity (src/LBM/app.py:132-175);
-    polynomial properties stop the run."""
+    a polynomial capacity becomes the fluid's per-cell property set, a mixture stops the run."""
     cfg = yaml.safe_load(CASE2D)
     cfg["thermalPropertiesFluid"]["thermalDiff"] = {"type": "derived"}
     cfg["thermalPropertiesFluid"]["conductivity"] = {"type": "constant", "value": 0.03}
@@ -222,5 +222,9 @@ def test_derived_thermal_properties_from_yaml():
     lb = build_case(cfg, _log())
     assert lb.TF.derived and lb.TF.cond == 0.03 and lb.TF.cm == 1000.0
     cfg["thermalPropertiesFluid"]["capacity"] = {"type": "polynomial", "data": [1000, 0, 0, 0, 0]}
-    with pytest.raises(NotImplementedError, match="capacity_poly"):
+    lb = build_case(cfg, _log())
+    assert lb.TF.cm is None and lb.TF.cm_poly == [1000, 0, 0, 0, 0]
+    assert lb._config().tprop_fluid["cap_lo"] == [1000.0, 0.0, 0.0, 0.0, 0.0]
+    cfg["thermalPropertiesFluid"]["capacity"] = {"type": "mixture"}
+    with pytest.raises(NotImplementedError, match="capacity_mixture"):
         build_case(cfg, _log())

@@ -122,3 +122,21 @@ def test_frozen_solid_quirk_matters(oracle_mod):
     s = z["solid"]
     assert rel(T[~s], z["T_ref"][~s]) <= TOL
     assert rel(T[s], z["T_ref"][s]) > 1e-3
+
+
+@pytest.mark.parametrize("name", ["ref_tprop2d", "ref_tprop3d"])
+def test_temperature_dependent_properties_matter(oracle_mod, name):
+    """The derived fluid diffusivity matters: with the constant relaxation times the case also
+    carries, the fluid temperatures differ from the reference's.  The solid's properties
+    leave no trace in these outputs: the reference's pure-solid cells keep their initial
+    temperature and equilibrium populations w T (macro skips them), whatever their relaxation
+    time, so only the kernels' evolving solid (against this oracle) exercises that path."""
+    z, meta, cfg = load_case(name)
+    fl = ~z["solid"]
+    errs = []
+    for c in (cfg.replace(tprop_fluid=None, tprop_solid=None), cfg.replace(tprop_solid=None)):
+        o = oracle_mod.Oracle(c, real="f64", ref_quirk_frozen_solid_T=True)
+        o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+        o.step(meta["steps"])
+        errs.append(rel(o.fields()["T"][fl], z["T_ref"][fl]))
+    assert errs[0] > 1e-3 and errs[1] <= TOL, errs

@@ -212,10 +212,10 @@ def test_reference_surface_is_complete():
     """Every method and attribute the reference's driver touches exists (src/LBM/app.py:
     101-677); those outside the CUDA path raise NotImplementedError naming themselves."""
     s = LBM3DSolver(X=8, Y=8, Z=8, dx=1, isThermal=True)
-    for n in ("set_fluid_conductivity_poly", "set_fluid_capacity_NASA7", "set_solid_capacity_mixture",
+    for n in ("set_fluid_conductivity_mixture", "set_solid_capacity_mixture",
               "set_specie_diff", "set_specie_BC", "set_species_BC", "init_specie", "set_radiation"):
         with pytest.raises(NotImplementedError, match=n if n != "set_radiation" else "radiation"):
-            getattr(s, n)(*([None] * (2 if n in ("set_radiation", "set_fluid_capacity_NASA7") else 1)))
+            getattr(s, n)(*([None] * (2 if n == "set_radiation" else 1)))
     assert s.specieName == [] and s.TS.radiation_surface is not None and s.TS.emissivity is not None
 
 
@@ -240,4 +240,50 @@ def test_derived_thermal_diffusivity():
     assert cfg.tauT_solid == pytest.approx(3 * (0.5 / (500.0 * 1500.0)) * lu + 0.5)
     s.add_rho_solid(solid * np.linspace(0, 1, 16)[:, None, None])     # no longer uniform
     with pytest.raises(NotImplementedError, match="solid density"):
+        s._config()
+
+
+def test_temperature_dependent_properties_map_to_tprop():
+    """Polynomial conductivity and NASA7 / polynomial capacity under the derived model
+    (src/LBM/LBM2D/_io.py:182-251) become the descriptor's per-cell property sets, in the
+    reference's nested coefficient form; a later constant setter replaces the model."""
+    from lbm_porouschem_b200.config import GAS_CONSTANT
+    s = LBM2DSolver(X=0.016, Y=0.008, Z=0, dx=1e-3, dt=1e-4, isThermal=True)
+    s.set_viscosity(2e-5)
+    solid = np.zeros((16, 8, 1))
+    solid[6:10, 2:6] = 1.0
+    s.add_solid(solid)
+    s.add_rho_solid(solid * 500.0)
+    s.set_fluid_Trange([300.0, 800.0])
+    s.set_fluid_thermal_diff_derived()
+    s.set_fluid_conductivity_poly([0.02, 1e-4, 0, 0, 0])
+    s.set_fluid_capacity_NASA7([200.0, 1000.0, 3500.0], [[3.5, 1e-4, 0, 0, 0, 0, 0], [3.0, 2e-4, 0, 0, 0, 0, 0]])
+    s.set_solid_thermal_diff_derived()
+    s.set_solid_conductivity_poly([0.5, 1e-3, 0, 2e-9, 7.0])
+    s.set_solid_capacity_poly([1500.0, 0.1, 0, 0, 0])
+    cfg = s._config()
+    f, so = cfg.tprop_fluid, cfg.tprop_solid
+    assert f["cond"] == [0.02, 1e-4, 0.0, 0.0, 0.0] and f["cap_Tmid"] == 1000.0 and f["cap_mul"] == GAS_CONSTANT
+    assert f["cap_lo"][0] == 3.5 and f["cap_hi"][0] == 3.0
+    assert so["cond"] == [0.5, 1e-3, 0.0, 2e-9, 0.0]      # the solid's conductivity uses four coefficients
+    assert so["cap_lo"] == so["cap_hi"] == [1500.0, 0.1, 0.0, 0.0, 0.0] and so["cap_mul"] == 1.0
+    assert cfg.tp_rhos == 500.0 and cfg.tp_dt == 1e-4 and cfg.tp_dx2 == pytest.approx(1e-6)
+    d = cfg.to_desc()
+    assert d.tprop == 3 and d.tp_cap_mul[0] == GAS_CONSTANT and d.tp_cond[1][3] == 2e-9
+    s.set_fluid_capacity(1000.0)
+    assert s._config().tprop_fluid["cap_lo"] == [1000.0, 0.0, 0.0, 0.0, 0.0]
+    s.set_fluid_thermal_diff(3e-5)           # back to the constant model: no per-cell fluid rate
+    assert s._config().tprop_fluid is None
+
+
+def test_temperature_dependent_properties_refused_with_porous_cells():
+    s = LBM2DSolver(X=0.016, Y=0.008, Z=0, dx=1e-3, dt=1e-4, isThermal=True, isPoro=True)
+    s.set_viscosity(2e-5)
+    frac = np.zeros((16, 8, 1))
+    frac[6:10, 2:6] = 0.5
+    s.add_solid(frac)
+    s.set_fluid_thermal_diff_derived()
+    s.set_fluid_conductivity_poly([0.02, 1e-4, 0, 0, 0])
+    s.set_fluid_capacity(1000.0)
+    with pytest.raises(NotImplementedError, match="porous"):
         s._config()
