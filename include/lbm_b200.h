@@ -182,13 +182,17 @@ typedef struct lbm_desc {
    * c0 + T (c1 + T (c2 T + T (c3 + T c4))) (a constant is {c0, 0, 0, 0, 0}; the solid
    * conductivity takes c4 = 0); c uses tp_cap_lo below tp_cap_Tmid and tp_cap_hi from it on
    * (NASA7 ranges; equal arrays for one polynomial), times tp_cap_mul (the gas constant for
-   * a fluid NASA7 capacity, else 1).  Temperature fields THERMAL_CONJUGATE / TWO_FIELD
-   * only, without porous cells. */
+   * a fluid NASA7 capacity, else 1).  Bit 2 instead of bit 0 selects the fluid's
+   * THERMAL_DIFF_MODEL.PRANDTL: D = kinetic_viscosity / tp_prandtl, the cell's lattice
+   * viscosity (constant or Sutherland) divided by its density under LBM_EOS_IDEAL_GAS
+   * (src/LBM/LBM2D/_thermal.py:62-71, _evolution.py:227-246).  Temperature fields
+   * THERMAL_CONJUGATE / TWO_FIELD only, without porous cells. */
   int32_t tprop;
   double tp_cond[2][5], tp_cap_lo[2][5], tp_cap_hi[2][5];
   double tp_cap_Tmid[2], tp_cap_mul[2];
   double tp_rhos;         /* solid density of the derived solid diffusivity (uniform) */
   double tp_dt, tp_dx2;   /* dt and dx^2 of the physical units */
+  double tp_prandtl;      /* tprop bit 2: the fluid's Prandtl number */
 } lbm_desc;
 
 /* Diagnostics (FP64 accumulation).  No reference counterpart except umax,

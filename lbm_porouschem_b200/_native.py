@@ -82,7 +82,7 @@ class lbm_desc(C.Structure):
         ("dx_phys", C.c_double), ("T_ambient", C.c_double), ("radiation", C.c_int32), ("fp16_rounding", C.c_int32),
         ("tprop", C.c_int32), ("tp_cond", (C.c_double * 5) * 2), ("tp_cap_lo", (C.c_double * 5) * 2),
         ("tp_cap_hi", (C.c_double * 5) * 2), ("tp_cap_Tmid", C.c_double * 2), ("tp_cap_mul", C.c_double * 2),
-        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double),
+        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double), ("tp_prandtl", C.c_double),
     ]
 
 

@@ -126,6 +126,9 @@ class LatticeConfig:
     tp_rhos: float = 1.0
     tp_dt: float = 1.0
     tp_dx2: float = 1.0
+    # > 0: the fluid's PRANDTL diffusivity, the cell's kinetic viscosity / tp_prandtl
+    # (instead of tprop_fluid and tauT_fluid)
+    tp_prandtl: float = 0.0
 
     @property
     def shape(self) -> tuple:
@@ -218,6 +221,11 @@ class LatticeConfig:
                 d.tp_cap_hi[ph][i] = float(tp["cap_hi"][i])
             d.tp_cap_Tmid[ph], d.tp_cap_mul[ph] = float(tp["cap_Tmid"]), float(tp["cap_mul"])
         d.tp_rhos, d.tp_dt, d.tp_dx2 = self.tp_rhos, self.tp_dt, self.tp_dx2
+        if self.tp_prandtl > 0:
+            if self.tprop_fluid is not None:
+                raise ValueError("tp_prandtl and tprop_fluid both set the fluid's diffusivity")
+            d.tprop |= 4
+            d.tp_prandtl = self.tp_prandtl
         return d
 
     @property

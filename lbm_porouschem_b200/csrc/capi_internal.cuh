@@ -334,6 +334,7 @@ StepParams<S> make_params(lbm_handle* h, int buf) {
   p.tp_Tsc[1] = (C)d.Ts_scale; p.tp_Tref[1] = (C)d.Ts_ref;
   p.tp_rhos = (C)d.tp_rhos; p.tp_dt = (C)d.tp_dt; p.tp_dx2 = (C)d.tp_dx2;
   p.tp_lat = (C)(d.dim == 2 ? 3 : 4);
+  p.tp_prandtl = (C)d.tp_prandtl;
   p.poro = (const C*)h->ptr[LBM_FIELD_PORO];
   p.darcy = (const C*)h->ptr[LBM_FIELD_DARCY];
   p.forch = (const C*)h->ptr[LBM_FIELD_FORCH];

@@ -67,9 +67,11 @@ static int validate(const lbm_desc* d) {
   if (d->fp16_rounding != LBM_FP16_STOCHASTIC && d->fp16_rounding != LBM_FP16_NEAREST)
     return fail(LBM_ERR_ARG, "fp16_rounding must be LBM_FP16_STOCHASTIC or LBM_FP16_NEAREST");
   if (d->tprop) {
-    if ((d->tprop & ~3) || d->thermal == LBM_THERMAL_NONE || d->porous)
-      return fail(LBM_ERR_ARG, "temperature-dependent thermal properties (tprop bits 0, 1) need the conjugate or "
+    if ((d->tprop & ~7) || d->thermal == LBM_THERMAL_NONE || d->porous)
+      return fail(LBM_ERR_ARG, "temperature-dependent thermal properties (tprop bits 0-2) need the conjugate or "
                                "two-field temperature, without porous cells");
+    if ((d->tprop & 4) && ((d->tprop & 1) || !(d->tp_prandtl > 0)))
+      return fail(LBM_ERR_ARG, "the fluid's Prandtl diffusivity (tprop bit 2) excludes bit 0 and needs tp_prandtl > 0");
     if (!(d->tp_dt > 0 && d->tp_dx2 > 0) || ((d->tprop & 2) && !(d->tp_rhos > 0)))
       return fail(LBM_ERR_ARG, "tprop needs tp_dt > 0, tp_dx2 > 0 and, for the solid, tp_rhos > 0");
     for (int ph = 0; ph < 2; ++ph) {

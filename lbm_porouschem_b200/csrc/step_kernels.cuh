@@ -164,7 +164,7 @@ struct StepParams {
   C suthA, suthTs;
   int tprop;
   C tp_cond[2][5], tp_lo[2][5], tp_hi[2][5], tp_Tmid[2], tp_mul[2], tp_Tsc[2], tp_Tref[2];
-  C tp_rhos, tp_dt, tp_dx2, tp_lat;
+  C tp_rhos, tp_dt, tp_dx2, tp_lat, tp_prandtl;
   const C* poro;   // porous cells (collision codes kCollPorous + BGK/MRT): solid fraction,
   const C* darcy;  //   Darcy and Forchheimer coefficients per cell, and the model
   const C* forch;  //   (LBM_PORO_*)
@@ -632,6 +632,16 @@ struct Kern {
   template <int COLL>
   __device__ __forceinline__ static C itau_thermal(const P& p, bool fluid, C T, C rho) {
     if constexpr (coll_sutherland(COLL)) {
+      if (fluid && ((p.tprop >> 2) & 1)) {
+        // PRANDTL: kinetic_viscosity / Pr, src/LBM/LBM2D/_thermal.py:66-67, _evolution.py:227-246
+        C nu = p.nu;
+        if (p.suth) {
+          const C TK = T * p.Tscale + p.Tref;
+          nu = p.suthA * TK * sqrt(TK) / (TK + p.suthTs);
+        }
+        if (p.eos == 0) nu = nu / rho;
+        return (C)1 / (p.tp_lat * (nu / p.tp_prandtl) + (C)0.5);
+      }
       const int ph = fluid ? 0 : 1;
       if ((p.tprop >> ph) & 1) {
         const C Tp = T * p.tp_Tsc[ph] + p.tp_Tref[ph];

@@ -91,6 +91,7 @@ class ScalarFieldView:
         # THERMAL_DIFF_MODEL.DERIVED (src/LBM/LBM2D/_thermal.py:62-107): D = cond / (rho cm),
         # conductivity constant or polynomial, capacity constant, polynomial or NASA7
         self.derived = False
+        self.Pr: Optional[float] = None         # THERMAL_DIFF_MODEL.PRANDTL (fluid)
         self.cond: Optional[float] = None
         self.cond_poly: Optional[list] = None
         self.cm: Optional[float] = None
@@ -242,13 +243,15 @@ class _SolverBase:
 
     # each diffusivity setter selects its model (src/LBM/LBM2D/_io.py:174-184, :218-224)
     def set_fluid_thermal_diff(self, diff):
-        self.TF.thermal_diff, self.TF.derived = diff, False
+        self.TF.thermal_diff, self.TF.derived, self.TF.Pr = diff, False, None
 
     def set_solid_thermal_diff(self, diff):
         self.TS.thermal_diff, self.TS.derived = diff, False
 
+    # D = kinetic_viscosity(i) / Pr per cell (the cell's viscosity, constant or Sutherland,
+    # over its density for an ideal gas); thermal_diff keeps the value at rho = 1
     def set_fluid_Prandtl(self, Pr):
-        self.TF.thermal_diff, self.TF.derived = self.visco / Pr, False
+        self.TF.thermal_diff, self.TF.derived, self.TF.Pr = self.visco / Pr, False, float(Pr)
 
     # derived diffusivity D = cond(T) / (rho cm(T)) (src/LBM/LBM2D/_io.py:182-251,
     # _thermal.py:62-107, :167-210), evaluated per cell at its temperature by the kernels
@@ -256,7 +259,7 @@ class _SolverBase:
     # density from add_rho_solid (uniform over the solid cells).  Each setter replaces the
     # phase's previous conductivity or capacity model, as the reference's do.
     def set_fluid_thermal_diff_derived(self):
-        self.TF.derived = True
+        self.TF.derived, self.TF.Pr = True, None
 
     def set_fluid_conductivity(self, value):
         self.TF.cond, self.TF.cond_poly = float(value), None
@@ -519,6 +522,8 @@ class _SolverBase:
             if porous and (self._temperature_dependent(self.TF) or self._temperature_dependent(self.TS)):
                 raise NotImplementedError("temperature-dependent conductivity or capacity with porous cells is not "
                                           "on the CUDA path (their heat exchange uses constant capacities)")
+            if not porous and self.TF.Pr is not None:
+                cfg.tp_prandtl = self.TF.Pr
             if not porous and (self.TF.derived or self.TS.derived):
                 # per cell at its temperature and (fluid) density, _thermal.py:62-71, :167-174
                 if self.TF.derived:

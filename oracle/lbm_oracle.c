@@ -115,6 +115,8 @@ typedef struct orc_cfg {
     double tp_cond[2][5], tp_cap_lo[2][5], tp_cap_hi[2][5]; /* nested-form coefficients per phase */
     double tp_cap_Tmid[2], tp_cap_mul[2]; /* NASA7 switch temperature (K), R for a fluid NASA7 */
     double tp_rhos, tp_dt, tp_dx2;        /* solid density, dt, dx^2 */
+    double tp_prandtl;       /* tprop bit 2: the fluid's THERMAL_DIFF_MODEL.PRANDTL,
+                              * D = kinetic_viscosity(i)/Pr (LBM2D/_thermal.py:66-67) */
 } orc_cfg;
 
 #define ORC_SIGMA 5.670374419e-8   /* Stefan-Boltzmann constant, src/LBM/util/constant.py:20 */
@@ -538,6 +540,8 @@ static REAL nested5(const double* c, REAL T) {
  * at the temperature the cell's collision uses (T*v_scale + v_ref of its phase) */
 static REAL tau_thermal(const orc* o, long c, int solid) {
     int ph = solid ? 1 : 0;
+    if (!solid && (o->c.tprop & 4))
+        return (REAL)(o->c.dim == 2 ? 3 : 4)*(visc_kin(o, o->rho[c], o->T[c])/(REAL)o->c.tp_prandtl) + (REAL)0.5;
     if (!((o->c.tprop >> ph) & 1)) return solid ? (REAL)o->c.tauT_solid : (REAL)o->c.tauT_fluid;
     REAL Tp = o->T[c]*(REAL)(ph ? o->c.Ts_scale : o->c.T_scale) + (REAL)(ph ? o->c.Ts_ref : o->c.T_ref);
     REAL k = nested5(o->c.tp_cond[ph], Tp);

@@ -46,7 +46,7 @@ class orc_cfg(C.Structure):
         ("ref_quirk_nebb", C.c_int),
         ("tprop", C.c_int), ("tp_cond", (C.c_double * 5) * 2), ("tp_cap_lo", (C.c_double * 5) * 2),
         ("tp_cap_hi", (C.c_double * 5) * 2), ("tp_cap_Tmid", C.c_double * 2), ("tp_cap_mul", C.c_double * 2),
-        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double),
+        ("tp_rhos", C.c_double), ("tp_dt", C.c_double), ("tp_dx2", C.c_double), ("tp_prandtl", C.c_double),
     ]
 
 
@@ -150,6 +150,9 @@ class Oracle:
             c.tp_cap_Tmid[ph], c.tp_cap_mul[ph] = float(tp["cap_Tmid"]), float(tp["cap_mul"])
         c.tp_rhos = getattr(cfg, "tp_rhos", 1.0)
         c.tp_dt, c.tp_dx2 = getattr(cfg, "tp_dt", 1.0), getattr(cfg, "tp_dx2", 1.0)
+        if getattr(cfg, "tp_prandtl", 0.0) > 0:
+            c.tprop |= 4
+            c.tp_prandtl = cfg.tp_prandtl
         for r, v in enumerate(cfg.mrt_s()):
             c.mrt_s[r] = v
         for i, s in enumerate(cfg.sides):

@@ -363,10 +363,21 @@ def case_tprop3d():
     return _tprop_case(case_channel3d_thermal, "ref_tprop3d", 20)
 
 
+def case_prandtl2d():
+    """THERMAL_DIFF_MODEL.PRANDTL with the Sutherland viscosity: the fluid's diffusivity is
+    the cell's kinetic viscosity over Pr, both following its temperature and density."""
+    d = case_channel2d_thermal()
+    As, Ts, Pr = 0.008, 110.0, 0.71          # nu 0.10-0.20 over 300-800 K (dt = dx = 1)
+    d["cfg"] = d["cfg"].replace(T_ref=300.0, T_scale=500.0, viscosity="sutherland", suth_A=As, suth_Ts=Ts,
+                                tp_prandtl=Pr)
+    d.update(name="ref_prandtl2d", steps=60, sutherland=(As, Ts), prandtl=Pr)
+    return d
+
+
 CASES = [case_periodic2d, case_channel2d_thermal, case_channel2d_es, case_nee_periodic2d,
          case_periodic3d, case_channel3d_thermal, case_periodic3d_x32, case_channel3d_flow_x32,
          case_porous2d_darcy, case_porous2d_ergun, case_porous3d_df, case_porous2d_heat, case_porous3d_heat,
-         case_nebb_channel2d, case_nebb_quirks2d, case_tprop2d, case_tprop3d]
+         case_nebb_channel2d, case_nebb_quirks2d, case_tprop2d, case_tprop3d, case_prandtl2d]
 
 
 # --------------------------------------------------------------------------- driver
@@ -427,6 +438,12 @@ def run_reference(case, Solver2D, Solver3D, flag):
         lb.set_solid_thermal_diff(Ds)
         lb.init_field(lb.TF.S, case["T"].copy())
         lb.init_field(lb.TS.S, (case["T"] if heat is None else heat["Ts0"]).copy())
+    if "sutherland" in case:
+        # src/LBM/LBM2D/_io.py:144-147; GetTF needs the fluid's temperature range
+        lb.set_fluid_Trange([cfg.T_ref, cfg.T_ref + cfg.T_scale])
+        lb.set_viscosity_sutherland(*case["sutherland"])
+    if "prandtl" in case:
+        lb.set_fluid_Prandtl(case["prandtl"])
     if "tprop" in case:
         # src/LBM/app.py:143-175 with thermalDiff "derived" and polynomial / NASA7 properties
         fl, so, rhos = case["tprop"]

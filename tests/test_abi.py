@@ -76,7 +76,7 @@ _TP = thermal_props(cond=0.5, cap=10.0)
     dict(tauT_fluid=0.4, thermal="conjugate"),
     dict(tprop_fluid=_TP), dict(tprop_solid=_TP, thermal="conjugate", tp_rhos=0.0),
     dict(tprop_fluid=_TP, thermal="two_field", porous="darcy"), dict(tprop_fluid=_TP, thermal="conjugate", tp_dt=0.0),
-    dict(tprop_fluid={**_TP, "cap_mul": 0.0}, thermal="conjugate"),
+    dict(tprop_fluid={**_TP, "cap_mul": 0.0}, thermal="conjugate"), dict(tp_prandtl=0.7),
 ])
 def test_descriptor_validation(lib, bad):
     kw = dict(dim=2, nx=16, ny=8, nz=1)

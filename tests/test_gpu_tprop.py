@@ -156,3 +156,20 @@ def test_tprop_batch_equals_single_lattices():
     batch.close()
     for lat in lats:
         lat.close()
+
+
+@pytest.mark.parametrize("dim,thermal,suth,form", [(2, "conjugate", True, "list"), (2, "two_field", False, "tile"),
+                                                   (3, "conjugate", True, "dense"), (3, "two_field", True, "list")])
+def test_prandtl_fp64(oracle_mod, dim, thermal, suth, form):
+    """THERMAL_DIFF_MODEL.PRANDTL: the fluid's diffusivity is the cell's kinetic viscosity
+    (constant or Sutherland, over its density) / Pr; FP64 vs the FP64 oracle, 1e-10."""
+    c = _case(dim, "mrt", thermal, suth=suth, shape=(32, 16, 12) if form == "dense" else None)
+    c.cfg = c.cfg.replace(tprop_fluid=None, tp_prandtl=0.71)
+    if thermal == "two_field":
+        c.init["T"] = np.where(c.solid, 0.6, 0.2)
+    n = 150 if dim == 2 else 60
+    g, r = _gpu(c, n, cfg=c.cfg.replace(bulk_form=form)), _oracle(oracle_mod, c, n, "f64")
+    fl = ~r["solid"]
+    assert _rel(g["rho"], r["rho"], fl) < 1e-10
+    assert _rel(g["u"], r["u"], fl) < 1e-10
+    assert _rel(g["T"], r["T"]) < 1e-10

@@ -140,3 +140,20 @@ def test_temperature_dependent_properties_matter(oracle_mod, name):
         o.step(meta["steps"])
         errs.append(rel(o.fields()["T"][fl], z["T_ref"][fl]))
     assert errs[0] > 1e-3 and errs[1] <= TOL, errs
+
+
+def test_prandtl_and_sutherland_matter(oracle_mod):
+    """The Prandtl case's fluid temperature depends on the per-cell diffusivity
+    kinetic_viscosity / Pr and its velocity on the Sutherland viscosity: replacing either by
+    its constant counterpart moves the result away from the reference's."""
+    z, meta, cfg = load_case("ref_prandtl2d")
+    fl = ~z["solid"]
+    for c, key, bound in ((cfg.replace(tp_prandtl=0.0), "T", 1e-4),
+                          (cfg.replace(viscosity="constant"), "u", 1e-3)):
+        o = oracle_mod.Oracle(c, real="f64", ref_quirk_frozen_solid_T=True)
+        o.init(z["solid"], None, rho=z["rho0"], u=z["u0"], T=z["T0"])
+        o.step(meta["steps"])
+        r = o.fields()
+        got = r[key][..., fl] if key == "u" else r[key][fl]
+        ref = z[key + "_ref"][..., fl] if key == "u" else z[key + "_ref"][fl]
+        assert rel(got, ref) > bound, (key, rel(got, ref))
