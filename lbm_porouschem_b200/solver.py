@@ -312,7 +312,7 @@ class _SolverBase:
         def nested(c):
             return c[0] + T * (c[1] + T * (c[2] * T + T * (c[3] + T * c[4])))
         cm = (nested(tp["cap_lo"]) if T < tp["cap_Tmid"] else nested(tp["cap_hi"])) * tp["cap_mul"]
-        return nested(tp["cond"]) / rho / cm
+        return nested(tp["cond"]) / rho / cm if cm != 0 else 0.0
 
     def _solid_density(self) -> float:
         s = self.solid._host >= 1

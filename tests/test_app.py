@@ -212,6 +212,36 @@ def test_cli_runs_case(tmp_path, monkeypatch):
     assert d["velocity"].shape == (d["rho"].size, 3)
 
 
+@pytest.mark.gpu
+def test_cli_runs_temperature_dependent_properties(tmp_path, monkeypatch):
+    """thermalDiff derived with a polynomial conductivity and a NASA7 capacity (the form of
+    the reference's examples/2D/pyrolysis/config.yaml), and the Prandtl model: the YAML run
+    reaches the kernels' per-cell rates and the two give different temperatures."""
+    from lbm_porouschem_b200.cli import run
+    from lbm_porouschem_b200.vtk import read_pvd, read_vts
+    out = {}
+    for mode in ("derived", "prandtl"):
+        cfg = yaml.safe_load(CASE2D)
+        tf = cfg["thermalPropertiesFluid"]
+        if mode == "derived":
+            tf["thermalDiff"] = {"type": "derived"}
+            tf["conductivity"] = {"type": "polynomial", "data": [0.01, 5e-5, 0, 0, 0]}
+            tf["capacity"] = {"type": "NASA7", "Trange": [200, 1000, 3500],
+                              "data": [[3.5, 1e-4, 0, 0, 0, 0, 0], [3.6, 5e-5, 0, 0, 0, 0, 0]]}
+        else:
+            tf["thermalDiff"] = {"type": "Prandtl", "Pr": 0.71}
+        cfg["basic"]["name"] = mode
+        cfg["outputControl"]["vtk"] = {"interval": 2.0e-3, "path": str(tmp_path / mode)}
+        p = tmp_path / f"{mode}.yaml"
+        p.write_text(yaml.safe_dump(cfg))
+        monkeypatch.chdir(tmp_path)
+        assert run(["-c", str(p), "-v", "0"]) == 0
+        series = read_pvd(str(next((tmp_path / mode).glob("*.pvd"))))
+        out[mode] = read_vts(str(tmp_path / mode / series[-1][1]))
+        assert np.isfinite(out[mode]["Tf"]).all() and out[mode]["Tf"].max() > 300.0
+    assert not np.allclose(out["derived"]["Tf"], out["prandtl"]["Tf"])
+
+
 def test_derived_thermal_properties_from_yaml():
     """thermalDiff type derived with constant conductivity and capacity (src/LBM/app.py:132-175);
     a polynomial capacity becomes the fluid's per-cell property set, a mixture stops the run."""

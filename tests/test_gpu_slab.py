@@ -103,3 +103,27 @@ def test_porous_heat_slabs_equal_the_whole_lattice():
     s.close()
     for k in ("rho", "u", "T", "Ts"):
         assert np.array_equal(got[k], ref[k]), k
+
+
+@pytest.mark.parametrize("mode", ["derived", "prandtl"])
+def test_temperature_dependent_slabs_equal_the_whole_lattice(mode):
+    """Per-cell thermal diffusivities (derived from polynomial / NASA7 properties of both
+    phases, or the fluid's Prandtl model over the Sutherland viscosity) through pyrolysis flips:
+    the rates depend on the cell's own state only, so the slabs stay bit for bit equal."""
+    from lbm_porouschem_b200.config import thermal_props
+    cfg, solid, reactive, init = _pyro("fp32")
+    if mode == "derived":
+        cfg = cfg.replace(
+            Ts_ref=cfg.T_ref, Ts_scale=cfg.T_scale, tp_rhos=5.0,
+            tprop_fluid=thermal_props(cond_poly=[0.2, 4e-4, 2e-10, 1e-10, -1e-13],
+                                      nasa7=([200.0, 550.0, 3500.0], [[1.0, 4e-4, 1e-10, -5e-11, 2e-14, 0, 0],
+                                                                      [1.2, 2e-4, 5e-11, 0, 0, 0, 0]])),
+            tprop_solid=thermal_props(cond_poly=[1.0, 1e-3, 1e-9, 1e-9], cap_poly=[2.0, 5e-3, 1e-10, 0, 0],
+                                      solid=True))
+    else:
+        cfg = cfg.replace(viscosity="sutherland", suth_A=0.005, suth_Ts=170.0, tp_prandtl=0.71)
+    ref = _whole(cfg, solid, reactive, init, 60)
+    got = _slabs(cfg, solid, reactive, init, 60, 2)
+    assert (solid & ~ref["solid"]).sum() >= 3
+    for k in KEYS:
+        assert np.array_equal(got[k], ref[k]), k
