@@ -4,7 +4,8 @@ Sections read: ``basic`` (dimension, name; ``arch`` is ignored, the lattice alwa
 GPU; ``collision`` / ``precision`` select BGK|MRT and fp32|fp16|fp64), ``spaceControl``
 (geometry, DX), ``timeControl`` (DT, startTime, endTime), ``module``, ``flowProperties``
 (constant viscosity, optional ``force``), ``thermalPropertiesFluid`` / ``thermalPropertiesSolid``
-(normalize.Trange, thermalDiff constant|Prandtl|derived, constant conductivity and capacity),
+(normalize.Trange, thermalDiff constant|Prandtl|derived, constant or polynomial conductivity,
+constant, polynomial or NASA7 capacity),
 ``chemicalProperties`` with ``type: pyrolysis``
 (single-step pyrolysis of reactive solid zones), ``boundaryCondition`` (inlet / outlet / wall /
 periodic flow sides, fixedValue / zeroGradient / periodic temperature), ``geometry`` (sphere,
@@ -177,7 +178,7 @@ def build_case(config: dict, logger: logging.Logger):
                 setter("thermal_diff_derived")()
             else:
                 raise NotImplementedError(f"{key}.thermalDiff.type {ttype!r} is not on the CUDA path")
-        # src/LBM/app.py:143-175: constant values; polynomial / NASA7 / mixture raise in the setters
+        # src/LBM/app.py:143-175: constant, polynomial and NASA7 values; mixture raises in the setters
         for prop in ("conductivity", "capacity"):
             pd = tp.get(prop)
             if not pd:

@@ -6,13 +6,15 @@ reference's YAML driver calls (src/LBM/app.py:101-602), ``init_simulation``,
 ``TS.S`` with ``to_numpy``/``from_numpy``) of src/LBM/LBM2D/__init__.py:29-70 and
 src/LBM/LBM3D/__init__.py:11-62, and run every step through the C ABI.
 
-Supported on the CUDA path: constant viscosity (IDEAL_GAS or INCOMPRESSIBLE),
-binary solid masks with halfway bounce-back, body force (Guo), BGK or MRT,
-the reference's two temperature fields (TF in fluid, TS in solid; with a binary mask
-they exchange no heat, so the interface is adiabatic), or with pyrolysis the conjugate
-temperature field (one distribution over fluid and solid), the
-single-step pyrolysis model with solid->fluid flip, and NEE boundaries
-(inlet / outlet / wall / symmetric, temperature fixedValue / zeroGradient).
+Supported on the CUDA path: constant or Sutherland viscosity (IDEAL_GAS or
+INCOMPRESSIBLE), binary solid masks with halfway bounce-back, porous cells, body force
+(Guo), BGK or MRT, the reference's two temperature fields (TF in fluid, TS in solid; with a
+binary mask they exchange no heat, so the interface is adiabatic; in porous cells they
+exchange heat and radiate), or with pyrolysis the conjugate temperature field (one
+distribution over fluid and solid), constant, Prandtl or derived thermal diffusivities (the
+latter two per cell, derived from constant, polynomial or NASA7 properties), the
+single-step pyrolysis model with solid->fluid flip, and NEE / ES / NEBB boundaries
+(inlet / outlet / wall / symmetric / flow-rate inlet, temperature fixedValue / zeroGradient).
 Features of the reference outside that set raise NotImplementedError with the
 reason instead of silently running something else.
 """
