@@ -627,13 +627,14 @@ struct Kern {
   // Thermal relaxation rate of a cell: its phase's constant, or where the phase's bit of
   // tprop is set (collision codes kCollSutherland + BGK/MRT) the derived diffusivity at
   // the cell's temperature, TF/TS.coefDiff with DERIVED (src/LBM/LBM2D/_thermal.py:62-71,
-  // :167-174), conductivity and capacity in the nested form of :72-107 / :175-210, and
+  // :167-174), conductivity and capacity in the nested form of :79, :93, :97-99 / :182, :196,
+  // :200-202, and
   // tau = 3 D + 1/2 (2D) or 4 D + 1/2 (3D) (_scalarField.py:56-58 of LBM2D / LBM3D).
   template <int COLL>
   __device__ __forceinline__ static C itau_thermal(const P& p, bool fluid, C T, C rho) {
     if constexpr (coll_sutherland(COLL)) {
       if (fluid && ((p.tprop >> 2) & 1)) {
-        // PRANDTL: kinetic_viscosity / Pr, src/LBM/LBM2D/_thermal.py:66-67, _evolution.py:227-246
+        // PRANDTL: kinetic_viscosity / Pr, src/LBM/LBM2D/_thermal.py:67-68, _evolution.py:227-246
         C nu = p.nu;
         if (p.suth) {
           const C TK = T * p.Tscale + p.Tref;

@@ -116,7 +116,7 @@ typedef struct orc_cfg {
     double tp_cap_Tmid[2], tp_cap_mul[2]; /* NASA7 switch temperature (K), R for a fluid NASA7 */
     double tp_rhos, tp_dt, tp_dx2;        /* solid density, dt, dx^2 */
     double tp_prandtl;       /* tprop bit 2: the fluid's THERMAL_DIFF_MODEL.PRANDTL,
-                              * D = kinetic_viscosity(i)/Pr (LBM2D/_thermal.py:66-67) */
+                              * D = kinetic_viscosity(i)/Pr (LBM2D/_thermal.py:67-68) */
 } orc_cfg;
 
 #define ORC_SIGMA 5.670374419e-8   /* Stefan-Boltzmann constant, src/LBM/util/constant.py:20 */
@@ -528,7 +528,7 @@ void orc_init_solid_T(orc* o, const double* Ts) {
 /* --------------------------------------------------------------- the step */
 
 /* c0 + T (c1 + T (c2 T + T (c3 + T c4))): conductivity and capacity_m in the reference's
- * evaluation order (LBM2D/_thermal.py:76-78, :86-101, :179-181, :192-201) */
+ * evaluation order (LBM2D/_thermal.py:79, :93, :97-99, :182, :196, :200-202) */
 static REAL nested5(const double* c, REAL T) {
     return (REAL)c[0] + T*((REAL)c[1] + T*((REAL)c[2]*T + T*((REAL)c[3] + T*(REAL)c[4])));
 }
